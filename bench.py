@@ -1,0 +1,466 @@
+"""Benchmark: subgame solves/s (and p50/p99 latency) of the B200 street solver.
+
+Workload (one step = one full solve): the 3-player turn subgame with
+depth-limited leaves -- seeded 4-card board, all 1128 non-board combos per
+player with weights U(0,1) and ~30% zeroed, pot 150, stacks 500, bets
+{0.33, 0.75, 1.5 pot, all-in}, 3 raises, continuation leaves with per-hand
+values N(0, 0.3 pot); 1000 Linear-CFR iterations in FP32 (21,436 nodes,
+15,616 leaves).  Synthetic seeded inputs stand in for the reference's
+realtime requests; there is no dataset.
+
+  value  -- solves/s with the subgame resident in HBM (ss_session_reset +
+            ss_session_run), timed with CUDA events on the session's stream
+  e2e    -- solves/s through the reference-facing C ABI (ss_solve_gpu) from a
+            host-built tree: tables, ranges and leaf values host->device,
+            average strategies device->host, inside the timed region
+N GPUs (torchrun): every rank solves its own seeded subgames (weak scaling,
+no data-path collective); the step time is the max over ranks.
+
+--impl reference times the reference's own implementation of this path on
+the host cores: src/cuda/street_solve.cu with its kernels run on the CPU
+(oracle/_ref, built by oracle/build_ref.py).  Its tuple enumeration is
+O(H^3) per leaf and hand for three players, so each step is a bounded sample
+(one iteration of the full tree at small range sizes, all cores busy) and the
+full-size rate is extrapolated with the fitted size exponent.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "poker-solver_b200")
+sys.path[:0] = [ROOT, PKG]
+
+METRIC = "subgame solves/s and p50/p99 latency at <=0.5% pot exploitability vs plain GPU"
+UNIT = "solves/s"
+WORKLOAD = "turn3"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--iterations", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if _cuda_ok() else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def _cuda_ok():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def dist_max(x):
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x):
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our solver
+# ---------------------------------------------------------------------------
+
+def build_subgame(seed, iterations):
+    import workloads as wl
+    cfg = wl.config(WORKLOAD, seed=seed, iterations=iterations)
+    sg = wl.AbiSubgame(cfg, max_hands=1326)
+    sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
+    return cfg, sg
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import street_solver_gpu as ssg
+
+    torch.cuda.set_device(local)
+    lib = ssg.load_library(1326)
+    lib.ss_session_create.restype = ctypes.c_int
+    lib.ss_session_run.restype = ctypes.c_int
+    lib.ss_session_reset.restype = ctypes.c_int
+    lib.ss_session_synchronize.restype = ctypes.c_int
+    lib.ss_session_profile.restype = ctypes.c_int
+    lib.ss_session_stream.restype = ctypes.c_void_p
+    lib.ss_session_stream.argtypes = [ctypes.c_void_p]
+    lib.ss_session_destroy.argtypes = [ctypes.c_void_p]
+    for f in ("ss_session_run", "ss_session_reset", "ss_session_synchronize"):
+        getattr(lib, f).argtypes = [ctypes.c_void_p] + ([ctypes.c_int] if f == "ss_session_run" else [])
+
+    cfg, sg = build_subgame(args.seed + rank, args.iterations)
+    opts = ssg.SSSolveOptions(local, 10, -1.0, 50, 0)
+    sess = ctypes.c_void_p()
+    rc = lib.ss_session_create(ctypes.byref(sg.td), ctypes.byref(opts), ctypes.byref(sess))
+    if rc != 0:
+        raise RuntimeError(f"ss_session_create failed ({rc}): {ssg.last_error(lib)}")
+
+    class Prof(ctypes.Structure):
+        _fields_ = [("num_classes", ctypes.c_int), ("name", (ctypes.c_char * 16) * 8),
+                    ("launches", ctypes.c_int * 8), ("ms", ctypes.c_double * 8),
+                    ("bytes", ctypes.c_double * 8), ("iteration_ms", ctypes.c_double)]
+
+    def check(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc}): {ssg.last_error(lib)}")
+
+    # one profiled iteration (graph with event nodes between kernel classes)
+    check(lib.ss_session_reset(sess), "reset")
+    prof = Prof()
+    check(lib.ss_session_profile(sess, ctypes.byref(prof)), "profile")
+    classes = {}
+    for k in range(prof.num_classes):
+        name = bytes(prof.name[k]).split(b"\0")[0].decode()
+        classes[name] = {"launches": prof.launches[k], "ms": prof.ms[k], "bytes": prof.bytes[k]}
+    launches_per_iter = sum(v["launches"] for v in classes.values())
+    reach_launches = classes["reach"]["launches"]
+
+    stream = torch.cuda.ExternalStream(lib.ss_session_stream(sess), device=local)
+
+    def step():
+        check(lib.ss_session_reset(sess), "reset")
+        check(lib.ss_session_run(sess, args.iterations), "run")
+
+    for _ in range(args.warmup):
+        step()
+    check(lib.ss_session_synchronize(sess), "sync")
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    times = []
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev_end = torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev0.record(stream)
+    evs[0].record(stream)
+    for i in range(args.steps):
+        step()
+        evs[i + 1].record(stream)
+    ev_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = ev0.elapsed_time(ev_end)
+    times = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms_max = dist_max(total_ms)
+    solves = dist_sum(args.steps)
+    value = solves / (total_ms_max / 1000.0)
+
+    # end to end through ss_solve_gpu with host buffers
+    out = ssg.SSOutput()
+    stats = ssg.SSSolveStats()
+    e2e_opts = ssg.SSSolveOptions(local, 10, -1.0, 50, 0)
+
+    def e2e_step():
+        r = lib.ss_solve_gpu_ex(ctypes.byref(sg.td), args.iterations, ctypes.byref(e2e_opts),
+                                ctypes.byref(out), ctypes.byref(stats))
+        check(r, "ss_solve_gpu")
+        lib.ss_free_output(ctypes.byref(out))
+
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = dist_max(time.perf_counter() - t0)
+    e2e_value = dist_sum(args.steps) / e2e_s
+
+    np_ = cfg["num_players"]
+    nh = [len(h) for h in cfg["hands"]]
+    mh = max(nh)
+    ndec, nnodes = sg.td.num_decision_nodes, sg.td.num_nodes
+    h2d = (nnodes * 104 + sg.td.num_children_total * 4 + np_ * mh * 8 + np_ * mh * 4
+           + sg.num_leaves * np_ * mh * 4)
+    d2h = ndec * 8 * mh * 4 + sum(nh) * 4 + np_ * mh * 4
+
+    dom = max((k for k in classes if k != "other"), key=lambda k: classes[k]["ms"])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    if not peak:
+        peak = 6650.0
+    d = classes[dom]
+    achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else 0.0
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
+        if dom in tr.get("classes", {}):
+            traffic = tr["classes"][dom].get("dram_bytes_per_iteration")
+    except Exception:
+        pass
+
+    lib.ss_session_destroy(sess)
+    sg.free()
+    return {
+        "value": value, "ms_per_step": total_ms_max / args.steps, "times": times,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "clocks": clk,
+        "gpu_launches": int(args.steps * (args.iterations * launches_per_iter + reach_launches)),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "bytes_per_iteration": d["bytes"],
+                     "kernel_ms_per_iteration": d["ms"]},
+        "profile": {k: {"ms": round(v["ms"], 4), "launches": v["launches"],
+                        "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
+                    for k, v in classes.items() if v["launches"]},
+        "iteration_ms": prof.iteration_ms,
+        "tree": {"nodes": nnodes, "decision": ndec, "leaves": sg.num_leaves, "hands": nh},
+    }
+
+
+# ---------------------------------------------------------------------------
+# the reference on the host cores
+# ---------------------------------------------------------------------------
+
+class _Quiet:
+    """Silence the reference's printf progress lines (fd 1) during a call."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def reference_cpu(seed, budget_s=25.0):
+    """Seconds per CFR iteration of the reference kernels (host build) on the
+    full turn3 tree, measured at small range sizes with every core running
+    its own solve, and extrapolated to 1128 hands per player."""
+    import workloads as wl
+    from oracle.oracle import RefStreetSolve, ref_available
+    if not ref_available(200, 3):
+        return None
+    ref = RefStreetSolve(200, 3, "cpu")
+    cores = os.cpu_count() or 1
+    full = wl.config(WORKLOAD, seed=seed)
+    sizes, per_iter = [], []
+    t_start = time.perf_counter()
+    for H in (6, 8, 10, 12):
+        cfg = wl.config(WORKLOAD, seed=seed, num_hands=H)
+        Hm, Wm, nh = wl.padded(cfg)
+        results = [None] * cores
+
+        def one(i):
+            td = ref.build(cfg["board"], cfg["pot"], cfg["stack"], cfg["bet_sizes"], 3)
+            lv = wl.leaf_values_for(cfg, td.num_leaves)
+            t0 = time.perf_counter()
+            ref.solve(td, Hm, Wm, nh, 1, leaf_values=lv)
+            results[i] = time.perf_counter() - t0
+            ref.free(td)
+
+        with _Quiet():
+            th = [threading.Thread(target=one, args=(i,)) for i in range(cores)]
+            t0 = time.perf_counter()
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            wall = time.perf_counter() - t0
+        sizes.append(H)
+        per_iter.append(wall / cores)  # aggregate seconds per iteration per solve
+        if time.perf_counter() - t_start > budget_s:
+            break
+    x, y = np.log(np.array(sizes[-2:], float)), np.log(np.array(per_iter[-2:], float))
+    expo = float((y[1] - y[0]) / (x[1] - x[0])) if len(sizes) >= 2 else 3.0
+    H_full = len(full["hands"][0])
+    s_iter_full = per_iter[-1] * (H_full / sizes[-1]) ** expo
+    return {"cores": cores, "sizes": sizes, "sec_per_iter": per_iter, "exponent": expo,
+            "sec_per_iter_full": s_iter_full,
+            "solves_per_s": 1.0 / (s_iter_full * 1000)}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        if rank == 0:
+            r = reference_cpu(args.seed)
+            if r is None:
+                print(json.dumps({"impl": "reference",
+                                  "unavailable": "oracle/_ref reference build missing"}))
+            else:
+                line = {
+                    "impl": "reference", "metric": METRIC, "value": r["solves_per_s"], "unit": UNIT,
+                    "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": 1000.0 / r["solves_per_s"], "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                    "config": {"workload": "3-player turn subgame, 1128 combos/player, "
+                                           "continuation leaves, 1000 Linear-CFR iterations",
+                               "iterations": args.iterations},
+                    "cpu_baseline": {"value": r["solves_per_s"], "unit": UNIT, "cores": r["cores"],
+                                     "kind": "reference",
+                                     "sample": f"street_solve.cu kernels on the host, full 21,436-node "
+                                               f"tree, 1 iteration at {r['sizes']} hands/player, "
+                                               f"extrapolated to 1128 with exponent "
+                                               f"{r['exponent']:.2f}"},
+                    "e2e": {"value": r["solves_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0},
+                }
+                print(json.dumps(line))
+        return 0
+
+    res = run_ours(args, world, rank, local)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = reference_cpu(args.seed, budget_s=20.0)
+        if r is not None:
+            cpu = {"value": r["solves_per_s"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                   "sample": f"street_solve.cu kernels on the host, full tree, 1 iteration at "
+                             f"{r['sizes']} hands/player, extrapolated to 1128 (exponent "
+                             f"{r['exponent']:.2f})"}
+    if rank == 0:
+        t = sorted(res["times"])
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "3-player turn subgame, 1128 combos/player, continuation leaves, "
+                                   "1000 Linear-CFR iterations",
+                       "iterations": args.iterations, "tree": res["tree"],
+                       "l2": "state larger than L2 (regrets, sums, reach, values ~400 MB)",
+                       "parallelism": f"replicas x{world}",
+                       "p50_ms": t[len(t) // 2], "p99_ms": t[-1]},
+            "roofline": res["roofline"], "cpu_baseline": cpu, "clocks": res["clocks"],
+            "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
+            "iteration_ms": res["iteration_ms"], "profile": res["profile"],
+        }
+        print(json.dumps(line))
+    try:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            dist.destroy_process_group()
+    except Exception:
+        pass
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,273 @@
+/*
+ * street_solve.h -- C ABI of the B200 single-street N-player Linear-CFR
+ * subgame solver.
+ *
+ * Drop-in for the reference interface src/cuda/street_solve.cuh: the structs
+ * SSNode / SSTreeData / SSOutput keep the reference field order, types and
+ * sizes byte for byte (street_solve.cuh:52-65, 69-122, 126-143), and the four
+ * entry points keep the reference names, argument meaning and "0 on success"
+ * convention (street_solve.cuh:172-194), so python/street_solver_gpu.py and
+ * python/leaf_values.py bind this library unchanged.
+ *
+ * Two builds of the same source differ only in SS_MAX_HANDS, which is part
+ * of the SSTreeData layout:
+ *   libstreet_solve.so       SS_MAX_HANDS = 200   (reference layout)
+ *   libstreet_solve_wide.so  SS_MAX_HANDS = 1326  (every 2-card combo)
+ * ss_abi_info() reports which one is loaded.
+ *
+ * Entry points marked EXTENSION have no counterpart in the reference.
+ */
+#ifndef B200_STREET_SOLVE_H
+#define B200_STREET_SOLVE_H
+
+#include <stdint.h>
+
+/* ── Limits (street_solve.cuh:35-42) ─────────────────────────────────── */
+
+#define SS_MAX_PLAYERS     6
+#ifndef SS_MAX_HANDS
+#define SS_MAX_HANDS       200
+#endif
+#define SS_MAX_ACTIONS     8
+#define SS_MAX_TREE_NODES  4096   /* informational, as in the reference (never enforced there) */
+#define SS_MAX_BOARD       5
+#define SS_MAX_LEAVES      64     /* informational, as in the reference */
+#define SS_NUM_CONT_STRATS 4
+#define SS_MAX_RAISES      3      /* default raise cap of ss_build_tree */
+
+/* Node types (street_solve.cuh:45-49) */
+#define SS_NODE_DECISION  0
+#define SS_NODE_FOLD      1
+#define SS_NODE_SHOWDOWN  2
+#define SS_NODE_LEAF      4
+
+/* Return codes.  0 is success; every failure is negative, so callers that
+ * test "!= 0" (the reference convention, street_solve.cu:29-36) still work. */
+#define SS_OK                0
+#define SS_ERR_INVALID      -1   /* malformed tree, ranges or arguments */
+#define SS_ERR_CUDA         -2   /* CUDA runtime or launch failure */
+#define SS_ERR_NOMEM        -3   /* device or host allocation failed */
+#define SS_ERR_UNSUPPORTED  -4   /* terminal class this build cannot solve at this size */
+#define SS_ERR_NO_DEVICE    -5   /* no CUDA device */
+
+/* ── Flat tree node (street_solve.cuh:52-65), 26 x int32 = 104 bytes ─── */
+
+typedef struct {
+    int type;                     /* SS_NODE_* */
+    int player;                   /* acting player at decisions; winner at folds; -1 otherwise */
+    int num_children;
+    int first_child;              /* index into SSTreeData.children */
+    int pot;                      /* chips */
+    int bets[SS_MAX_PLAYERS];     /* each player's total bet this street */
+    int board_cards[5];
+    int num_board;
+    int leaf_idx;                 /* SS_NODE_LEAF: row of leaf_values */
+    int fold_player;              /* kept for layout; the builder leaves it -1 */
+    int num_players;              /* active (non-folded) players at this node */
+    int active_players[SS_MAX_PLAYERS];
+} SSNode;
+
+/* ── Solver input (street_solve.cuh:69-122) ──────────────────────────── */
+
+typedef struct {
+    SSNode *nodes;
+    int *children;
+    int num_nodes;
+    int num_children_total;
+
+    int num_players;
+
+    int hands[SS_MAX_PLAYERS][SS_MAX_HANDS][2];
+    float weights[SS_MAX_PLAYERS][SS_MAX_HANDS];
+    int num_hands[SS_MAX_PLAYERS];
+
+    int board[SS_MAX_BOARD];
+    int num_board;
+
+    /* leaf_values[leaf_idx * num_players * max_hands + p * max_hands + h],
+     * max_hands = max(num_hands).  Caller-owned: ss_free_tree never frees it. */
+    float *leaf_values;
+    int num_leaves;
+
+    int *level_order;
+    int *node_depth;
+    int max_depth;
+
+    int *decision_node_indices;
+    int num_decision_nodes;
+    int *showdown_node_indices;
+    int num_showdown_nodes;
+    int *leaf_node_indices;
+    int num_leaf_nodes;
+    int *fold_node_indices;
+    int num_fold_nodes;
+
+    int starting_pot;
+    int effective_stack;
+    int is_river;
+
+    /* frozen_action[node] = action index forced at that node for every hand
+     * (-1 = free); NULL disables freezing.  Caller-owned. */
+    int *frozen_action;
+} SSTreeData;
+
+/* ── Solver output (street_solve.cuh:126-143) ────────────────────────── */
+
+typedef struct {
+    float *root_strategy;         /* [root_num_actions][num_hands[root_player]], last iterate */
+    int root_num_actions;
+    int root_player;
+    float *root_ev;               /* [num_players][max_hands]; row 0 = root values of the last traverser */
+    float *avg_strategies;        /* [num_avg_nodes][SS_MAX_ACTIONS][max_hands] */
+    int *avg_strategy_node_ids;   /* [num_avg_nodes], decision nodes in index order */
+    int num_avg_nodes;
+    int num_players;
+    int max_hands;
+} SSOutput;
+
+/* ── EXTENSION types ─────────────────────────────────────────────────── */
+
+typedef struct {
+    int abi_version;              /* 1 */
+    int max_hands;                /* SS_MAX_HANDS of this build */
+    int max_players;
+    int max_actions;
+    int sizeof_node;
+    int sizeof_tree;
+    int sizeof_output;
+} SSAbiInfo;
+
+typedef struct {
+    int device;                   /* CUDA device ordinal (default 0) */
+    int graph_iterations;         /* CFR iterations per captured CUDA graph (default 10) */
+    float target_exploitability;  /* stop at this exploitability, % of pot; <= 0: run all iterations */
+    int check_every;              /* iterations between exploitability checks (default 50) */
+    int compute_exploitability;   /* 1: report the final exploitability in SSSolveStats */
+} SSSolveOptions;
+
+typedef struct {
+    int iterations_run;
+    double exploitability_pct;    /* NashConv / num_players / starting_pot * 100, FP64; -1 if not computed */
+    double nashconv;              /* sum over players of best-response gain per unit of deal mass */
+    double solve_ms;              /* device time of the CFR iterations */
+    double node_hand_updates;     /* num_nodes x sum of hand counts x iterations */
+} SSSolveStats;
+
+/* A resident subgame: plan, device state and captured CUDA graphs stay on the
+ * GPU between calls, so iterations can be added, the state reset or the
+ * outputs read without re-uploading anything. */
+typedef struct SSSession SSSession;
+
+/* Per-kernel-class device time of one iteration (ss_session_profile). */
+#define SS_PROFILE_CLASSES 8
+typedef struct {
+    int num_classes;
+    char name[SS_PROFILE_CLASSES][16];
+    int launches[SS_PROFILE_CLASSES];
+    double ms[SS_PROFILE_CLASSES];       /* summed device time of the class in the iteration */
+    double bytes[SS_PROFILE_CLASSES];    /* bytes the class must move in the iteration (minimum) */
+    double iteration_ms;                 /* device time of the whole iteration */
+} SSKernelProfile;
+
+/* ── Host API ────────────────────────────────────────────────────────── */
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Build the betting tree for one street.  Replaces street_solve.cuh:172-178
+ * (definition street_solve.cu:1192-1296): same node numbering, children
+ * order, leaf numbering, BFS order and per-type index lists, with the
+ * reference raise cap SS_MAX_RAISES.  Zeroes *tree_out first; the caller then
+ * fills hands / weights / num_hands and, optionally, leaf_values and
+ * frozen_action. */
+int ss_build_tree(const int *board, int num_board,
+                  int starting_pot, int effective_stack,
+                  const float *bet_sizes, int num_bet_sizes,
+                  int num_players, const int *acting_order,
+                  int is_river, int use_cont_strats,
+                  SSTreeData *tree_out);
+
+/* Run max_iterations Linear-CFR iterations (every player traverses once per
+ * iteration, in player order) on the GPU and fill *output.  Replaces
+ * street_solve.cuh:186-190 (definition street_solve.cu:1298-1639).  Returns
+ * SS_OK or a negative SS_ERR_* code; on failure *output is left zeroed and
+ * nothing is leaked. */
+int ss_solve_gpu(SSTreeData *tree_data, int max_iterations, SSOutput *output);
+
+/* Free what ss_build_tree allocated (street_solve.cuh:192).  Unlike the
+ * reference (street_solve.cu:1650) it does not free the caller-owned
+ * leaf_values or frozen_action buffers. */
+void ss_free_tree(SSTreeData *tree_data);
+
+/* Free what ss_solve_gpu allocated (street_solve.cuh:193). */
+void ss_free_output(SSOutput *output);
+
+/* EXTENSION: layout of this build (which SS_MAX_HANDS the structs use). */
+int ss_abi_info(SSAbiInfo *info);
+
+/* EXTENSION: ss_build_tree with an explicit raise cap (the reference fixes it
+ * at compile time, street_solve.cuh:42). */
+int ss_build_tree_ex(const int *board, int num_board,
+                     int starting_pot, int effective_stack,
+                     const float *bet_sizes, int num_bet_sizes,
+                     int num_players, const int *acting_order,
+                     int is_river, int use_cont_strats, int max_raises,
+                     SSTreeData *tree_out);
+
+/* EXTENSION: default options. */
+void ss_default_options(SSSolveOptions *opts);
+
+/* EXTENSION: ss_solve_gpu with options (device, graph block, early stop at
+ * an exploitability target) and statistics.  opts / stats may be NULL. */
+int ss_solve_gpu_ex(SSTreeData *tree_data, int max_iterations,
+                    const SSSolveOptions *opts, SSOutput *output, SSSolveStats *stats);
+
+/* EXTENSION: FP64 exploitability of an average-strategy profile given in the
+ * SSOutput layout ([num_decision_nodes][SS_MAX_ACTIONS][max_hands]) on the GPU.
+ * br_value / cur_value (may be NULL) receive, per player, the best-response
+ * and profile value summed over the player's hands weighted by range weight;
+ * *deal_mass the valid-deal mass.  Returns SS_OK or SS_ERR_*. */
+int ss_exploitability_gpu(const SSTreeData *tree_data, const float *avg_strategies,
+                          double *exploitability_pct, double *nashconv,
+                          double *br_value, double *cur_value, double *deal_mass);
+
+/* EXTENSION: create a resident session for one subgame (copies everything it
+ * needs; tree_data may be freed afterwards). */
+int ss_session_create(const SSTreeData *tree_data, const SSSolveOptions *opts, SSSession **out);
+
+/* EXTENSION: enqueue `iterations` more CFR iterations (asynchronous). */
+int ss_session_run(SSSession *session, int iterations);
+
+/* EXTENSION: wait for the session's queued work. */
+int ss_session_synchronize(SSSession *session);
+
+/* EXTENSION: back to iteration 0 (regrets, strategy sums and reach reset). */
+int ss_session_reset(SSSession *session);
+
+/* EXTENSION: iterations run since creation or the last reset. */
+int ss_session_iterations(const SSSession *session);
+
+/* EXTENSION: wait, then fill *output exactly as ss_solve_gpu would after the
+ * same number of iterations (free it with ss_free_output). */
+int ss_session_output(SSSession *session, SSOutput *output);
+
+/* EXTENSION: run one more iteration as a graph with event nodes between the
+ * kernel classes and report their device times and minimum bytes. */
+int ss_session_profile(SSSession *session, SSKernelProfile *profile);
+
+/* EXTENSION: the CUDA stream (cudaStream_t) the session's kernels run on, so a
+ * caller can order its own work or time the session with CUDA events. */
+void *ss_session_stream(SSSession *session);
+
+/* EXTENSION: release the session. */
+void ss_session_destroy(SSSession *session);
+
+/* EXTENSION: message for the last failure on the calling thread ("" if none). */
+const char *ss_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200_STREET_SOLVE_H */

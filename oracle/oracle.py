@@ -39,7 +39,7 @@ class Node(ctypes.Structure):
     _fields_ = NODE_FIELDS
 
 
-NODE_INTS = ctypes.sizeof(Node) // 4  # 23
+NODE_INTS = ctypes.sizeof(Node) // 4  # 26
 
 
 class OrcTree(ctypes.Structure):

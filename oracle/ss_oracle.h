@@ -19,7 +19,7 @@
 #define ORC_NODE_SHOWDOWN 2
 #define ORC_NODE_LEAF 4
 
-/* Same 23-int field set and order as the reference SSNode
+/* Same 26-int field set and order as the reference SSNode
  * (src/cuda/street_solve.cuh:52-65), so node arrays compare byte for byte. */
 typedef struct {
     int type;

@@ -1,0 +1,560 @@
+// ss_engine.cu -- host orchestration: one resident subgame per Session.
+//
+// Replaces the per-iteration launch loop of the reference (street_solve.cu:
+// 1471-1550), which re-runs regret matching for every node and re-propagates
+// every opponent's reach for every traverser, with blocking copies in between.
+// Here:
+//   * regret matching is fused into the kernels that consume the strategy
+//     (reach propagation and the traverser's value/regret update), so no
+//     strategy array exists;
+//   * a player's strategy only changes when that player traverses (the
+//     reference's regret pruning never changes a strategy), so each player's
+//     reach is re-propagated once per iteration, right after its own regret
+//     update, instead of once per other traverser;
+//   * an iteration (terminals, bottom-up updates, reach) is captured once as
+//     a CUDA graph and replayed; the iteration number lives on the device;
+//   * plan, tables and state stay resident in a Session, so a solve can be
+//     extended, reset or read without re-uploading.
+#include "ss_kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace ssb {
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Blob {
+    std::vector<char> host;
+    size_t add(const void *src, size_t bytes) {
+        size_t off = (host.size() + 255) & ~static_cast<size_t>(255);
+        host.resize(off + bytes);
+        if (bytes) std::memcpy(host.data() + off, src, bytes);
+        return off;
+    }
+    template <class T>
+    size_t add(const std::vector<T> &v) {
+        return add(v.data(), v.size() * sizeof(T));
+    }
+};
+
+void keep_pool_warm(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = 8ull << 30;  // keep up to 8 GiB cached between solves
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done[device] = true;
+}
+
+// tuple visits of the enumeration kernel that one solve may spend
+constexpr double kEnumLimitPerIter = 4e9;
+constexpr double kEnumLimitTotal = 2e11;
+
+enum ProfClass { PC_REACH = 0, PC_CFV, PC_FILL, PC_CR1, PC_CR2, PC_SD1, PC_ENUM, PC_OTHER };
+const char *kClassName[SS_PROFILE_CLASSES] = {"reach", "cfv", "term_fill", "term_cr1",
+                                             "term_cr2", "term_sd1", "term_enum", "other"};
+
+int term_class(int kind) {
+    switch (kind) {
+        case TK_ZERO:
+        case TK_LEAF0: return PC_FILL;
+        case TK_CR1: return PC_CR1;
+        case TK_CR2: return PC_CR2;
+        case TK_SD1: return PC_SD1;
+        default: return PC_ENUM;
+    }
+}
+
+}  // namespace
+
+void set_error(const std::string &msg) { g_err = msg; }
+const char *last_error() { return g_err.c_str(); }
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            set_error(std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #call); \
+            return e_ == cudaErrorMemoryAllocation ? SS_ERR_NOMEM : SS_ERR_CUDA;      \
+        }                                                                             \
+    } while (0)
+
+class Session {
+  public:
+    Plan P;
+    int device = 0;
+    int graph_iters = 10;
+    int iterations = 0;
+    cudaStream_t stream = nullptr;
+    char *dbase = nullptr;    // static tables
+    float *dstate = nullptr;  // R, S, reach, val
+    float *dleaf = nullptr;
+    float *dsmall = nullptr;  // root strategy snapshot + root values
+    int *diter = nullptr;
+    size_t nR = 0, nReach = 0, nVal = 0, n_rs = 0;
+    int frozen_root = -1;
+    DevCtx c{};
+    const ReachItem *reach_items[SS_MAX_PLAYERS] = {};
+    std::vector<std::pair<int, int>> reach_lv[SS_MAX_PLAYERS];
+    const CfvItem *cfv_items[SS_MAX_PLAYERS] = {};
+    std::vector<std::pair<int, int>> cfv_lv[SS_MAX_PLAYERS];
+    const TermItem *term_items[SS_MAX_PLAYERS][TK_COUNT] = {};
+    const int *root_fr[SS_MAX_PLAYERS] = {};
+    const int *dec_fe = nullptr, *dec_na = nullptr, *dec_pl = nullptr;
+    // per (player, level) / (traverser, kind) minimum bytes, for the profile
+    std::vector<double> reach_bytes[SS_MAX_PLAYERS], cfv_bytes[SS_MAX_PLAYERS];
+    double term_bytes[SS_MAX_PLAYERS][TK_COUNT] = {};
+    cudaGraphExec_t gA = nullptr, gC = nullptr, gB = nullptr;  // G iters, 1 iter, 1 iter + snapshot
+
+    // profiling hook: when set, every launch is preceded by an event record
+    struct Mark {
+        int cls;
+        double bytes;
+        cudaEvent_t ev;
+    };
+    std::vector<Mark> *marks = nullptr;
+
+    ~Session() {
+        if (gA) cudaGraphExecDestroy(gA);
+        if (gB) cudaGraphExecDestroy(gB);
+        if (gC) cudaGraphExecDestroy(gC);
+        if (stream) {
+            if (dbase) cudaFreeAsync(dbase, stream);
+            if (dstate) cudaFreeAsync(dstate, stream);
+            if (dleaf) cudaFreeAsync(dleaf, stream);
+            if (dsmall) cudaFreeAsync(dsmall, stream);
+            if (diter) cudaFreeAsync(diter, stream);
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+    }
+
+    cudaError_t mark(int cls, double bytes) {
+        if (!marks) return cudaSuccess;
+        Mark m{cls, bytes, nullptr};
+        cudaError_t e = cudaEventCreate(&m.ev);
+        if (e != cudaSuccess) return e;
+        marks->push_back(m);
+        return cudaEventRecord(m.ev, stream);
+    }
+
+    cudaError_t reach(int p) {
+        for (size_t l = 0; l < reach_lv[p].size(); ++l) {
+            cudaError_t e = mark(PC_REACH, reach_bytes[p][l]);
+            if (e == cudaSuccess)
+                e = launch_reach(c, reach_items[p] + reach_lv[p][l].first, reach_lv[p][l].second,
+                                 P.H[p], stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
+    cudaError_t pass(int t, bool snapshot_root) {
+        cudaError_t e = cudaSuccess;
+        if (snapshot_root) {
+            e = mark(PC_OTHER, 0);
+            if (e == cudaSuccess)
+                e = launch_root_strategy(c, P.first_edge[0], P.root_na, frozen_root,
+                                         P.H[P.root_player], dsmall, stream);
+            if (e != cudaSuccess) return e;
+        }
+        for (int k = 0; k < TK_COUNT; ++k) {
+            const int n = static_cast<int>(P.term[t][k].size());
+            if (n == 0) continue;
+            e = mark(term_class(k), term_bytes[t][k]);
+            if (e == cudaSuccess) e = launch_terms(c, k, term_items[t][k], n, t, stream);
+            if (e != cudaSuccess) return e;
+        }
+        for (size_t l = 0; l < cfv_lv[t].size(); ++l) {
+            e = mark(PC_CFV, cfv_bytes[t][l]);
+            if (e == cudaSuccess)
+                e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.H[t],
+                               stream);
+            if (e != cudaSuccess) return e;
+        }
+        return reach(t);
+    }
+
+    cudaError_t iteration(bool last) {
+        cudaError_t e = mark(PC_OTHER, 0);
+        if (e == cudaSuccess) e = launch_bump(diter, stream);
+        for (int t = 0; t < P.np && e == cudaSuccess; ++t) e = pass(t, last && t == P.np - 1);
+        return e;
+    }
+
+    cudaError_t capture(int iters, bool last, cudaGraphExec_t *exec) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        cudaError_t body = cudaSuccess;
+        for (int i = 0; i < iters && body == cudaSuccess; ++i) body = iteration(last && i == iters - 1);
+        e = cudaStreamEndCapture(stream, &g);
+        if (body != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return body;
+        }
+        if (e != cudaSuccess) return e;
+        e = cudaGraphInstantiate(exec, g, 0);
+        cudaGraphDestroy(g);
+        return e;
+    }
+
+    int init(const Problem &pb, const SolveConfig &cfg);
+    int reset();
+    int run(int iters);
+    int output(SSOutput *out);
+    int profile(SSKernelProfile *prof);
+};
+
+int Session::init(const Problem &pb, const SolveConfig &cfg) {
+    int rc = build_plan(pb, &P);
+    if (rc != SS_OK) return rc;
+    if (P.enum_work > kEnumLimitPerIter) {
+        set_error("terminals with three or more counted opponents (or multiway showdowns) need " +
+                  std::to_string(P.enum_work) +
+                  " tuple visits per iteration; only small ranges are supported for them");
+        return SS_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device");
+        return SS_ERR_NO_DEVICE;
+    }
+    if (cfg.device < 0 || cfg.device >= ndev) {
+        set_error("device ordinal out of range");
+        return SS_ERR_INVALID;
+    }
+    device = cfg.device;
+    graph_iters = std::max(1, cfg.graph_iterations);
+    CK(cudaSetDevice(device));
+    keep_pool_warm(device);
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    const int np = P.np;
+    const size_t HS = static_cast<size_t>(P.HS);
+    const size_t E = static_cast<size_t>(P.E), N = static_cast<size_t>(P.N);
+
+    // ---- static tables and the minimum bytes of every launch ------------
+    Blob b;
+    size_t o_reach[SS_MAX_PLAYERS], o_cfv[SS_MAX_PLAYERS], o_term[SS_MAX_PLAYERS][TK_COUNT],
+        o_rootfr[SS_MAX_PLAYERS];
+    for (int p = 0; p < np; ++p) {
+        std::vector<ReachItem> all;
+        for (auto &lv : P.reach_levels[p]) {
+            reach_lv[p].push_back({static_cast<int>(all.size()), static_cast<int>(lv.size())});
+            double by = 0;
+            for (auto &it : lv) by += (2.0 * it.na + 1.0) * 4.0 * P.H[p];
+            reach_bytes[p].push_back(by);
+            all.insert(all.end(), lv.begin(), lv.end());
+        }
+        o_reach[p] = b.add(all);
+        std::vector<CfvItem> call;
+        for (auto &lv : P.cfv_levels[p]) {
+            cfv_lv[p].push_back({static_cast<int>(call.size()), static_cast<int>(lv.size())});
+            double by = 0;
+            for (auto &it : lv) {
+                const int nfr = P.fr_off[it.first_edge + it.na] - P.fr_off[it.first_edge];
+                by += (4.0 * it.na + nfr + 1.0) * 4.0 * P.H[p];
+            }
+            cfv_bytes[p].push_back(by);
+            call.insert(call.end(), lv.begin(), lv.end());
+        }
+        o_cfv[p] = b.add(call);
+        for (int k = 0; k < TK_COUNT; ++k) {
+            double by = 0;
+            for (auto &it : P.term[p][k]) {
+                by += 4.0 * HS;  // value row
+                if (it.leaf_off >= 0 && k != TK_ZERO) by += 4.0 * P.H[p];
+                if (k != TK_ZERO && k != TK_LEAF0)
+                    for (int i = 0; i < it.k; ++i) by += 4.0 * P.H[it.opp_player[i]];
+            }
+            term_bytes[p][k] = by;
+            o_term[p][k] = b.add(P.term[p][k]);
+        }
+        o_rootfr[p] = b.add(P.root_fr[p]);
+    }
+    const size_t o_fr_off = b.add(P.fr_off);
+    const size_t o_fr_items = b.add(P.fr_items);
+    const size_t o_code = b.add(P.hand_code);
+    const size_t o_sdpos = b.add(P.sd_pos);
+    const size_t o_str = b.add(P.strength);
+    const size_t o_sdc = b.add(P.sd_combo);
+    const size_t o_sdl = b.add(P.sd_card_list);
+    std::vector<int> dfe, dna, dpl;
+    for (int x : P.dec_nodes) {
+        dfe.push_back(P.first_edge[x]);
+        dna.push_back(pb.nodes[x].num_children);
+        dpl.push_back(pb.nodes[x].player);
+    }
+    const size_t o_dfe = b.add(dfe), o_dna = b.add(dna), o_dpl = b.add(dpl);
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dbase), std::max<size_t>(b.host.size(), 256), stream));
+    CK(cudaMemcpyAsync(dbase, b.host.data(), b.host.size(), cudaMemcpyHostToDevice, stream));
+    for (int p = 0; p < np; ++p) {
+        reach_items[p] = reinterpret_cast<const ReachItem *>(dbase + o_reach[p]);
+        cfv_items[p] = reinterpret_cast<const CfvItem *>(dbase + o_cfv[p]);
+        for (int k = 0; k < TK_COUNT; ++k)
+            term_items[p][k] = reinterpret_cast<const TermItem *>(dbase + o_term[p][k]);
+        root_fr[p] = reinterpret_cast<const int *>(dbase + o_rootfr[p]);
+    }
+    dec_fe = reinterpret_cast<const int *>(dbase + o_dfe);
+    dec_na = reinterpret_cast<const int *>(dbase + o_dna);
+    dec_pl = reinterpret_cast<const int *>(dbase + o_dpl);
+
+    // ---- state: regrets, strategy sums, reach (weights in the last np rows), values
+    nR = E * HS;
+    nReach = (E + np) * HS;
+    nVal = N * HS;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dstate), (2 * nR + nReach + nVal) * sizeof(float), stream));
+    CK(cudaMemsetAsync(dstate, 0, (2 * nR + nReach + nVal) * sizeof(float), stream));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&diter), sizeof(int), stream));
+    float *R = dstate, *S = R + nR, *reach = S + nR, *val = reach + nReach;
+    {
+        std::vector<float> w(static_cast<size_t>(np) * HS, 0.f);
+        for (int p = 0; p < np; ++p)
+            for (int h = 0; h < P.H[p]; ++h) w[p * HS + h] = pb.weights[p][h];
+        CK(cudaMemcpyAsync(reach + E * HS, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice,
+                           stream));
+        CK(cudaStreamSynchronize(stream));  // the staging vector must outlive the copy
+    }
+    if (pb.leaf_values && pb.num_leaves > 0) {
+        const size_t n = static_cast<size_t>(pb.num_leaves) * np * P.max_h;
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&dleaf), n * sizeof(float), stream));
+        CK(cudaMemcpyAsync(dleaf, pb.leaf_values, n * sizeof(float), cudaMemcpyHostToDevice, stream));
+    }
+    n_rs = static_cast<size_t>(P.root_na) * P.H[P.root_player];
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dsmall), (n_rs + HS) * sizeof(float), stream));
+
+    c.R = R;
+    c.S = S;
+    c.reach = reach;
+    c.val = val;
+    c.fr_off = reinterpret_cast<const int *>(dbase + o_fr_off);
+    c.fr_items = reinterpret_cast<const int *>(dbase + o_fr_items);
+    c.hand_code = reinterpret_cast<const int *>(dbase + o_code);
+    c.sd_pos = reinterpret_cast<const int *>(dbase + o_sdpos);
+    c.strength = reinterpret_cast<const unsigned *>(dbase + o_str);
+    c.sd_combo = reinterpret_cast<const SdCombo *>(dbase + o_sdc);
+    c.sd_card_list = reinterpret_cast<const short *>(dbase + o_sdl);
+    c.leaf_values = dleaf;
+    c.iter = diter;
+    c.HS = P.HS;
+    c.np = np;
+    c.ncomb = P.ncomb;
+    for (int p = 0; p < SS_MAX_PLAYERS; ++p) c.H[p] = p < np ? P.H[p] : 0;
+    frozen_root = pb.frozen ? pb.frozen[0] : -1;
+    return reset();
+}
+
+int Session::reset() {
+    CK(cudaSetDevice(device));
+    CK(cudaMemsetAsync(dstate, 0, 2 * nR * sizeof(float), stream));
+    CK(cudaMemsetAsync(c.val, 0, nVal * sizeof(float), stream));
+    CK(cudaMemsetAsync(diter, 0, sizeof(int), stream));
+    CK(cudaMemsetAsync(dsmall, 0, (n_rs + P.HS) * sizeof(float), stream));
+    for (int p = 0; p < P.np; ++p) CK(reach(p));  // all regrets zero: uniform (or frozen) play
+    iterations = 0;
+    return SS_OK;
+}
+
+int Session::run(int iters) {
+    if (iters < 0) {
+        set_error("iterations must be >= 0");
+        return SS_ERR_INVALID;
+    }
+    if (iters == 0) return SS_OK;
+    if (P.enum_work * (iterations + iters) > kEnumLimitTotal) {
+        set_error("enumerated terminals would need more than " + std::to_string(kEnumLimitTotal) +
+                  " tuple visits; only small ranges are supported for them");
+        return SS_ERR_UNSUPPORTED;
+    }
+    CK(cudaSetDevice(device));
+    const int rest = iters - 1;
+    const int qA = rest / graph_iters, rC = rest % graph_iters;
+    if (qA > 0 && !gA) CK(capture(graph_iters, false, &gA));
+    if (rC > 0 && !gC) CK(capture(1, false, &gC));
+    if (!gB) CK(capture(1, true, &gB));
+    for (int i = 0; i < qA; ++i) CK(cudaGraphLaunch(gA, stream));
+    for (int i = 0; i < rC; ++i) CK(cudaGraphLaunch(gC, stream));
+    CK(cudaGraphLaunch(gB, stream));
+    iterations += iters;
+    return SS_OK;
+}
+
+int Session::output(SSOutput *out) {
+    std::memset(out, 0, sizeof(*out));
+    CK(cudaSetDevice(device));
+    const int np = P.np, tl = np - 1;
+    const size_t n_avg = static_cast<size_t>(P.num_dec) * SS_MAX_ACTIONS * P.max_h;
+    float *davg = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&davg), std::max<size_t>(n_avg, 1) * sizeof(float), stream));
+    float *d_rev = dsmall + n_rs;
+    cudaError_t e = cudaSuccess;
+    if (iterations >= 1)
+        e = launch_sum_rows(c, root_fr[tl], static_cast<int>(P.root_fr[tl].size()), d_rev, P.H[tl], stream);
+    if (e == cudaSuccess)
+        e = launch_avg_strategy(c, dec_fe, dec_na, dec_pl, P.num_dec, P.max_h, davg, stream);
+    float *h_rs = static_cast<float *>(std::calloc(std::max<size_t>(n_rs, 1), sizeof(float)));
+    float *h_rev = static_cast<float *>(std::calloc(static_cast<size_t>(np) * P.max_h, sizeof(float)));
+    float *h_avg = static_cast<float *>(std::malloc(std::max<size_t>(n_avg, 1) * sizeof(float)));
+    int *h_ids = static_cast<int *>(std::malloc(std::max<size_t>(P.num_dec, 1) * sizeof(int)));
+    if (!h_rs || !h_rev || !h_avg || !h_ids) {
+        std::free(h_rs);
+        std::free(h_rev);
+        std::free(h_avg);
+        std::free(h_ids);
+        cudaFreeAsync(davg, stream);
+        set_error("host allocation of the outputs failed");
+        return SS_ERR_NOMEM;
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h_avg, davg, n_avg * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && iterations >= 1)
+        e = cudaMemcpyAsync(h_rs, dsmall, n_rs * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && iterations >= 1)
+        e = cudaMemcpyAsync(h_rev, d_rev, static_cast<size_t>(P.H[tl]) * sizeof(float),
+                            cudaMemcpyDeviceToHost, stream);
+    cudaFreeAsync(davg, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        std::free(h_rs);
+        std::free(h_rev);
+        std::free(h_avg);
+        std::free(h_ids);
+        set_error(std::string("CUDA: ") + cudaGetErrorString(e));
+        return SS_ERR_CUDA;
+    }
+    for (int i = 0; i < P.num_dec; ++i) h_ids[i] = P.dec_nodes[i];
+    out->root_strategy = h_rs;
+    out->root_num_actions = P.root_na;
+    out->root_player = P.root_player;
+    out->root_ev = h_rev;
+    out->avg_strategies = h_avg;
+    out->avg_strategy_node_ids = h_ids;
+    out->num_avg_nodes = P.num_dec;
+    out->num_players = np;
+    out->max_hands = P.max_h;
+    return SS_OK;
+}
+
+int Session::profile(SSKernelProfile *prof) {
+    std::memset(prof, 0, sizeof(*prof));
+    CK(cudaSetDevice(device));
+    std::vector<Mark> ms;
+    marks = &ms;
+    cudaGraphExec_t g = nullptr;
+    cudaError_t e = capture(1, true, &g);
+    marks = nullptr;
+    cudaEvent_t end = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&end);
+    if (e == cudaSuccess) e = cudaGraphLaunch(g, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(end, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) {
+        iterations += 1;
+        prof->num_classes = SS_PROFILE_CLASSES;
+        for (int k = 0; k < SS_PROFILE_CLASSES; ++k)
+            std::strncpy(prof->name[k], kClassName[k], sizeof(prof->name[k]) - 1);
+        for (size_t i = 0; i < ms.size() && e == cudaSuccess; ++i) {
+            float t = 0.f;
+            e = cudaEventElapsedTime(&t, ms[i].ev, i + 1 < ms.size() ? ms[i + 1].ev : end);
+            prof->ms[ms[i].cls] += t;
+            prof->bytes[ms[i].cls] += ms[i].bytes;
+            prof->launches[ms[i].cls] += 1;
+        }
+        float tot = 0.f;
+        if (e == cudaSuccess && !ms.empty()) e = cudaEventElapsedTime(&tot, ms.front().ev, end);
+        prof->iteration_ms = tot;
+    }
+    for (auto &m : ms) cudaEventDestroy(m.ev);
+    if (end) cudaEventDestroy(end);
+    if (g) cudaGraphExecDestroy(g);
+    CK(e);
+    return SS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// entry points used by the ABI layer
+// ---------------------------------------------------------------------------
+
+int session_create(const Problem &pb, const SolveConfig &cfg, Session **out) {
+    *out = nullptr;
+    Session *s = new Session();
+    int rc = s->init(pb, cfg);
+    if (rc != SS_OK) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return SS_OK;
+}
+
+int session_run(Session *s, int iters) { return s->run(iters); }
+
+int session_sync(Session *s) {
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    return SS_OK;
+}
+
+int session_reset(Session *s) { return s->reset(); }
+int session_iterations(const Session *s) { return s->iterations; }
+int session_output(Session *s, SSOutput *out) { return s->output(out); }
+int session_profile(Session *s, SSKernelProfile *p) { return s->profile(p); }
+void session_destroy(Session *s) { delete s; }
+void *session_stream(Session *s) { return static_cast<void *>(s->stream); }
+
+int solve(const Problem &pb, int iterations, const SolveConfig &cfg, SSOutput *out,
+          SSSolveStats *stats) {
+    std::memset(out, 0, sizeof(*out));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->exploitability_pct = -1.0;
+        stats->nashconv = -1.0;
+    }
+    if (iterations < 0) {
+        set_error("max_iterations must be >= 0");
+        return SS_ERR_INVALID;
+    }
+    Session *s = nullptr;
+    int rc = session_create(pb, cfg, &s);
+    if (rc != SS_OK) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float ms = 0.f;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        set_error("cudaEventCreate failed");
+        rc = SS_ERR_CUDA;
+    }
+    if (rc == SS_OK && cudaEventRecord(e0, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+    if (rc == SS_OK) rc = s->run(iterations);
+    if (rc == SS_OK && cudaEventRecord(e1, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+    if (rc == SS_OK) rc = s->output(out);
+    if (rc == SS_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = -1.f;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc == SS_OK && stats) {
+        stats->iterations_run = iterations;
+        stats->solve_ms = ms;
+        stats->node_hand_updates = s->P.node_hands * iterations;
+    }
+    session_destroy(s);
+    return rc;
+}
+
+int exploitability(const Problem &, const float *, double *, double *, double *, double *, double *) {
+    set_error("exploitability: not available in this build yet");
+    return SS_ERR_UNSUPPORTED;
+}
+
+}  // namespace ssb

@@ -1,0 +1,191 @@
+// ss_engine.h -- internal interface of the B200 street solver.
+//
+// The engine never sees SSTreeData (whose layout depends on SS_MAX_HANDS);
+// the ABI layer (ss_abi.cpp, compiled once per SS_MAX_HANDS) turns it into a
+// Problem of plain pointers.  SSNode and SSOutput do not depend on
+// SS_MAX_HANDS and are shared.
+#pragma once
+
+#include "street_solve.h"
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ssb {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+const char *last_error();
+
+// ---------------------------------------------------------------------------
+// tree builder (ss_tree.cpp)
+// ---------------------------------------------------------------------------
+struct BuiltTree {
+    std::vector<SSNode> nodes;
+    std::vector<int> children;
+    std::vector<int> level_order;
+    std::vector<int> node_depth;
+    int max_depth = 0;
+    int num_leaves = 0;
+};
+
+int build_street_tree(const int *board, int num_board, int starting_pot, int effective_stack,
+                      const float *bet_sizes, int num_bet_sizes, int num_players,
+                      const int *acting_order, int is_river, int use_cont_strats, int max_raises,
+                      BuiltTree *out);
+
+// ---------------------------------------------------------------------------
+// problem: one subgame as plain pointers
+// ---------------------------------------------------------------------------
+struct Problem {
+    const SSNode *nodes = nullptr;
+    const int *children = nullptr;
+    int num_nodes = 0;
+    int num_children_total = 0;
+    int num_players = 0;
+    const int *hands[SS_MAX_PLAYERS] = {};     // [num_hands[p]][2]
+    const float *weights[SS_MAX_PLAYERS] = {}; // [num_hands[p]]
+    int num_hands[SS_MAX_PLAYERS] = {};
+    int board[SS_MAX_BOARD] = {};
+    int num_board = 0;
+    const float *leaf_values = nullptr;        // [num_leaves][num_players][max_hands] or null
+    int num_leaves = 0;
+    const int *frozen = nullptr;               // [num_nodes] or null
+    int starting_pot = 0;
+    int is_river = 0;
+};
+
+// ---------------------------------------------------------------------------
+// device work items (16-byte aligned PODs shared by host planner and kernels)
+// ---------------------------------------------------------------------------
+
+// Top-down reach of one player through one of its own decision nodes:
+// reach[first_edge + a] = reach[parent_row] * sigma_a.
+struct alignas(16) ReachItem {
+    int first_edge;
+    int na;
+    int parent_row;
+    int frozen;
+};
+
+// Bottom-up value and regret update at one traverser decision node; the value
+// of edge e is the sum of val[] over frontier(e) = fr_items[fr_off[e] .. fr_off[e+1]).
+struct alignas(16) CfvItem {
+    int first_edge;
+    int na;
+    int frozen;
+    int node;
+};
+
+// Terminal kinds per traverser.
+enum TermKind : int {
+    TK_ZERO = 0,     // value 0 (folded traverser at showdown, leaves without leaf values)
+    TK_LEAF0 = 1,    // leaf with no live opponent: value = leaf value
+    TK_CR1 = 2,      // fold / leaf with one counted opponent: factor * card-removal mass
+    TK_CR2 = 3,      // fold / leaf with two counted opponents
+    TK_SD1 = 4,      // showdown against one live opponent
+    TK_ENUM = 5,     // anything else: exact tuple enumeration (small ranges only)
+    TK_COUNT = 6
+};
+
+// One terminal for one traverser.  factor: payoff for folds; leaf_off >= 0
+// selects leaf_values[leaf_off + h] instead.  Showdowns use pot / bet.
+struct alignas(16) TermItem {
+    int node;
+    int kind_detail;          // TK_ENUM: 0 fold, 1 leaf, 2 showdown
+    int k;                    // number of counted opponents
+    int leaf_off;
+    float payoff;
+    float pot;
+    float bet;
+    int pad;
+    int opp_row[SS_MAX_PLAYERS - 1];
+    int opp_player[SS_MAX_PLAYERS - 1];
+    int pad2[2];
+};
+
+// Showdown tables for one board: every non-board 2-card combo ranked by the
+// 7-card strength.  pos = rank position (ascending strength), tie group of a
+// position = [lo, hi).  card_list[c] = positions of the combos holding card c,
+// ascending; for a combo at position q with cards (c1, c2), cl[q] holds the
+// number of entries of card_list[c1] below lo, below hi, and the same for c2.
+struct alignas(16) SdCombo {
+    int lo, hi;
+    short c1, c2;
+    short l1lo, l1hi, l2lo, l2hi;
+};
+
+// ---------------------------------------------------------------------------
+// plan: the flattened tree and every per-traverser work list
+// ---------------------------------------------------------------------------
+struct Plan {
+    int np = 0, N = 0, E = 0;
+    int max_h = 0;           // max(num_hands): output stride, leaf_values stride
+    int HS = 0;              // device row stride in floats (multiple of 32)
+    int H[SS_MAX_PLAYERS] = {};
+    int root_player = -1, root_na = 0;
+    int num_dec = 0;
+    std::vector<int> dec_nodes;        // decision node ids in index order
+    std::vector<int> first_edge;       // [N], -1 for terminals
+    std::vector<int> edge_node;        // [E]
+    // per player: reach levels (top-down)
+    std::vector<std::vector<ReachItem>> reach_levels[SS_MAX_PLAYERS];
+    // per traverser: cfv levels (bottom-up order)
+    std::vector<std::vector<CfvItem>> cfv_levels[SS_MAX_PLAYERS];
+    std::vector<int> fr_off;           // [E + 1]
+    std::vector<int> fr_items;         // val rows (= node ids)
+    std::vector<int> root_fr[SS_MAX_PLAYERS];
+    // per traverser, per TermKind: terminal items
+    std::vector<TermItem> term[SS_MAX_PLAYERS][TK_COUNT];
+    // hand tables, [np][HS]: c0 | c1 << 8 | board_blocked << 16; -1 padding
+    std::vector<int> hand_code;
+    // showdown tables (river only)
+    int ncomb = 0;
+    std::vector<SdCombo> sd_combo;     // [ncomb]
+    std::vector<short> sd_card_list;   // [52][52]
+    std::vector<int> sd_pos;           // [np][HS], -1 if blocked / padding
+    std::vector<uint32_t> strength;    // [np][HS], 0 if blocked / padding
+    double enum_work = 0;              // tuple visits per iteration on TK_ENUM
+    double node_hands = 0;             // num_nodes x sum_p H_p
+};
+
+int build_plan(const Problem &pb, Plan *plan);
+
+// 7-card rank of board (num_board == 5) plus two hole cards, reference
+// encoding (src/hand_eval.h:26-35, 138-156); 0 if any card repeats.
+uint32_t rank7_host(const int *board5, int c0, int c1);
+
+// ---------------------------------------------------------------------------
+// solve (ss_engine.cu)
+// ---------------------------------------------------------------------------
+struct SolveConfig {
+    int device = 0;
+    int graph_iterations = 10;
+    float target_exploitability = -1.f;
+    int check_every = 50;
+    int compute_exploitability = 0;
+};
+
+int solve(const Problem &pb, int iterations, const SolveConfig &cfg, SSOutput *out,
+          SSSolveStats *stats);
+
+// resident sessions (ss_engine.cu)
+class Session;
+int session_create(const Problem &pb, const SolveConfig &cfg, Session **out);
+int session_run(Session *s, int iterations);
+int session_sync(Session *s);
+int session_reset(Session *s);
+int session_iterations(const Session *s);
+int session_output(Session *s, SSOutput *out);
+int session_profile(Session *s, SSKernelProfile *prof);
+void session_destroy(Session *s);
+void *session_stream(Session *s);
+
+int exploitability(const Problem &pb, const float *avg_strategies, double *expl_pct,
+                   double *nashconv, double *br_value, double *cur_value, double *deal_mass);
+
+}  // namespace ssb

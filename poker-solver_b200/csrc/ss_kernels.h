@@ -1,0 +1,50 @@
+// ss_kernels.h -- device context and kernel launchers of the street solver.
+#pragma once
+
+#include "ss_engine.h"
+
+#include <cuda_runtime.h>
+
+namespace ssb {
+
+// Everything a kernel needs about one solve, passed by value.
+struct DevCtx {
+    float *R;              // regrets            [E][HS]
+    float *S;              // strategy sums      [E][HS]
+    float *reach;          // reach per sequence [E + np][HS]
+    float *val;            // node values        [N][HS]
+    const int *fr_off;     // [E + 1]
+    const int *fr_items;
+    const int *hand_code;  // [np][HS]
+    const int *sd_pos;     // [np][HS]
+    const unsigned *strength;    // [np][HS]
+    const SdCombo *sd_combo;     // [ncomb]
+    const short *sd_card_list;   // [52][52]
+    const float *leaf_values;
+    const int *iter;       // current CFR iteration (device counter)
+    int HS;
+    int np;
+    int ncomb;
+    int H[SS_MAX_PLAYERS];
+};
+
+// threads per block of the per-hand kernels; each thread covers 4 hands
+constexpr int kHandThreads = 64;
+constexpr int kHandsPerBlock = kHandThreads * 4;
+// threads per block of the per-terminal kernels
+constexpr int kTermThreads = 256;
+
+cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s);
+cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s);
+cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
+                         cudaStream_t s);
+cudaError_t launch_bump(int *iter, cudaStream_t s);
+cudaError_t launch_sum_rows(const DevCtx &c, const int *rows, int n, float *out, int H,
+                            cudaStream_t s);
+cudaError_t launch_root_strategy(const DevCtx &c, int first_edge, int na, int frozen, int H,
+                                 float *out, cudaStream_t s);
+cudaError_t launch_avg_strategy(const DevCtx &c, const int *dec_first_edge, const int *dec_na,
+                                const int *dec_player, int num_dec, int max_h, float *out,
+                                cudaStream_t s);
+
+}  // namespace ssb

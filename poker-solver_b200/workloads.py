@@ -1,0 +1,203 @@
+"""Seeded synthetic subgames with the shapes of the benchmark configurations,
+and a direct C-ABI driver (build -> fill -> solve -> read -> free).
+
+The configurations (sizes, bet sizes, raise caps, weight distributions) are
+the ones the reference's benchmark plan quotes; inputs are synthetic and
+seeded, there is no dataset:
+
+  hu_river   2 players, 5-card board, all 1081 combos each, weights U(0,1),
+             pot 100, stack 400, bets {0.5, 1.0} + all-in, 2 raises
+  turn3      3 players, 4-card board, all 1128 combos each, weights U(0,1)
+             with ~30% zeroed, pot 150, stack 500, bets {0.33, 0.75, 1.5}
+             + all-in, 3 raises, continuation leaves with values N(0, 0.3 pot)
+  river6     6 players, 5-card board, 1081 combos each, Dirichlet(0.3)-style
+             sparse weights (40-70% zero), pot 300, stack 1000,
+             bets {0.5, 1.0} + all-in, 2 raises
+"""
+import ctypes
+
+import numpy as np
+
+NODE_INTS = 26  # SSNode is 26 x int32
+
+try:
+    import street_solver_gpu as ssg
+except ImportError:  # imported as part of a package
+    from . import street_solver_gpu as ssg
+
+
+def all_combos(board):
+    deck = [c for c in range(52) if c not in set(board)]
+    return [(a, b) for i, a in enumerate(deck) for b in deck[i + 1:]]
+
+
+def make_ranges(rng, board, num_players, num_hands=None, weights="uniform", zero_frac=0.0):
+    """Per player: hands [H, 2] int32 and weights [H] float32 over non-board
+    combos (all of them when num_hands is None, else a random subset)."""
+    combos = all_combos(board)
+    hands, ws = [], []
+    for _ in range(num_players):
+        if num_hands is None or num_hands >= len(combos):
+            sel = np.arange(len(combos))
+        else:
+            sel = np.sort(rng.choice(len(combos), num_hands, replace=False))
+        h = np.array([combos[i] for i in sel], np.int32)
+        if weights == "dirichlet":
+            w = rng.gamma(0.3, 1.0, len(sel))
+            w = w / w.max()
+            zf = rng.uniform(0.4, 0.7)
+            w[rng.random(len(sel)) < zf] = 0.0
+        else:
+            w = rng.uniform(0.0, 1.0, len(sel))
+            if zero_frac > 0:
+                w[rng.random(len(sel)) < zero_frac] = 0.0
+        hands.append(h)
+        ws.append(w.astype(np.float32))
+    return hands, ws
+
+
+def config(name, seed=0, num_hands=None, **over):
+    """A seeded subgame description: dict with board, pot, stack, bet_sizes,
+    max_raises, num_players, hands, weights and (for non-river) a leaf-value
+    generator."""
+    rng = np.random.default_rng(seed)
+    deck = rng.permutation(52)
+    if name == "hu_river":
+        board = [int(c) for c in deck[:5]]
+        cfg = dict(board=board, pot=100, stack=400, bet_sizes=[0.5, 1.0], max_raises=2,
+                   num_players=2, iterations=1000)
+        hands, ws = make_ranges(rng, board, 2, num_hands)
+    elif name == "turn3":
+        board = [int(c) for c in deck[:4]]
+        cfg = dict(board=board, pot=150, stack=500, bet_sizes=[0.33, 0.75, 1.5], max_raises=3,
+                   num_players=3, iterations=1000, leaf_sigma=0.3 * 150)
+        hands, ws = make_ranges(rng, board, 3, num_hands, zero_frac=0.3)
+    elif name == "river6":
+        board = [int(c) for c in deck[:5]]
+        cfg = dict(board=board, pot=300, stack=1000, bet_sizes=[0.5, 1.0], max_raises=2,
+                   num_players=6, iterations=2000)
+        hands, ws = make_ranges(rng, board, 6, num_hands, weights="dirichlet")
+    else:
+        raise KeyError(name)
+    cfg.update(over)
+    cfg["hands"], cfg["weights"], cfg["seed"], cfg["name"] = hands, ws, seed, name
+    return cfg
+
+
+def padded(cfg):
+    """hands [np, max_h, 2], weights [np, max_h], num_hands [np]."""
+    np_ = cfg["num_players"]
+    nh = np.array([len(h) for h in cfg["hands"]], np.int32)
+    mh = int(nh.max())
+    H = np.zeros((np_, mh, 2), np.int32)
+    W = np.zeros((np_, mh), np.float32)
+    for p in range(np_):
+        H[p, :nh[p]] = cfg["hands"][p]
+        W[p, :nh[p]] = cfg["weights"][p]
+    return H, W, nh
+
+
+def leaf_values_for(cfg, num_leaves, seed_offset=1000):
+    if num_leaves == 0:
+        return None
+    rng = np.random.default_rng(cfg["seed"] + seed_offset)
+    mh = max(len(h) for h in cfg["hands"])
+    return rng.normal(0.0, cfg.get("leaf_sigma", 30.0),
+                      (num_leaves, cfg["num_players"], mh)).astype(np.float32)
+
+
+class AbiSubgame:
+    """One subgame driven through the C ABI of libstreet_solve(_wide).so."""
+
+    def __init__(self, cfg, max_hands=None, acting_order=None, use_cont_strats=True):
+        need = max(len(h) for h in cfg["hands"])
+        self.max_hands_cap = max_hands or (ssg.SS_MAX_HANDS if need <= ssg.SS_MAX_HANDS
+                                           else ssg.SS_MAX_HANDS_WIDE)
+        self.lib = ssg.load_library(self.max_hands_cap)
+        self.cfg = cfg
+        np_ = cfg["num_players"]
+        order = list(range(np_)) if acting_order is None else acting_order
+        board = cfg["board"]
+        self.td = ssg.tree_struct(self.max_hands_cap)()
+        b = (ctypes.c_int * len(board))(*board)
+        s = (ctypes.c_float * len(cfg["bet_sizes"]))(*cfg["bet_sizes"])
+        o = (ctypes.c_int * np_)(*order)
+        rc = self.lib.ss_build_tree_ex(b, len(board), cfg["pot"], cfg["stack"], s, len(cfg["bet_sizes"]),
+                                       np_, o, int(len(board) == 5),
+                                       int(use_cont_strats and len(board) < 5), cfg["max_raises"],
+                                       ctypes.byref(self.td))
+        if rc != 0:
+            raise RuntimeError(f"ss_build_tree_ex failed ({rc}): {ssg.last_error(self.lib)}")
+        self.H, self.W, self.nh = padded(cfg)
+        for p in range(np_):
+            self.td.num_hands[p] = int(self.nh[p])
+            arr_h = np.ctypeslib.as_array(self.td.hands[p])
+            arr_h[:self.nh[p]] = self.H[p, :self.nh[p]]
+            arr_w = np.ctypeslib.as_array(self.td.weights[p])
+            arr_w[:self.nh[p]] = self.W[p, :self.nh[p]]
+        self.leaf_values = None
+        self.frozen = None
+
+    @property
+    def num_leaves(self):
+        return self.td.num_leaves
+
+    def set_leaf_values(self, lv):
+        self.leaf_values = None if lv is None else np.ascontiguousarray(lv, np.float32)
+        self.td.leaf_values = (None if lv is None else
+                               self.leaf_values.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+
+    def set_frozen(self, frozen):
+        self.frozen = None if frozen is None else np.ascontiguousarray(frozen, np.int32)
+        self.td.frozen_action = (None if frozen is None else
+                                 self.frozen.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
+    def tree_arrays(self):
+        n = self.td.num_nodes
+        nodes = np.ctypeslib.as_array(ctypes.cast(self.td.nodes, ctypes.POINTER(ctypes.c_int)),
+                                      shape=(n * NODE_INTS,)).reshape(n, NODE_INTS).copy()
+        ch = np.ctypeslib.as_array(self.td.children, shape=(max(self.td.num_children_total, 1),))[
+            :self.td.num_children_total].copy()
+        lo = np.ctypeslib.as_array(self.td.level_order, shape=(n,)).copy()
+        nd = np.ctypeslib.as_array(self.td.node_depth, shape=(n,)).copy()
+        return nodes, ch, lo, nd
+
+    def solve(self, iterations, graph_iterations=10, device=0, target=None):
+        out = ssg.SSOutput()
+        stats = ssg.SSSolveStats()
+        opts = ssg.SSSolveOptions(device, graph_iterations, -1.0 if target is None else target, 50, 0)
+        rc = self.lib.ss_solve_gpu_ex(ctypes.byref(self.td), iterations, ctypes.byref(opts),
+                                      ctypes.byref(out), ctypes.byref(stats))
+        if rc != 0:
+            return rc, None
+        res = read_output(out, self.nh)
+        res["stats"] = {k: getattr(stats, k) for k, _ in ssg.SSSolveStats._fields_}
+        self.lib.ss_free_output(ctypes.byref(out))
+        return 0, res
+
+    def free(self):
+        self.td.leaf_values = None
+        self.td.frozen_action = None
+        self.lib.ss_free_tree(ctypes.byref(self.td))
+
+    def __del__(self):
+        try:
+            if self.td.nodes:
+                self.free()
+        except Exception:
+            pass
+
+
+def read_output(out, num_hands):
+    mh, na, rp, nd = out.max_hands, out.root_num_actions, out.root_player, out.num_avg_nodes
+    nh_root = int(num_hands[rp])
+    return {
+        "root_strategy": np.ctypeslib.as_array(out.root_strategy, shape=(na * nh_root,)).copy()
+        .reshape(na, nh_root),
+        "root_ev": np.ctypeslib.as_array(out.root_ev, shape=(out.num_players_out * mh,)).copy()[:mh],
+        "avg_strategies": np.ctypeslib.as_array(out.avg_strategies, shape=(nd * ssg.SS_MAX_ACTIONS * mh,))
+        .copy().reshape(nd, ssg.SS_MAX_ACTIONS, mh),
+        "avg_node_ids": np.ctypeslib.as_array(out.avg_strategy_node_ids, shape=(nd,)).copy(),
+        "root_player": rp,
+        "root_num_actions": na,
+    }
