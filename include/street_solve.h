@@ -263,6 +263,15 @@ void *ss_session_stream(SSSession *session);
 /* EXTENSION: release the session. */
 void ss_session_destroy(SSSession *session);
 
+/* EXTENSION: 7-card strengths of n hands (cards7 [n][7], cards 0..51) with
+ * the device ranker, in the reference encoding (src/hand_eval.h:26-35). */
+int ss_rank7_batch(const int *cards7, int n, unsigned int *strength_out);
+
+/* EXTENSION: rank every 7-card set on the device; *checksum = sum over sets of
+ * mix64(52-bit card mask) * strength (mod 2^64), category_counts[0..9] = sets
+ * per category (may be NULL).  mix64 is the splitmix64 finaliser. */
+int ss_rank7_checksum(unsigned long long *checksum, unsigned long long *category_counts);
+
 /* EXTENSION: message for the last failure on the calling thread ("" if none). */
 const char *ss_last_error(void);
 

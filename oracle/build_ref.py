@@ -49,7 +49,7 @@ def build_handeval():
     hdr = os.path.join(REF, "src", "hand_eval.h")
     if _fresh(out, [src, hdr]):
         return out
-    _run(["gcc", "-O2", "-fPIC", "-shared", "-I", os.path.join(REF, "src"), src, "-o", out])
+    _run(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-I", os.path.join(REF, "src"), src, "-o", out])
     return out
 
 

@@ -64,6 +64,8 @@ int orc_build_tree(const int *board, int num_board, int starting_pot, int effect
 void orc_free_tree(OrcTree *t);
 
 uint32_t orc_eval7_cards(const int *cards7);
+uint64_t orc_eval7_checksum(uint64_t *category_counts10);
+void orc_eval7_many(const int *cards7, long n, uint32_t *out);
 
 /* Solve with the reference semantics.  hands: [np][max_h][2], weights:
  * [np][max_h], num_hands: [np]; max_h = max(num_hands).  leaf_values:

@@ -294,6 +294,15 @@ void ss_session_destroy(SSSession *s) {
     delete s;
 }
 
+int ss_rank7_batch(const int *cards7, int n, unsigned int *strength_out) {
+    return ssb::rank7_batch(cards7, n, strength_out);
+}
+
+int ss_rank7_checksum(unsigned long long *checksum, unsigned long long *category_counts) {
+    if (!checksum) return SS_ERR_INVALID;
+    return ssb::rank7_checksum(checksum, category_counts);
+}
+
 const char *ss_last_error(void) { return ssb::last_error(); }
 
 }  // extern "C"

@@ -148,7 +148,8 @@ class Session {
         cudaError_t e = cudaEventCreate(&m.ev);
         if (e != cudaSuccess) return e;
         marks->push_back(m);
-        return cudaEventRecord(m.ev, stream);
+        // an external record becomes an event-record node of the captured graph
+        return cudaEventRecordWithFlags(m.ev, stream, cudaEventRecordExternal);
     }
 
     cudaError_t reach(int p) {

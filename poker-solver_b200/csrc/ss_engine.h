@@ -158,6 +158,8 @@ int build_plan(const Problem &pb, Plan *plan);
 // 7-card rank of board (num_board == 5) plus two hole cards, reference
 // encoding (src/hand_eval.h:26-35, 138-156); 0 if any card repeats.
 uint32_t rank7_host(const int *board5, int c0, int c1);
+int rank7_batch(const int *cards7, int n, unsigned *out);
+int rank7_checksum(unsigned long long *checksum, unsigned long long *hist10);
 
 // ---------------------------------------------------------------------------
 // solve (ss_engine.cu)

@@ -167,11 +167,15 @@ def test_uneven_ranges(oracle):
 
 @pytest.mark.gpu
 def test_full_size_hu_river(oracle):
-    # the heads-up river benchmark shape at full size (1081 combos each)
+    """The heads-up river benchmark shape at full size (1081 combos each).
+    Here the reference's own float sums over 1081 opponent hands are ~2e-4
+    away from exact arithmetic, so the 1e-4 bound is asserted against the
+    FP64 restatement, and the envelope against the FP32 one."""
     cfg = wl.config("hu_river", seed=0)
     ours, lv = solve(cfg, 3)
     r32, r64 = oracle_pair(oracle, cfg, 3, lv)
-    strict(ours, r32)
+    strict(ours, r64)
+    envelope(ours, r32, r64)
     # the closed form sits closer to exact arithmetic than the reference's floats
     assert diffs(ours, r64)[0] <= diffs(r32, r64)[0] + 1e-6
 
