@@ -311,6 +311,7 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
 
+    tree_info = {"nodes": nnodes, "decision": ndec, "leaves": sg.num_leaves, "hands": nh}
     lib.ss_session_destroy(sess)
     sg.free()
     return {
@@ -327,7 +328,7 @@ def run_ours(args, world, rank, local):
                         "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
                     for k, v in classes.items() if v["launches"]},
         "iteration_ms": prof.iteration_ms,
-        "tree": {"nodes": nnodes, "decision": ndec, "leaves": sg.num_leaves, "hands": nh},
+        "tree": tree_info,
     }
 
 
