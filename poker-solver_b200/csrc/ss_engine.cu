@@ -293,6 +293,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     const size_t o_str = b.add(P.strength);
     const size_t o_sdc = b.add(P.sd_combo);
     const size_t o_sdl = b.add(P.sd_card_list);
+    const size_t o_sdp = b.add(P.sd_card_partner);
     std::vector<int> dfe, dna, dpl;
     for (int x : P.dec_nodes) {
         dfe.push_back(P.first_edge[x]);
@@ -348,12 +349,16 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.strength = reinterpret_cast<const unsigned *>(dbase + o_str);
     c.sd_combo = reinterpret_cast<const SdCombo *>(dbase + o_sdc);
     c.sd_card_list = reinterpret_cast<const short *>(dbase + o_sdl);
+    c.sd_card_partner = reinterpret_cast<const short *>(dbase + o_sdp);
     c.leaf_values = dleaf;
     c.iter = diter;
     c.HS = P.HS;
     c.np = np;
     c.ncomb = P.ncomb;
-    for (int p = 0; p < SS_MAX_PLAYERS; ++p) c.H[p] = p < np ? P.H[p] : 0;
+    for (int p = 0; p < SS_MAX_PLAYERS; ++p) {
+        c.H[p] = p < np ? P.H[p] : 0;
+        c.dup[p] = p < np ? P.dup[p] : 0;
+    }
     frozen_root = pb.frozen ? pb.frozen[0] : -1;
     return reset();
 }

@@ -146,9 +146,11 @@ struct Plan {
     // showdown tables (river only)
     int ncomb = 0;
     std::vector<SdCombo> sd_combo;     // [ncomb]
-    std::vector<short> sd_card_list;   // [52][52]
+    std::vector<short> sd_card_list;   // [52][52] rank positions of the combos holding each card
+    std::vector<short> sd_card_partner;// [52][52] the other card of each of those combos
     std::vector<int> sd_pos;           // [np][HS], -1 if blocked / padding
     std::vector<uint32_t> strength;    // [np][HS], 0 if blocked / padding
+    int dup[SS_MAX_PLAYERS] = {};      // range holds some combo more than once
     double enum_work = 0;              // tuple visits per iteration on TK_ENUM
     double node_hands = 0;             // num_nodes x sum_p H_p
 };

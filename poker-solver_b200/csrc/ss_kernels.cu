@@ -18,7 +18,7 @@ namespace ssb {
 
 namespace {
 
-constexpr int MS = 56;  // shared-memory row stride of a 52x52 combo matrix
+constexpr int MS = 52;  // shared-memory row stride of a 52x52 combo matrix (16-byte rows)
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
@@ -101,36 +101,72 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c, const ReachIte
 // --------------------------------------------------------------------------
 // cfv: value, regret and strategy-sum update at traverser nodes
 // (street_solve.cu:1155-1175): v = sum_a sigma_a ev_a; r_a = (r_a + (ev_a - v))
-// * t/(t+1); s_a += t * sigma_a; ev_a = sum of val over frontier(edge a)
+// * t/(t+1); s_a += t * sigma_a; ev_a = sum of val over frontier(edge a).
+// Each thread owns 2 hands.  Edge values are gathered first (four frontier
+// rows in flight at a time), then the regrets are loaded and matched, which
+// keeps the live state to the edge values and regrets.
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(kHandThreads) k_cfv(DevCtx c, const CfvItem *__restrict__ items,
-                                                      int nchunk, int H) {
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+
+__global__ void __launch_bounds__(kCfvThreads) k_cfv(DevCtx c, const CfvItem *__restrict__ items,
+                                                     int nchunk, int H) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
-    const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
+    const int h0 = (ch * kCfvThreads + threadIdx.x) * 2;
     if (h0 >= H) return;
     const CfvItem I = items[it];
     const size_t HS = static_cast<size_t>(c.HS);
-    float r[SS_MAX_ACTIONS][4], sig[SS_MAX_ACTIONS][4], ev[SS_MAX_ACTIONS][4];
-    regret_match4(c.R, HS, I.first_edge, I.na, I.frozen, h0, r, sig);
-    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    const float *val = c.val + h0;
+    float2 ev[SS_MAX_ACTIONS];
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
-            float e[4] = {0.f, 0.f, 0.f, 0.f};
-            const int k0 = c.fr_off[I.first_edge + a], k1 = c.fr_off[I.first_edge + a + 1];
-            for (int k = k0; k < k1; ++k) {
-                const float4 x = ld4(c.val + static_cast<size_t>(c.fr_items[k]) * HS + h0);
-                e[0] += x.x;
-                e[1] += x.y;
-                e[2] += x.z;
-                e[3] += x.w;
+            float2 e = make_float2(0.f, 0.f);
+            int k = c.fr_off[I.first_edge + a];
+            const int k1 = c.fr_off[I.first_edge + a + 1];
+            for (; k + 4 <= k1; k += 4) {
+                const int n0 = c.fr_items[k], n1 = c.fr_items[k + 1];
+                const int n2 = c.fr_items[k + 2], n3 = c.fr_items[k + 3];
+                const float2 x0 = ld2(val + static_cast<size_t>(n0) * HS);
+                const float2 x1 = ld2(val + static_cast<size_t>(n1) * HS);
+                const float2 x2 = ld2(val + static_cast<size_t>(n2) * HS);
+                const float2 x3 = ld2(val + static_cast<size_t>(n3) * HS);
+                e.x += x0.x; e.y += x0.y;
+                e.x += x1.x; e.y += x1.y;
+                e.x += x2.x; e.y += x2.y;
+                e.x += x3.x; e.y += x3.y;
             }
+            for (; k < k1; ++k) {
+                const float2 x = ld2(val + static_cast<size_t>(c.fr_items[k]) * HS);
+                e.x += x.x; e.y += x.y;
+            }
+            ev[a] = e;
+        }
+    }
+    float2 r[SS_MAX_ACTIONS];
+    float s0 = 0.f, s1 = 0.f;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                ev[a][i] = e[i];
-                v[i] += sig[a][i] * e[i];
-            }
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+        if (a < I.na) {
+            r[a] = ld2(c.R + static_cast<size_t>(I.first_edge + a) * HS + h0);
+            s0 += r[a].x > 0.f ? r[a].x : 0.f;
+            s1 += r[a].y > 0.f ? r[a].y : 0.f;
+        }
+    }
+    const float uni = 1.0f / static_cast<float>(I.na);
+    const float inv0 = s0 > 0.f ? 1.0f / s0 : 0.f, inv1 = s1 > 0.f ? 1.0f / s1 : 0.f;
+    // strategy of action a (regret matching, A3 freeze)
+    auto sigma = [&](int a, float ra, float sum, float inv) {
+        if (I.frozen >= 0) return a == I.frozen ? 1.0f : 0.0f;
+        return sum > 0.f ? (ra > 0.f ? ra : 0.f) * inv : uni;
+    };
+    float v0 = 0.f, v1 = 0.f;
+#pragma unroll
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+        if (a < I.na) {
+            v0 += sigma(a, r[a].x, s0, inv0) * ev[a].x;
+            v1 += sigma(a, r[a].y, s1, inv1) * ev[a].y;
         }
     }
     const int t = *c.iter;
@@ -140,21 +176,17 @@ __global__ void __launch_bounds__(kHandThreads) k_cfv(DevCtx c, const CfvItem *_
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
             const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
-            float4 nr, ns;
-            const float4 s = ld4(c.S + off);
-            nr.x = (r[a][0] + (ev[a][0] - v[0])) * d;
-            nr.y = (r[a][1] + (ev[a][1] - v[1])) * d;
-            nr.z = (r[a][2] + (ev[a][2] - v[2])) * d;
-            nr.w = (r[a][3] + (ev[a][3] - v[3])) * d;
-            ns.x = s.x + w * sig[a][0];
-            ns.y = s.y + w * sig[a][1];
-            ns.z = s.z + w * sig[a][2];
-            ns.w = s.w + w * sig[a][3];
-            st4(c.R + off, nr);
-            st4(c.S + off, ns);
+            const float2 sm = ld2(c.S + off);
+            float2 nr, ns;
+            nr.x = (r[a].x + (ev[a].x - v0)) * d;
+            nr.y = (r[a].y + (ev[a].y - v1)) * d;
+            ns.x = sm.x + w * sigma(a, r[a].x, s0, inv0);
+            ns.y = sm.y + w * sigma(a, r[a].y, s1, inv1);
+            st2(c.R + off, nr);
+            st2(c.S + off, ns);
         }
     }
-    st4(c.val + static_cast<size_t>(I.node) * HS + h0, make_float4(v[0], v[1], v[2], v[3]));
+    st2(c.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0, v1));
 }
 
 // --------------------------------------------------------------------------
@@ -182,35 +214,57 @@ __global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c, const Term
     st4(c.val + static_cast<size_t>(I.node) * c.HS + h0, make_float4(o[0], o[1], o[2], o[3]));
 }
 
-// Scatter one opponent's reach at a terminal into a 52x52 combo matrix, and
-// mark the combos holding positive reach in per-card 64-bit masks (bit b of
-// B[a] = combo {a, b}).  The masks give the exact number of compatible
-// positive-reach opponent tuples through the same inclusion-exclusion as the
-// float sums, with popcounts; where that number is 0 the value is exactly 0,
-// as the reference's enumeration returns (it only adds positive products,
-// street_solve.cu:810-812).  Without it the float formula would leave rounding
-// residue there, and regret matching turns a residue into a pure strategy
-// where the reference plays uniformly.
-__device__ __forceinline__ void scatter_combo(const DevCtx &c, int opp, int row, float *M,
-                                              unsigned long long *B) {
+// Scatter one opponent's reach at a terminal into a 52x52 combo matrix
+// (row stride MS): M[a][b] = M[b][a] = reach of the opponent's hand {a, b}.
+// Board-blocked hands never count (street_solve.cu:755-757).  A range that
+// holds some combo twice accumulates atomically; otherwise each cell has one
+// writer and plain stores suffice.
+__device__ __forceinline__ void scatter_combo(const DevCtx &c, int opp, int row, float *M) {
     const float *r = c.reach + static_cast<size_t>(row) * c.HS;
     const int *code = c.hand_code + static_cast<size_t>(opp) * c.HS;
     const int Ho = c.H[opp];
+    const bool dup = c.dup[opp] != 0;
     for (int j = threadIdx.x; j < Ho; j += blockDim.x) {
         const int hc = code[j];
-        if (hc & 0x10000) continue;  // board-blocked hands never count (street_solve.cu:755-757)
+        if (hc & 0x10000) continue;
         const int a = hc & 0xff, b = (hc >> 8) & 0xff;
         const float x = r[j];
-        atomicAdd(&M[a * MS + b], x);
-        atomicAdd(&M[b * MS + a], x);
-        if (x > 0.f) {
-            atomicOr(&B[a], 1ull << b);
-            atomicOr(&B[b], 1ull << a);
+        if (dup) {
+            atomicAdd(&M[a * MS + b], x);
+            atomicAdd(&M[b * MS + a], x);
+        } else {
+            M[a * MS + b] = x;
+            M[b * MS + a] = x;
         }
     }
 }
 
 __device__ __forceinline__ int bit(unsigned long long m, int b) { return static_cast<int>((m >> b) & 1ull); }
+
+__device__ __forceinline__ void zero_matrix(float *M) {
+    float4 *m4 = reinterpret_cast<float4 *>(M);
+    for (int i = threadIdx.x; i < 52 * MS / 4; i += blockDim.x) m4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Row pass over a combo matrix, one warp per card row r: the row sum u(r) in
+// FP64 and the 64-bit mask of the row's positive cells.  The masks give the
+// exact number of compatible positive-reach opponent tuples through the same
+// inclusion-exclusion as the float sums; where that number is 0 the value is
+// exactly 0, as in the reference, which only adds positive products
+// (street_solve.cu:810-812).  Without it rounding residue of the closed form
+// would turn into a pure strategy under regret matching where the reference
+// plays uniformly.
+__device__ __forceinline__ void row_stats(const float *M, int r, int lane, double *sum_out,
+                                          unsigned long long *mask_out, float *x0, float *x1) {
+    const float a = M[r * MS + lane];
+    const float b = lane + 32 < 52 ? M[r * MS + lane + 32] : 0.f;
+    const unsigned lo = __ballot_sync(0xffffffffu, a > 0.f);
+    const unsigned hi = __ballot_sync(0xffffffffu, b > 0.f);
+    *sum_out = warp_sum(static_cast<double>(a) + static_cast<double>(b));
+    *mask_out = static_cast<unsigned long long>(lo) | (static_cast<unsigned long long>(hi) << 32);
+    *x0 = a;
+    *x1 = b;
+}
 
 // One counted opponent: mass(h) = F - u(c1) - u(c2) + f(h), F the opponent's
 // total reach, u(c) its reach on hands holding card c, f(h) its reach on the
@@ -218,29 +272,32 @@ __device__ __forceinline__ int bit(unsigned long long m, int b) { return static_
 // leaves: leaf value * mass (:1047-1066).
 __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermItem *__restrict__ items,
                                                            int trav) {
-    __shared__ float M[52 * MS];
-    __shared__ unsigned long long B[52];
+    __shared__ __align__(16) float M[52 * MS];
     __shared__ double u[52];
+    __shared__ unsigned long long B[52];
     __shared__ double F;
     __shared__ int npos;
     const TermItem I = items[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < 52 * MS; i += blockDim.x) M[i] = 0.f;
-    if (tid < 52) B[tid] = 0ull;
+    zero_matrix(M);
     __syncthreads();
-    scatter_combo(c, I.opp_player[0], I.opp_row[0], M, B);
+    scatter_combo(c, I.opp_player[0], I.opp_row[0], M);
     __syncthreads();
     for (int r = warp; r < 52; r += blockDim.x / 32) {
-        double s = static_cast<double>(M[r * MS + lane]) +
-                   (lane + 32 < 52 ? static_cast<double>(M[r * MS + lane + 32]) : 0.0);
-        s = warp_sum(s);
-        if (lane == 0) u[r] = s;
+        double s;
+        unsigned long long m;
+        float x0, x1;
+        row_stats(M, r, lane, &s, &m, &x0, &x1);
+        if (lane == 0) {
+            u[r] = s;
+            B[r] = m;
+        }
     }
     __syncthreads();
     if (warp == 0) {
         double s = u[lane] + (lane + 32 < 52 ? u[lane + 32] : 0.0);
-        s = warp_sum(s);
         int n = __popcll(B[lane]) + (lane + 32 < 52 ? __popcll(B[lane + 32]) : 0);
+        s = warp_sum(s);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
         if (lane == 0) {
@@ -257,7 +314,8 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermI
         if (h < Ht) {
             const int hc = tc[h];
             const int a = hc & 0xff, b = (hc >> 8) & 0xff;
-            const int live = npos - __popcll(B[a]) - __popcll(B[b]) + bit(B[a], b);
+            const unsigned long long Ba = B[a], Bb = B[b];
+            const int live = npos - __popcll(Ba) - __popcll(Bb) + bit(Ba, b);
             if (live > 0) {
                 const double z = F - u[a] - u[b] + static_cast<double>(M[a * MS + b]);
                 v = static_cast<float>(static_cast<double>(term_factor(c, I, h)) * z);
@@ -267,58 +325,60 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermI
     }
 }
 
+// Per-card aggregates of the two-opponent closed form, packed so a hand
+// needs two 16-byte shared loads per card.
+struct alignas(16) CardAgg {
+    double u1, u2;      // per-card reach sums of opponents 1 and 2
+    double w, d;        // (M2 u1 + M1 u2)(c), sum_b M1[c][b] M2[c][b]
+};
+struct alignas(16) CardCnt {
+    int u1, u2, w, d;   // the same on the 0/1 positive-reach matrices
+};
+
 // Two counted opponents (1, 2) with combo matrices M1, M2, per-card sums
-// u_i = M_i 1, d(c) = sum_b M1[c][b] M2[c][b], w12 = M2 u1, w21 = M1 u2,
+// u_i = M_i 1, d(c) = sum_b M1[c][b] M2[c][b], w = M2 u1 + M1 u2,
 // P = M1 M2, F_i = sum u_i / 2, Q = sum u1 u2, D = sum d / 2.  For a traverser
 // hand (a, b), m_i = M_i[a][b], A_i = F_i - u_i(a) - u_i(b) + m_i, the mass of
 // opponent pairs disjoint from each other and from (a, b) is
-//   A1 A2 - Q + u1(a)u2(a) + u1(b)u2(b) + w12(a) + w12(b) + w21(a) + w21(b)
+//   A1 A2 - Q + u1(a)u2(a) + u1(b)u2(b) + w(a) + w(b)
 //   - m2 (u1(a) + u1(b)) - m1 (u2(a) + u2(b)) - 2 (d(a) + d(b)) + 3 m1 m2
 //   - P[a][b] - P[b][a] + D
 // (inclusion-exclusion over shared cards), equal to the reference odometer
 // sum of street_solve.cu:771-823 / :1079-1127 for two opponents.
-__global__ void __launch_bounds__(kTermThreads) k_term_cr2(DevCtx c, const TermItem *__restrict__ items,
+__global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const TermItem *__restrict__ items,
                                                            int trav) {
     __shared__ __align__(16) float M1[52 * MS];
     __shared__ __align__(16) float M2[52 * MS];
     __shared__ __align__(16) float P[52 * MS];
-    __shared__ double u1[52], u2[52], dd[52], w12[52], w21[52];
+    __shared__ CardAgg agg[52];
+    __shared__ CardCnt cnt[52];
+    __shared__ ulonglong2 Bm[52];   // positive-reach masks of M1 (x) and M2 (y)
     __shared__ double F1, F2, Q, D;
-    // exact counts of positive-reach combos, same formula on 0/1 matrices
-    __shared__ unsigned long long B1[52], B2[52];
-    __shared__ int iu1[52], iu2[52], idd[52], iw12[52], iw21[52];
     __shared__ long long IF1, IF2, IQ, ID;
     const TermItem I = items[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwarp = blockDim.x / 32;
-    for (int i = tid; i < 52 * MS; i += blockDim.x) {
-        M1[i] = 0.f;
-        M2[i] = 0.f;
-    }
-    if (tid < 52) {
-        B1[tid] = 0ull;
-        B2[tid] = 0ull;
-    }
+    zero_matrix(M1);
+    zero_matrix(M2);
     __syncthreads();
-    scatter_combo(c, I.opp_player[0], I.opp_row[0], M1, B1);
-    scatter_combo(c, I.opp_player[1], I.opp_row[1], M2, B2);
+    scatter_combo(c, I.opp_player[0], I.opp_row[0], M1);
+    scatter_combo(c, I.opp_player[1], I.opp_row[1], M2);
     __syncthreads();
-    if (tid < 52) {
-        iu1[tid] = __popcll(B1[tid]);
-        iu2[tid] = __popcll(B2[tid]);
-        idd[tid] = __popcll(B1[tid] & B2[tid]);
-    }
     for (int r = warp; r < 52; r += nwarp) {
-        const double x1 = M1[r * MS + lane], x2 = M2[r * MS + lane];
-        const double y1 = lane + 32 < 52 ? M1[r * MS + lane + 32] : 0.0;
-        const double y2 = lane + 32 < 52 ? M2[r * MS + lane + 32] : 0.0;
-        const double s1 = warp_sum(x1 + y1);
-        const double s2 = warp_sum(x2 + y2);
-        const double sd = warp_sum(x1 * x2 + y1 * y2);
+        double s1, s2;
+        unsigned long long b1, b2;
+        float a0, a1, e0, e1;
+        row_stats(M1, r, lane, &s1, &b1, &a0, &a1);
+        row_stats(M2, r, lane, &s2, &b2, &e0, &e1);
+        const double sd = warp_sum(static_cast<double>(a0) * e0 + static_cast<double>(a1) * e1);
         if (lane == 0) {
-            u1[r] = s1;
-            u2[r] = s2;
-            dd[r] = sd;
+            agg[r].u1 = s1;
+            agg[r].u2 = s2;
+            agg[r].d = sd;
+            Bm[r] = make_ulonglong2(b1, b2);
+            cnt[r].u1 = __popcll(b1);
+            cnt[r].u2 = __popcll(b2);
+            cnt[r].d = __popcll(b1 & b2);
         }
     }
     __syncthreads();
@@ -339,42 +399,37 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr2(DevCtx c, const TermI
         for (int i = 0; i < 4; ++i)
             *reinterpret_cast<float4 *>(&P[(i0 + i) * MS + j0]) =
                 make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-    } else {
-        for (int q = tid - 169; q < 104; q += blockDim.x - 169) {
-            const int col = q % 52;
-            double s = 0.0;
-            int n = 0;
-            if (q < 52) {
-                for (int b = 0; b < 52; ++b) {
-                    s += u1[b] * static_cast<double>(M2[b * MS + col]);
-                    n += bit(B2[b], col) * __popcll(B1[b]);
-                }
-                w12[col] = s;
-                iw12[col] = n;
-            } else {
-                for (int b = 0; b < 52; ++b) {
-                    s += u2[b] * static_cast<double>(M1[b * MS + col]);
-                    n += bit(B1[b], col) * __popcll(B2[b]);
-                }
-                w21[col] = s;
-                iw21[col] = n;
-            }
+    } else if (tid < 169 + 52) {
+        const int col = tid - 169;
+        double s = 0.0;
+        int n = 0;
+        for (int b = 0; b < 52; ++b) {
+            const CardAgg g = agg[b];
+            s += g.u1 * static_cast<double>(M2[b * MS + col]) + g.u2 * static_cast<double>(M1[b * MS + col]);
+            const ulonglong2 m = Bm[b];
+            n += bit(m.y, col) * cnt[b].u1 + bit(m.x, col) * cnt[b].u2;
         }
-    }
-    if (warp == 0) {
-        const double a1 = u1[lane] + (lane + 32 < 52 ? u1[lane + 32] : 0.0);
-        const double a2 = u2[lane] + (lane + 32 < 52 ? u2[lane + 32] : 0.0);
-        const double q = u1[lane] * u2[lane] + (lane + 32 < 52 ? u1[lane + 32] * u2[lane + 32] : 0.0);
-        const double e = dd[lane] + (lane + 32 < 52 ? dd[lane + 32] : 0.0);
-        const double s1 = warp_sum(a1), s2 = warp_sum(a2), sq = warp_sum(q), se = warp_sum(e);
+        agg[col].w = s;
+        cnt[col].w = n;
+    } else if (warp == nwarp - 1) {
+        double a1 = 0, a2 = 0, q = 0, e = 0;
         long long n1 = 0, n2 = 0, nq = 0, nd = 0;
         for (int k = lane; k < 52; k += 32) {
-            const int x1 = __popcll(B1[k]), x2 = __popcll(B2[k]);
-            n1 += x1;
-            n2 += x2;
-            nq += static_cast<long long>(x1) * x2;
-            nd += __popcll(B1[k] & B2[k]);
+            const CardAgg g = agg[k];
+            a1 += g.u1;
+            a2 += g.u2;
+            q += g.u1 * g.u2;
+            e += g.d;
+            const CardCnt m = cnt[k];
+            n1 += m.u1;
+            n2 += m.u2;
+            nq += static_cast<long long>(m.u1) * m.u2;
+            nd += m.d;
         }
+        a1 = warp_sum(a1);
+        a2 = warp_sum(a2);
+        q = warp_sum(q);
+        e = warp_sum(e);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             n1 += __shfl_xor_sync(0xffffffffu, n1, o);
@@ -383,10 +438,10 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr2(DevCtx c, const TermI
             nd += __shfl_xor_sync(0xffffffffu, nd, o);
         }
         if (lane == 0) {
-            F1 = 0.5 * s1;
-            F2 = 0.5 * s2;
-            Q = sq;
-            D = 0.5 * se;
+            F1 = 0.5 * a1;
+            F2 = 0.5 * a2;
+            Q = q;
+            D = 0.5 * e;
             IF1 = n1 / 2;
             IF2 = n2 / 2;
             IQ = nq;
@@ -402,26 +457,25 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr2(DevCtx c, const TermI
         if (h < Ht) {
             const int hc = tc[h];
             const int a = hc & 0xff, b = (hc >> 8) & 0xff;
-            const long long j1 = bit(B1[a], b), j2 = bit(B2[a], b);
-            const long long ja1 = iu1[a], jb1 = iu1[b], ja2 = iu2[a], jb2 = iu2[b];
-            const long long JA1 = IF1 - ja1 - jb1 + j1, JA2 = IF2 - ja2 - jb2 + j2;
-            const long long live = JA1 * JA2 - IQ + ja1 * ja2 + jb1 * jb2 +
-                                   (iw12[a] + iw12[b] + iw21[a] + iw21[b]) - j2 * (ja1 + jb1) -
-                                   j1 * (ja2 + jb2) - 2 * (idd[a] + idd[b]) + 3 * j1 * j2 -
-                                   (__popcll(B1[a] & B2[b]) + __popcll(B1[b] & B2[a])) + ID;
-            if (live <= 0) {
-                out[h] = 0.f;
-                continue;
+            const ulonglong2 Ba = Bm[a], Bb = Bm[b];
+            const CardCnt na = cnt[a], nb = cnt[b];
+            const long long j1 = bit(Ba.x, b), j2 = bit(Ba.y, b);
+            const long long JA1 = IF1 - na.u1 - nb.u1 + j1, JA2 = IF2 - na.u2 - nb.u2 + j2;
+            const long long live = JA1 * JA2 - IQ + static_cast<long long>(na.u1) * na.u2 +
+                                   static_cast<long long>(nb.u1) * nb.u2 + na.w + nb.w -
+                                   j2 * (na.u1 + nb.u1) - j1 * (na.u2 + nb.u2) - 2 * (na.d + nb.d) +
+                                   3 * j1 * j2 - (__popcll(Ba.x & Bb.y) + __popcll(Bb.x & Ba.y)) + ID;
+            if (live > 0) {
+                const CardAgg ga = agg[a], gb = agg[b];
+                const double m1 = M1[a * MS + b], m2 = M2[a * MS + b];
+                const double A1 = F1 - ga.u1 - gb.u1 + m1;
+                const double A2 = F2 - ga.u2 - gb.u2 + m2;
+                const double z = A1 * A2 - Q + ga.u1 * ga.u2 + gb.u1 * gb.u2 + ga.w + gb.w -
+                                 m2 * (ga.u1 + gb.u1) - m1 * (ga.u2 + gb.u2) - 2.0 * (ga.d + gb.d) +
+                                 3.0 * m1 * m2 -
+                                 (static_cast<double>(P[a * MS + b]) + static_cast<double>(P[b * MS + a])) + D;
+                v = static_cast<float>(static_cast<double>(term_factor(c, I, h)) * z);
             }
-            const double m1 = M1[a * MS + b], m2 = M2[a * MS + b];
-            const double ua1 = u1[a], ub1 = u1[b], ua2 = u2[a], ub2 = u2[b];
-            const double A1 = F1 - ua1 - ub1 + m1;
-            const double A2 = F2 - ua2 - ub2 + m2;
-            const double z = A1 * A2 - Q + ua1 * ua2 + ub1 * ub2 + (w12[a] + w12[b] + w21[a] + w21[b]) -
-                             m2 * (ua1 + ub1) - m1 * (ua2 + ub2) - 2.0 * (dd[a] + dd[b]) +
-                             3.0 * m1 * m2 -
-                             (static_cast<double>(P[a * MS + b]) + static_cast<double>(P[b * MS + a])) + D;
-            v = static_cast<float>(static_cast<double>(term_factor(c, I, h)) * z);
         }
         out[h] = v;
     }
@@ -436,6 +490,8 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr2(DevCtx c, const TermI
 //   W = P[lo] - PC[c1][<lo] - PC[c2][<lo]
 //   T = P[hi] - P[lo] - (PC[c1][<hi] - PC[c1][<lo]) - (PC[c2][<hi] - PC[c2][<lo]) + f(h)
 //   S = P[end] - PC[c1][end] - PC[c2][end] + f(h)
+// A traverser hand with no compatible positive-reach opponent hand gets
+// exactly 0 (positive-reach masks per card, as in the two-opponent kernels).
 __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermItem *__restrict__ items,
                                                            int trav) {
     __shared__ float Rr[1326];
@@ -449,32 +505,22 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nc = c.ncomb;
     for (int i = tid; i < nc; i += blockDim.x) Rr[i] = 0.f;
-    if (tid < 52) B[tid] = 0ull;
     __syncthreads();
     {
         const int o = I.opp_player[0];
         const float *r = c.reach + static_cast<size_t>(I.opp_row[0]) * c.HS;
         const int *pos = c.sd_pos + static_cast<size_t>(o) * c.HS;
-        const int *code = c.hand_code + static_cast<size_t>(o) * c.HS;
+        const bool dup = c.dup[o] != 0;
         for (int j = tid; j < c.H[o]; j += blockDim.x) {
             const int q = pos[j];
             if (q < 0) continue;
-            const float x = r[j];
-            atomicAdd(&Rr[q], x);
-            if (x > 0.f) {
-                const int a = code[j] & 0xff, b = (code[j] >> 8) & 0xff;
-                atomicOr(&B[a], 1ull << b);
-                atomicOr(&B[b], 1ull << a);
-            }
+            if (dup)
+                atomicAdd(&Rr[q], r[j]);
+            else
+                Rr[q] = r[j];
         }
     }
     __syncthreads();
-    if (warp == 0) {
-        int n = __popcll(B[lane]) + (lane + 32 < 52 ? __popcll(B[lane + 32]) : 0);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-        if (lane == 0) npos = n / 2;
-    }
     // exclusive prefix over rank positions: each thread scans a contiguous chunk
     {
         const int per = (nc + blockDim.x - 1) / blockDim.x;
@@ -502,13 +548,15 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
             Pp[nc] = tot;
         }
     }
-    // per-card exclusive prefix sums over each card's combos in rank order
+    // per card: exclusive prefix sums over its combos in rank order, and the
+    // mask of partner cards whose combo holds positive reach
     for (int card = warp; card < 52; card += blockDim.x / 32) {
         const short *L = c.sd_card_list + card * 52;
+        const short *Pt = c.sd_card_partner + card * 52;
         const int i0 = 2 * lane, i1 = 2 * lane + 1;
         const int q0 = i0 < 52 ? L[i0] : -1, q1 = i1 < 52 ? L[i1] : -1;
-        const double v0 = q0 >= 0 ? static_cast<double>(Rr[q0]) : 0.0;
-        const double v1 = q1 >= 0 ? static_cast<double>(Rr[q1]) : 0.0;
+        const float f0 = q0 >= 0 ? Rr[q0] : 0.f, f1 = q1 >= 0 ? Rr[q1] : 0.f;
+        const double v0 = f0, v1 = f1;
         const double pair = v0 + v1;
         double incl = pair;
 #pragma unroll
@@ -517,12 +565,25 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
             if (lane >= o) incl += y;
         }
         const double ex = incl - pair;
-        const unsigned have = __ballot_sync(0xffffffffu, q0 >= 0);
-        const unsigned have1 = __ballot_sync(0xffffffffu, q1 >= 0);
-        const int len = __popc(have) + __popc(have1);
+        const int len = __popc(__ballot_sync(0xffffffffu, q0 >= 0)) + __popc(__ballot_sync(0xffffffffu, q1 >= 0));
         if (i0 <= len) PC[card * 53 + i0] = ex;
         if (i1 <= len) PC[card * 53 + i1] = ex + v0;
-        if (lane == 0) clen[card] = len;
+        unsigned long long m = 0ull;
+        if (f0 > 0.f) m |= 1ull << Pt[i0];
+        if (f1 > 0.f) m |= 1ull << Pt[i1];
+        const unsigned lo = __reduce_or_sync(0xffffffffu, static_cast<unsigned>(m));
+        const unsigned hi = __reduce_or_sync(0xffffffffu, static_cast<unsigned>(m >> 32));
+        if (lane == 0) {
+            clen[card] = len;
+            B[card] = static_cast<unsigned long long>(lo) | (static_cast<unsigned long long>(hi) << 32);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int n = __popcll(B[lane]) + (lane + 32 < 52 ? __popcll(B[lane + 32]) : 0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+        if (lane == 0) npos = n / 2;
     }
     __syncthreads();
     const int Ht = c.H[trav];
@@ -532,17 +593,18 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
     for (int h = tid; h < c.HS; h += blockDim.x) {
         float v = 0.f;
         const int q = h < Ht ? tpos[h] : -1;
-        if (q >= 0 &&
-            npos - __popcll(B[c.sd_combo[q].c1]) - __popcll(B[c.sd_combo[q].c2]) +
-                    bit(B[c.sd_combo[q].c1], c.sd_combo[q].c2) > 0) {
+        if (q >= 0) {
             const SdCombo s = c.sd_combo[q];
-            const double *p1 = PC + s.c1 * 53, *p2 = PC + s.c2 * 53;
-            const double self = Rr[q];
-            const double W = Pp[s.lo] - p1[s.l1lo] - p2[s.l2lo];
-            const double T = (Pp[s.hi] - Pp[s.lo]) - (p1[s.l1hi] - p1[s.l1lo]) -
-                             (p2[s.l2hi] - p2[s.l2lo]) + self;
-            const double S = Pp[nc] - p1[clen[s.c1]] - p2[clen[s.c2]] + self;
-            v = static_cast<float>(pot * W + 0.5 * pot * T - bet * S);
+            const unsigned long long B1 = B[s.c1], B2 = B[s.c2];
+            if (npos - __popcll(B1) - __popcll(B2) + bit(B1, s.c2) > 0) {
+                const double *p1 = PC + s.c1 * 53, *p2 = PC + s.c2 * 53;
+                const double self = Rr[q];
+                const double W = Pp[s.lo] - p1[s.l1lo] - p2[s.l2lo];
+                const double T = (Pp[s.hi] - Pp[s.lo]) - (p1[s.l1hi] - p1[s.l1lo]) -
+                                 (p2[s.l2hi] - p2[s.l2lo]) + self;
+                const double S = Pp[nc] - p1[clen[s.c1]] - p2[clen[s.c2]] + self;
+                v = static_cast<float>(pot * W + 0.5 * pot * T - bet * S);
+            }
         }
         out[h] = v;
     }
@@ -699,8 +761,8 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
 
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s) {
     if (n <= 0 || H <= 0) return cudaSuccess;
-    const int nc = chunks(H);
-    k_cfv<<<n * nc, kHandThreads, 0, s>>>(c, items, nc, H);
+    const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
+    k_cfv<<<n * nc, kCfvThreads, 0, s>>>(c, items, nc, H);
     return cudaGetLastError();
 }
 

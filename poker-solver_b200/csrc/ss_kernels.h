@@ -20,17 +20,21 @@ struct DevCtx {
     const unsigned *strength;    // [np][HS]
     const SdCombo *sd_combo;     // [ncomb]
     const short *sd_card_list;   // [52][52]
+    const short *sd_card_partner;// [52][52]
     const float *leaf_values;
     const int *iter;       // current CFR iteration (device counter)
     int HS;
     int np;
     int ncomb;
     int H[SS_MAX_PLAYERS];
+    int dup[SS_MAX_PLAYERS];     // range holds some combo more than once
 };
 
 // threads per block of the per-hand kernels; each thread covers 4 hands
 constexpr int kHandThreads = 64;
 constexpr int kHandsPerBlock = kHandThreads * 4;
+// threads per block of the value/regret kernel (2 hands each)
+constexpr int kCfvThreads = 128;
 // threads per block of the per-terminal kernels
 constexpr int kTermThreads = 256;
 

@@ -318,6 +318,7 @@ int build_plan(const Problem &pb, Plan *out) {
     P.ncomb = 0;
     P.sd_combo.clear();
     P.sd_card_list.assign(52 * 52, -1);
+    P.sd_card_partner.assign(52 * 52, -1);
     P.sd_pos.assign(static_cast<size_t>(np) * HS, -1);
     P.strength.assign(static_cast<size_t>(np) * HS, 0u);
     if (need_sd) {
@@ -340,7 +341,9 @@ int build_plan(const Problem &pb, Plan *out) {
         for (int q = 0; q < nc; ++q) {
             pos_of[combos[q].a * 52 + combos[q].b] = q;
             pos_of[combos[q].b * 52 + combos[q].a] = q;
+            P.sd_card_partner[combos[q].a * 52 + len[combos[q].a]] = static_cast<short>(combos[q].b);
             P.sd_card_list[combos[q].a * 52 + len[combos[q].a]++] = static_cast<short>(q);
+            P.sd_card_partner[combos[q].b * 52 + len[combos[q].b]] = static_cast<short>(combos[q].a);
             P.sd_card_list[combos[q].b * 52 + len[combos[q].b]++] = static_cast<short>(q);
         }
         for (int q = 0; q < nc;) {
@@ -374,6 +377,18 @@ int build_plan(const Problem &pb, Plan *out) {
                 P.sd_pos[p * HS + h] = q;
                 P.strength[p * HS + h] = combos[q].s;
             }
+    }
+
+    // ranges holding the same combo twice need atomic accumulation in the
+    // terminal kernels' combo tables
+    for (int p = 0; p < np; ++p) {
+        std::vector<char> seen(52 * 52, 0);
+        P.dup[p] = 0;
+        for (int h = 0; h < P.H[p]; ++h) {
+            int a = pb.hands[p][2 * h], b = pb.hands[p][2 * h + 1];
+            if (a > b) std::swap(a, b);
+            if (seen[a * 52 + b]++) P.dup[p] = 1;
+        }
     }
 
     double hsum = 0;
