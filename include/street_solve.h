@@ -272,6 +272,24 @@ int ss_rank7_batch(const int *cards7, int n, unsigned int *strength_out);
  * per category (may be NULL).  mix64 is the splitmix64 finaliser. */
 int ss_rank7_checksum(unsigned long long *checksum, unsigned long long *category_counts);
 
+/* EXTENSION (no counterpart in the reference): ss_solve_gpu for callers that
+ * cannot allocate GPU memory at solve time -- e.g. a process whose device
+ * memory belongs to another allocator, or a serving path with a
+ * no-allocation policy.  It calls no CUDA allocation routine: all device
+ * state lives in a 64 MiB static device array that every GPU loading this
+ * library reserves until exit, and kernels run on the legacy default stream
+ * without graphs or events.  The caller provides the output arrays in
+ * *output: root_strategy (root actions x hands of the root player), root_ev
+ * (num_players x max_hands), avg_strategies (num_decision_nodes x 8 x
+ * max_hands) and avg_strategy_node_ids (num_decision_nodes); they are filled
+ * like ss_solve_gpu's, and ss_free_output must not be called on them.  A
+ * subgame whose state exceeds the array fails with SS_ERR_NOMEM and the size
+ * it needs.  The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * share the array and it keeps the previous call's data (each call rewrites
+ * what it reads); calls that overlap on the same GPU race. */
+int ss_solve_gpu_noalloc(SSTreeData *tree_data, int max_iterations, SSOutput *output);
+
 /* EXTENSION: message for the last failure on the calling thread ("" if none). */
 const char *ss_last_error(void);
 

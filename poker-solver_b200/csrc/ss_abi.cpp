@@ -194,6 +194,18 @@ int ss_solve_gpu(SSTreeData *td, int max_iterations, SSOutput *output) {
     return ss_solve_gpu_ex(td, max_iterations, nullptr, output, nullptr);
 }
 
+int ss_solve_gpu_noalloc(SSTreeData *td, int max_iterations, SSOutput *output) {
+    ssb::Problem pb;
+    int rc = to_problem(td, &pb);
+    if (rc != SS_OK) return rc;
+    try {
+        return ssb::solve_noalloc(pb, max_iterations, output);
+    } catch (const std::bad_alloc &) {
+        ssb::set_error("out of host memory");
+        return SS_ERR_NOMEM;
+    }
+}
+
 int ss_exploitability_gpu(const SSTreeData *td, const float *avg, double *expl_pct,
                           double *nashconv, double *br_value, double *cur_value,
                           double *deal_mass) {

@@ -189,6 +189,9 @@ int session_profile(Session *s, SSKernelProfile *prof);
 void session_destroy(Session *s);
 void *session_stream(Session *s);
 
+// ss_noalloc.cu: solve with all device state in a static device array
+int solve_noalloc(const Problem &pb, int iterations, SSOutput *out);
+
 int exploitability(const Problem &pb, const float *avg_strategies, double *expl_pct,
                    double *nashconv, double *br_value, double *cur_value, double *deal_mass);
 
