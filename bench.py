@@ -256,6 +256,12 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
+    # FP64 exploitability of the last solve's average strategy
+    lib.ss_session_exploitability.restype = ctypes.c_int
+    lib.ss_session_exploitability.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_double)] * 5
+    expl, nash = ctypes.c_double(-1), ctypes.c_double(-1)
+    erc = lib.ss_session_exploitability(sess, ctypes.byref(expl), ctypes.byref(nash), None, None, None)
+    exploit = expl.value if erc == 0 else None
     total_ms = ev0.elapsed_time(ev_end)
     times = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     total_ms_max = dist_max(total_ms)
@@ -328,6 +334,7 @@ def run_ours(args, world, rank, local):
                         "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
                     for k, v in classes.items() if v["launches"]},
         "iteration_ms": prof.iteration_ms,
+        "exploitability_pct": exploit,
         "tree": tree_info,
     }
 
@@ -452,6 +459,7 @@ def main():
             "roofline": res["roofline"], "cpu_baseline": cpu, "clocks": res["clocks"],
             "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
+            "exploitability_pct_after_solve": res["exploitability_pct"],
         }
         print(json.dumps(line))
     try:

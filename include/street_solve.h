@@ -260,6 +260,11 @@ int ss_session_profile(SSSession *session, SSKernelProfile *profile);
  * caller can order its own work or time the session with CUDA events. */
 void *ss_session_stream(SSSession *session);
 
+/* EXTENSION: FP64 exploitability of the session's current average strategy
+ * (same outputs as ss_exploitability_gpu; any pointer may be NULL). */
+int ss_session_exploitability(SSSession *session, double *exploitability_pct, double *nashconv,
+                              double *br_value, double *cur_value, double *deal_mass);
+
 /* EXTENSION: release the session. */
 void ss_session_destroy(SSSession *session);
 

@@ -298,6 +298,12 @@ int ss_session_profile(SSSession *s, SSKernelProfile *prof) {
     return ssb::session_profile(s->impl, prof);
 }
 
+int ss_session_exploitability(SSSession *s, double *pct, double *nash, double *br, double *cur,
+                              double *z) {
+    if (!s) return SS_ERR_INVALID;
+    return ssb::session_exploitability(s->impl, nullptr, pct, nash, br, cur, z);
+}
+
 void *ss_session_stream(SSSession *s) { return s ? ssb::session_stream(s->impl) : nullptr; }
 
 void ss_session_destroy(SSSession *s) {

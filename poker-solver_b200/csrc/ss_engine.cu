@@ -118,6 +118,11 @@ class Session {
     std::vector<double> reach_bytes[SS_MAX_PLAYERS], cfv_bytes[SS_MAX_PLAYERS];
     double term_bytes[SS_MAX_PLAYERS][TK_COUNT] = {};
     cudaGraphExec_t gA = nullptr, gC = nullptr, gB = nullptr;  // G iters, 1 iter, 1 iter + snapshot
+    // best response state (allocated on first use)
+    std::vector<float> host_w;          // range weights [np][HS]
+    double *dbr = nullptr;              // reach_d [E + np][HS], val_d [N + 1][HS]
+    char *dbr_tab = nullptr;            // edge -> decision index, deal item, row list, scalars
+    float *davg_br = nullptr;           // profile in the output layout
 
     // profiling hook: when set, every launch is preceded by an event record
     struct Mark {
@@ -137,6 +142,9 @@ class Session {
             if (dleaf) cudaFreeAsync(dleaf, stream);
             if (dsmall) cudaFreeAsync(dsmall, stream);
             if (diter) cudaFreeAsync(diter, stream);
+            if (dbr) cudaFreeAsync(dbr, stream);
+            if (dbr_tab) cudaFreeAsync(dbr_tab, stream);
+            if (davg_br) cudaFreeAsync(davg_br, stream);
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
         }
@@ -214,6 +222,8 @@ class Session {
     }
 
     int init(const Problem &pb, const SolveConfig &cfg);
+    int exploitability(const float *host_avg, double *pct, double *nash, double *br, double *cur,
+                       double *deal_mass);
     int reset();
     int run(int iters);
     int output(SSOutput *out);
@@ -329,6 +339,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
         CK(cudaMemcpyAsync(reach + E * HS, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice,
                            stream));
         CK(cudaStreamSynchronize(stream));  // the staging vector must outlive the copy
+        host_w = w;
     }
     if (pb.leaf_values && pb.num_leaves > 0) {
         const size_t n = static_cast<size_t>(pb.num_leaves) * np * P.max_h;
@@ -490,6 +501,111 @@ int Session::profile(SSKernelProfile *prof) {
     return SS_OK;
 }
 
+// NashConv of an average-strategy profile (the session's own when host_avg is
+// null, else avg given in the SSOutput layout), FP64 throughout: every
+// player's reach under the profile, then per player the terminal values
+// (same closed forms as the CFR path, in double), the profile value and the
+// best-response value at its own nodes, and the root sums weighted by the
+// player's range.  Exploitability = NashConv / np / starting pot * 100.
+int Session::exploitability(const float *host_avg, double *pct, double *nash, double *br, double *cur,
+                            double *deal_mass) {
+    CK(cudaSetDevice(device));
+    const int np = P.np;
+    const size_t HS = static_cast<size_t>(P.HS), E = static_cast<size_t>(P.E), N = static_cast<size_t>(P.N);
+    const size_t n_avg = static_cast<size_t>(P.num_dec) * SS_MAX_ACTIONS * P.max_h;
+    // deal mass term: the players' ranges against each other (valid deals)
+    TermItem deal;
+    std::memset(&deal, 0, sizeof(deal));
+    deal.node = P.N;
+    deal.leaf_off = -1;
+    deal.payoff = 1.f;
+    deal.k = np - 1;
+    for (int o = 1; o < np; ++o) {
+        deal.opp_row[o - 1] = P.E + o;
+        deal.opp_player[o - 1] = o;
+    }
+    const int deal_kind = np == 1 ? TK_LEAF0 : np == 2 ? TK_CR1 : np == 3 ? TK_CR2 : TK_ENUM;
+    if (deal_kind == TK_ENUM) {
+        double w = P.H[0];
+        for (int o = 1; o < np; ++o) w *= std::max(1, P.H[o]);
+        if (w > kEnumLimitPerIter) {
+            set_error("exploitability: the deal mass of " + std::to_string(np) +
+                      " players needs the multiway closed form; only small ranges are supported");
+            return SS_ERR_UNSUPPORTED;
+        }
+    }
+    if (!dbr) {
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&dbr), ((E + np) + (N + 1)) * HS * sizeof(double), stream));
+        CK(cudaMemsetAsync(dbr, 0, ((E + np) + (N + 1)) * HS * sizeof(double), stream));
+        std::vector<double> w(host_w.begin(), host_w.end());
+        CK(cudaMemcpyAsync(dbr + E * HS, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        Blob t;
+        std::vector<int> node_di(P.N, -1), edge_di(P.E);
+        for (int i = 0; i < P.num_dec; ++i) node_di[P.dec_nodes[i]] = i;
+        for (int e = 0; e < P.E; ++e) edge_di[e] = node_di[P.edge_node[e]];
+        t.add(edge_di);
+        t.add(&deal, sizeof(deal));
+        const int nrow = P.N;
+        t.add(&nrow, sizeof(int));
+        t.add(nullptr, (2 * SS_MAX_PLAYERS + 2) * sizeof(double));
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&dbr_tab), t.host.size(), stream));
+        CK(cudaMemcpyAsync(dbr_tab, t.host.data(), t.host.size(), cudaMemcpyHostToDevice, stream));
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&davg_br), std::max<size_t>(n_avg, 1) * sizeof(float), stream));
+        CK(cudaStreamSynchronize(stream));  // host staging must outlive the copies
+    }
+    c.reach_d = dbr;
+    c.val_d = dbr + (E + np) * HS;
+    // table offsets (same order as written above)
+    size_t off = 0;
+    auto next = [&](size_t bytes) {
+        off = (off + 255) & ~static_cast<size_t>(255);
+        size_t r = off;
+        off += bytes;
+        return r;
+    };
+    const int *edge_di = reinterpret_cast<const int *>(dbr_tab + next(P.E * sizeof(int)));
+    const TermItem *d_deal = reinterpret_cast<const TermItem *>(dbr_tab + next(sizeof(TermItem)));
+    const int *d_row = reinterpret_cast<const int *>(dbr_tab + next(sizeof(int)));
+    double *d_sc = reinterpret_cast<double *>(dbr_tab + next((2 * SS_MAX_PLAYERS + 2) * sizeof(double)));
+
+    if (host_avg)
+        CK(cudaMemcpyAsync(davg_br, host_avg, n_avg * sizeof(float), cudaMemcpyHostToDevice, stream));
+    else
+        CK(launch_avg_strategy(c, dec_fe, dec_na, dec_pl, P.num_dec, P.max_h, davg_br, stream));
+    for (int p = 0; p < np; ++p)
+        for (size_t l = 0; l < reach_lv[p].size(); ++l)
+            CK(launch_br_reach(c, reach_items[p] + reach_lv[p][l].first, reach_lv[p][l].second, P.H[p],
+                               davg_br, edge_di, P.max_h, stream));
+    for (int t = 0; t < np; ++t) {
+        for (int k = 0; k < TK_COUNT; ++k)
+            CK(launch_terms_fp64(c, k, term_items[t][k], static_cast<int>(P.term[t][k].size()), t, stream));
+        for (int mode = 0; mode < 2; ++mode) {
+            for (size_t l = 0; l < cfv_lv[t].size(); ++l)
+                CK(launch_br_value(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.H[t],
+                                   davg_br, edge_di, P.max_h, mode, stream));
+            CK(launch_br_root(c, root_fr[t], static_cast<int>(P.root_fr[t].size()), P.H[t], P.E + t, t, 0,
+                              d_sc + 2 * t + mode, stream));
+        }
+    }
+    CK(launch_terms_fp64(c, deal_kind, d_deal, 1, 0, stream));
+    CK(launch_br_root(c, d_row, 1, P.H[0], P.E, 0, 1, d_sc + 2 * SS_MAX_PLAYERS, stream));
+    double sc[2 * SS_MAX_PLAYERS + 2] = {};
+    CK(cudaMemcpyAsync(sc, d_sc, sizeof(sc), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    double nc = 0.0;
+    for (int t = 0; t < np; ++t) {
+        if (cur) cur[t] = sc[2 * t];
+        if (br) br[t] = sc[2 * t + 1];
+        nc += sc[2 * t + 1] - sc[2 * t];
+    }
+    const double z = sc[2 * SS_MAX_PLAYERS];
+    if (deal_mass) *deal_mass = z;
+    const double nash_v = z > 0 ? nc / z : 0.0;
+    if (nash) *nash = nash_v;
+    if (pct) *pct = P.starting_pot > 0 ? nash_v / np / P.starting_pot * 100.0 : 0.0;
+    return SS_OK;
+}
+
 // ---------------------------------------------------------------------------
 // entry points used by the ABI layer
 // ---------------------------------------------------------------------------
@@ -518,6 +634,10 @@ int session_reset(Session *s) { return s->reset(); }
 int session_iterations(const Session *s) { return s->iterations; }
 int session_output(Session *s, SSOutput *out) { return s->output(out); }
 int session_profile(Session *s, SSKernelProfile *p) { return s->profile(p); }
+int session_exploitability(Session *s, const float *host_avg, double *pct, double *nash, double *br,
+                           double *cur, double *z) {
+    return s->exploitability(host_avg, pct, nash, br, cur, z);
+}
 void session_destroy(Session *s) { delete s; }
 void *session_stream(Session *s) { return static_cast<void *>(s->stream); }
 
@@ -542,25 +662,58 @@ int solve(const Problem &pb, int iterations, const SolveConfig &cfg, SSOutput *o
         set_error("cudaEventCreate failed");
         rc = SS_ERR_CUDA;
     }
-    if (rc == SS_OK && cudaEventRecord(e0, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
-    if (rc == SS_OK) rc = s->run(iterations);
-    if (rc == SS_OK && cudaEventRecord(e1, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+    double pct = -1.0, nash = -1.0;
+    int done = 0;
+    if (cfg.target_exploitability > 0.f) {
+        // run in blocks of check_every iterations until the profile is within
+        // the target (or max_iterations); solve time covers the CFR blocks only
+        const int step = std::max(1, cfg.check_every);
+        float acc = 0.f;
+        while (rc == SS_OK && done < iterations) {
+            const int n = std::min(step, iterations - done);
+            if (cudaEventRecord(e0, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+            if (rc == SS_OK) rc = s->run(n);
+            if (rc == SS_OK && cudaEventRecord(e1, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+            if (rc == SS_OK) rc = s->exploitability(nullptr, &pct, &nash, nullptr, nullptr, nullptr);
+            if (rc == SS_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) acc += ms;
+            done += n;
+            if (rc == SS_OK && pct <= cfg.target_exploitability) break;
+        }
+        ms = acc;
+    } else {
+        if (rc == SS_OK && cudaEventRecord(e0, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+        if (rc == SS_OK) rc = s->run(iterations);
+        if (rc == SS_OK && cudaEventRecord(e1, s->stream) != cudaSuccess) rc = SS_ERR_CUDA;
+        if (rc == SS_OK && cudaEventSynchronize(e1) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            ms = -1.f;
+        done = iterations;
+        if (rc == SS_OK && cfg.compute_exploitability)
+            rc = s->exploitability(nullptr, &pct, &nash, nullptr, nullptr, nullptr);
+    }
     if (rc == SS_OK) rc = s->output(out);
-    if (rc == SS_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = -1.f;
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (rc == SS_OK && stats) {
-        stats->iterations_run = iterations;
+        stats->iterations_run = done;
         stats->solve_ms = ms;
-        stats->node_hand_updates = s->P.node_hands * iterations;
+        stats->node_hand_updates = s->P.node_hands * done;
+        stats->exploitability_pct = pct;
+        stats->nashconv = nash;
     }
     session_destroy(s);
     return rc;
 }
 
-int exploitability(const Problem &, const float *, double *, double *, double *, double *, double *) {
-    set_error("exploitability: not available in this build yet");
-    return SS_ERR_UNSUPPORTED;
+int exploitability(const Problem &pb, const float *avg, double *pct, double *nash, double *br,
+                   double *cur, double *z) {
+    SolveConfig cfg;
+    Session *s = nullptr;
+    int rc = session_create(pb, cfg, &s);
+    if (rc != SS_OK) return rc;
+    rc = s->exploitability(avg, pct, nash, br, cur, z);
+    session_destroy(s);
+    return rc;
 }
 
 }  // namespace ssb

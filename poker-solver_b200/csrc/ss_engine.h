@@ -129,6 +129,7 @@ struct Plan {
     int H[SS_MAX_PLAYERS] = {};
     int root_player = -1, root_na = 0;
     int num_dec = 0;
+    int starting_pot = 0;
     std::vector<int> dec_nodes;        // decision node ids in index order
     std::vector<int> first_edge;       // [N], -1 for terminals
     std::vector<int> edge_node;        // [E]
@@ -188,6 +189,8 @@ int session_output(Session *s, SSOutput *out);
 int session_profile(Session *s, SSKernelProfile *prof);
 void session_destroy(Session *s);
 void *session_stream(Session *s);
+int session_exploitability(Session *s, const float *host_avg, double *pct, double *nash, double *br,
+                           double *cur, double *z);
 
 // ss_noalloc.cu: solve with all device state in a static device array
 int solve_noalloc(const Problem &pb, int iterations, SSOutput *out);

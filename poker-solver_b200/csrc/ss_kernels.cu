@@ -198,8 +198,18 @@ __device__ __forceinline__ float term_factor(const DevCtx &c, const TermItem &I,
     return I.leaf_off >= 0 ? c.leaf_values[I.leaf_off + h] : I.payoff;
 }
 
+// The terminal kernels serve the CFR iterations (T = float: reach and values
+// in FP32, per-node aggregates in FP64) and the best response (T = double).
+template <class T> __device__ __forceinline__ const T *reach_rows(const DevCtx &c);
+template <> __device__ __forceinline__ const float *reach_rows<float>(const DevCtx &c) { return c.reach; }
+template <> __device__ __forceinline__ const double *reach_rows<double>(const DevCtx &c) { return c.reach_d; }
+template <class T> __device__ __forceinline__ T *val_rows(const DevCtx &c);
+template <> __device__ __forceinline__ float *val_rows<float>(const DevCtx &c) { return c.val; }
+template <> __device__ __forceinline__ double *val_rows<double>(const DevCtx &c) { return c.val_d; }
+
 // value rows of terminals with no opponent coupling: zero, or the factor itself
 // (a leaf without a live opponent, street_solve.cu:1062-1065)
+template <class T>
 __global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c, const TermItem *__restrict__ items,
                                                             int nchunk, int trav, int zero) {
     const int it = blockIdx.x / nchunk;
@@ -208,10 +218,9 @@ __global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c, const Term
     if (h0 >= c.HS) return;
     const TermItem I = items[it];
     const int Ht = c.H[trav];
-    float o[4];
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS + h0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) o[i] = (zero || h0 + i >= Ht) ? 0.f : term_factor(c, I, h0 + i);
-    st4(c.val + static_cast<size_t>(I.node) * c.HS + h0, make_float4(o[0], o[1], o[2], o[3]));
+    for (int i = 0; i < 4; ++i) out[i] = (zero || h0 + i >= Ht) ? T(0) : static_cast<T>(term_factor(c, I, h0 + i));
 }
 
 // Scatter one opponent's reach at a terminal into a 52x52 combo matrix
@@ -219,8 +228,9 @@ __global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c, const Term
 // Board-blocked hands never count (street_solve.cu:755-757).  A range that
 // holds some combo twice accumulates atomically; otherwise each cell has one
 // writer and plain stores suffice.
-__device__ __forceinline__ void scatter_combo(const DevCtx &c, int opp, int row, float *M) {
-    const float *r = c.reach + static_cast<size_t>(row) * c.HS;
+template <class T>
+__device__ __forceinline__ void scatter_combo(const DevCtx &c, int opp, int row, T *M) {
+    const T *r = reach_rows<T>(c) + static_cast<size_t>(row) * c.HS;
     const int *code = c.hand_code + static_cast<size_t>(opp) * c.HS;
     const int Ho = c.H[opp];
     const bool dup = c.dup[opp] != 0;
@@ -228,7 +238,7 @@ __device__ __forceinline__ void scatter_combo(const DevCtx &c, int opp, int row,
         const int hc = code[j];
         if (hc & 0x10000) continue;
         const int a = hc & 0xff, b = (hc >> 8) & 0xff;
-        const float x = r[j];
+        const T x = r[j];
         if (dup) {
             atomicAdd(&M[a * MS + b], x);
             atomicAdd(&M[b * MS + a], x);
@@ -241,42 +251,82 @@ __device__ __forceinline__ void scatter_combo(const DevCtx &c, int opp, int row,
 
 __device__ __forceinline__ int bit(unsigned long long m, int b) { return static_cast<int>((m >> b) & 1ull); }
 
-__device__ __forceinline__ void zero_matrix(float *M) {
+template <class T>
+__device__ __forceinline__ void zero_matrix(T *M) {
     float4 *m4 = reinterpret_cast<float4 *>(M);
-    for (int i = threadIdx.x; i < 52 * MS / 4; i += blockDim.x) m4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int n = 52 * MS * static_cast<int>(sizeof(T)) / 16;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// four consecutive matrix entries (16-byte aligned)
+__device__ __forceinline__ void load4(const float *p, double v[4]) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void load4(const double *p, double v[4]) {
+    const double2 x = *reinterpret_cast<const double2 *>(p);
+    const double2 y = *reinterpret_cast<const double2 *>(p + 2);
+    v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
+__device__ __forceinline__ void load4(const float *p, float v[4]) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
 }
 
 // Row pass over a combo matrix, one warp per card row r: the row sum u(r) in
 // FP64 and the 64-bit mask of the row's positive cells.  The masks give the
 // exact number of compatible positive-reach opponent tuples through the same
-// inclusion-exclusion as the float sums; where that number is 0 the value is
+// inclusion-exclusion as the sums; where that number is 0 the value is
 // exactly 0, as in the reference, which only adds positive products
 // (street_solve.cu:810-812).  Without it rounding residue of the closed form
 // would turn into a pure strategy under regret matching where the reference
 // plays uniformly.
-__device__ __forceinline__ void row_stats(const float *M, int r, int lane, double *sum_out,
-                                          unsigned long long *mask_out, float *x0, float *x1) {
-    const float a = M[r * MS + lane];
-    const float b = lane + 32 < 52 ? M[r * MS + lane + 32] : 0.f;
-    const unsigned lo = __ballot_sync(0xffffffffu, a > 0.f);
-    const unsigned hi = __ballot_sync(0xffffffffu, b > 0.f);
+template <class T>
+__device__ __forceinline__ void row_stats(const T *M, int r, int lane, double *sum_out,
+                                          unsigned long long *mask_out, double *x0, double *x1) {
+    const T a = M[r * MS + lane];
+    const T b = lane + 32 < 52 ? M[r * MS + lane + 32] : T(0);
+    const unsigned lo = __ballot_sync(0xffffffffu, a > T(0));
+    const unsigned hi = __ballot_sync(0xffffffffu, b > T(0));
     *sum_out = warp_sum(static_cast<double>(a) + static_cast<double>(b));
     *mask_out = static_cast<unsigned long long>(lo) | (static_cast<unsigned long long>(hi) << 32);
     *x0 = a;
     *x1 = b;
 }
 
+template <class T>
+__device__ __forceinline__ void store_value(T *out, int h, double v) { out[h] = static_cast<T>(v); }
+
+// shared-memory carve-up of the terminal kernels (dynamic, 16-byte aligned)
+struct Carve {
+    char *p;
+    template <class U>
+    __device__ __forceinline__ U *take(int n) {
+        U *r = reinterpret_cast<U *>(p);
+        p += (static_cast<size_t>(n) * sizeof(U) + 15) & ~static_cast<size_t>(15);
+        return r;
+    }
+};
+
+template <class T>
+constexpr size_t cr1_smem() {
+    return 52 * MS * sizeof(T) + 52 * 8 + 52 * 8 + 64;
+}
+
 // One counted opponent: mass(h) = F - u(c1) - u(c2) + f(h), F the opponent's
 // total reach, u(c) its reach on hands holding card c, f(h) its reach on the
 // traverser's own combo.  Folds: payoff * mass (street_solve.cu:745-761);
 // leaves: leaf value * mass (:1047-1066).
+template <class T>
 __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermItem *__restrict__ items,
                                                            int trav) {
-    __shared__ __align__(16) float M[52 * MS];
-    __shared__ double u[52];
-    __shared__ unsigned long long B[52];
-    __shared__ double F;
-    __shared__ int npos;
+    extern __shared__ __align__(16) char smem[];
+    Carve cv{smem};
+    T *M = cv.take<T>(52 * MS);
+    double *u = cv.take<double>(52);
+    unsigned long long *B = cv.take<unsigned long long>(52);
+    double *F = cv.take<double>(1);
+    int *npos = cv.take<int>(1);
     const TermItem I = items[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     zero_matrix(M);
@@ -284,9 +334,8 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermI
     scatter_combo(c, I.opp_player[0], I.opp_row[0], M);
     __syncthreads();
     for (int r = warp; r < 52; r += blockDim.x / 32) {
-        double s;
+        double s, x0, x1;
         unsigned long long m;
-        float x0, x1;
         row_stats(M, r, lane, &s, &m, &x0, &x1);
         if (lane == 0) {
             u[r] = s;
@@ -301,27 +350,29 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermI
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
         if (lane == 0) {
-            F = 0.5 * s;
-            npos = n / 2;
+            *F = 0.5 * s;
+            *npos = n / 2;
         }
     }
     __syncthreads();
     const int Ht = c.H[trav];
     const int *tc = c.hand_code + static_cast<size_t>(trav) * c.HS;
-    float *out = c.val + static_cast<size_t>(I.node) * c.HS;
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
+    const double Fv = *F;
+    const int np_ = *npos;
     for (int h = tid; h < c.HS; h += blockDim.x) {
-        float v = 0.f;
+        double v = 0.0;
         if (h < Ht) {
             const int hc = tc[h];
             const int a = hc & 0xff, b = (hc >> 8) & 0xff;
             const unsigned long long Ba = B[a], Bb = B[b];
-            const int live = npos - __popcll(Ba) - __popcll(Bb) + bit(Ba, b);
+            const int live = np_ - __popcll(Ba) - __popcll(Bb) + bit(Ba, b);
             if (live > 0) {
-                const double z = F - u[a] - u[b] + static_cast<double>(M[a * MS + b]);
-                v = static_cast<float>(static_cast<double>(term_factor(c, I, h)) * z);
+                const double z = Fv - u[a] - u[b] + static_cast<double>(M[a * MS + b]);
+                v = static_cast<double>(term_factor(c, I, h)) * z;
             }
         }
-        out[h] = v;
+        store_value(out, h, v);
     }
 }
 
@@ -334,6 +385,16 @@ struct alignas(16) CardAgg {
 struct alignas(16) CardCnt {
     int u1, u2, w, d;   // the same on the 0/1 positive-reach matrices
 };
+struct Cr2Scalars {
+    double F1, F2, Q, D;
+    long long IF1, IF2, IQ, ID;
+};
+
+template <class T>
+constexpr size_t cr2_smem() {
+    return 3 * 52 * MS * sizeof(T) + 52 * sizeof(CardAgg) + 52 * sizeof(CardCnt) + 52 * 16 +
+           sizeof(Cr2Scalars) + 64;
+}
 
 // Two counted opponents (1, 2) with combo matrices M1, M2, per-card sums
 // u_i = M_i 1, d(c) = sum_b M1[c][b] M2[c][b], w = M2 u1 + M1 u2,
@@ -345,16 +406,18 @@ struct alignas(16) CardCnt {
 //   - P[a][b] - P[b][a] + D
 // (inclusion-exclusion over shared cards), equal to the reference odometer
 // sum of street_solve.cu:771-823 / :1079-1127 for two opponents.
-__global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const TermItem *__restrict__ items,
-                                                           int trav) {
-    __shared__ __align__(16) float M1[52 * MS];
-    __shared__ __align__(16) float M2[52 * MS];
-    __shared__ __align__(16) float P[52 * MS];
-    __shared__ CardAgg agg[52];
-    __shared__ CardCnt cnt[52];
-    __shared__ ulonglong2 Bm[52];   // positive-reach masks of M1 (x) and M2 (y)
-    __shared__ double F1, F2, Q, D;
-    __shared__ long long IF1, IF2, IQ, ID;
+template <class T>
+__global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 6 : 2) k_term_cr2(DevCtx c, const TermItem *__restrict__ items,
+                                                              int trav) {
+    extern __shared__ __align__(16) char smem[];
+    Carve cv{smem};
+    T *M1 = cv.take<T>(52 * MS);
+    T *M2 = cv.take<T>(52 * MS);
+    T *P = cv.take<T>(52 * MS);
+    CardAgg *agg = cv.take<CardAgg>(52);
+    CardCnt *cnt = cv.take<CardCnt>(52);
+    ulonglong2 *Bm = cv.take<ulonglong2>(52);   // positive-reach masks of M1 (x) and M2 (y)
+    Cr2Scalars *sc = cv.take<Cr2Scalars>(1);
     const TermItem I = items[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwarp = blockDim.x / 32;
@@ -365,12 +428,11 @@ __global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const Te
     scatter_combo(c, I.opp_player[1], I.opp_row[1], M2);
     __syncthreads();
     for (int r = warp; r < 52; r += nwarp) {
-        double s1, s2;
+        double s1, s2, a0, a1, e0, e1;
         unsigned long long b1, b2;
-        float a0, a1, e0, e1;
         row_stats(M1, r, lane, &s1, &b1, &a0, &a1);
         row_stats(M2, r, lane, &s2, &b2, &e0, &e1);
-        const double sd = warp_sum(static_cast<double>(a0) * e0 + static_cast<double>(a1) * e1);
+        const double sd = warp_sum(a0 * e0 + a1 * e1);
         if (lane == 0) {
             agg[r].u1 = s1;
             agg[r].u2 = s2;
@@ -385,11 +447,11 @@ __global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const Te
     if (tid < 169) {
         // P = M1 M2 in 4x4 tiles; M1 is symmetric, so row b of M1 is column b
         const int i0 = (tid / 13) * 4, j0 = (tid % 13) * 4;
-        float acc[4][4] = {};
+        T acc[4][4] = {};
         for (int b = 0; b < 52; ++b) {
-            const float4 x = *reinterpret_cast<const float4 *>(&M1[b * MS + i0]);
-            const float4 y = *reinterpret_cast<const float4 *>(&M2[b * MS + j0]);
-            const float xs[4] = {x.x, x.y, x.z, x.w}, ys[4] = {y.x, y.y, y.z, y.w};
+            T xs[4], ys[4];
+            load4(&M1[b * MS + i0], xs);
+            load4(&M2[b * MS + j0], ys);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -397,8 +459,8 @@ __global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const Te
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            *reinterpret_cast<float4 *>(&P[(i0 + i) * MS + j0]) =
-                make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) P[(i0 + i) * MS + j0 + j] = acc[i][j];
     } else if (tid < 169 + 52) {
         const int col = tid - 169;
         double s = 0.0;
@@ -438,47 +500,54 @@ __global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const Te
             nd += __shfl_xor_sync(0xffffffffu, nd, o);
         }
         if (lane == 0) {
-            F1 = 0.5 * a1;
-            F2 = 0.5 * a2;
-            Q = q;
-            D = 0.5 * e;
-            IF1 = n1 / 2;
-            IF2 = n2 / 2;
-            IQ = nq;
-            ID = nd / 2;
+            sc->F1 = 0.5 * a1;
+            sc->F2 = 0.5 * a2;
+            sc->Q = q;
+            sc->D = 0.5 * e;
+            sc->IF1 = n1 / 2;
+            sc->IF2 = n2 / 2;
+            sc->IQ = nq;
+            sc->ID = nd / 2;
         }
     }
     __syncthreads();
+    const Cr2Scalars S = *sc;
     const int Ht = c.H[trav];
     const int *tc = c.hand_code + static_cast<size_t>(trav) * c.HS;
-    float *out = c.val + static_cast<size_t>(I.node) * c.HS;
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
     for (int h = tid; h < c.HS; h += blockDim.x) {
-        float v = 0.f;
+        double v = 0.0;
         if (h < Ht) {
             const int hc = tc[h];
             const int a = hc & 0xff, b = (hc >> 8) & 0xff;
             const ulonglong2 Ba = Bm[a], Bb = Bm[b];
             const CardCnt na = cnt[a], nb = cnt[b];
             const long long j1 = bit(Ba.x, b), j2 = bit(Ba.y, b);
-            const long long JA1 = IF1 - na.u1 - nb.u1 + j1, JA2 = IF2 - na.u2 - nb.u2 + j2;
-            const long long live = JA1 * JA2 - IQ + static_cast<long long>(na.u1) * na.u2 +
+            const long long JA1 = S.IF1 - na.u1 - nb.u1 + j1, JA2 = S.IF2 - na.u2 - nb.u2 + j2;
+            const long long live = JA1 * JA2 - S.IQ + static_cast<long long>(na.u1) * na.u2 +
                                    static_cast<long long>(nb.u1) * nb.u2 + na.w + nb.w -
                                    j2 * (na.u1 + nb.u1) - j1 * (na.u2 + nb.u2) - 2 * (na.d + nb.d) +
-                                   3 * j1 * j2 - (__popcll(Ba.x & Bb.y) + __popcll(Bb.x & Ba.y)) + ID;
+                                   3 * j1 * j2 - (__popcll(Ba.x & Bb.y) + __popcll(Bb.x & Ba.y)) + S.ID;
             if (live > 0) {
                 const CardAgg ga = agg[a], gb = agg[b];
                 const double m1 = M1[a * MS + b], m2 = M2[a * MS + b];
-                const double A1 = F1 - ga.u1 - gb.u1 + m1;
-                const double A2 = F2 - ga.u2 - gb.u2 + m2;
-                const double z = A1 * A2 - Q + ga.u1 * ga.u2 + gb.u1 * gb.u2 + ga.w + gb.w -
+                const double A1 = S.F1 - ga.u1 - gb.u1 + m1;
+                const double A2 = S.F2 - ga.u2 - gb.u2 + m2;
+                const double z = A1 * A2 - S.Q + ga.u1 * ga.u2 + gb.u1 * gb.u2 + ga.w + gb.w -
                                  m2 * (ga.u1 + gb.u1) - m1 * (ga.u2 + gb.u2) - 2.0 * (ga.d + gb.d) +
                                  3.0 * m1 * m2 -
-                                 (static_cast<double>(P[a * MS + b]) + static_cast<double>(P[b * MS + a])) + D;
-                v = static_cast<float>(static_cast<double>(term_factor(c, I, h)) * z);
+                                 (static_cast<double>(P[a * MS + b]) + static_cast<double>(P[b * MS + a])) +
+                                 S.D;
+                v = static_cast<double>(term_factor(c, I, h)) * z;
             }
         }
-        out[h] = v;
+        store_value(out, h, v);
     }
+}
+
+template <class T>
+constexpr size_t sd1_smem() {
+    return 1326 * sizeof(T) + 1327 * 8 + 52 * 53 * 8 + 52 * 4 + (kTermThreads / 32) * 8 + 52 * 8 + 64;
 }
 
 // Showdown against one live opponent (street_solve.cu:886-903): with W, T, S
@@ -492,23 +561,26 @@ __global__ void __launch_bounds__(kTermThreads, 6) k_term_cr2(DevCtx c, const Te
 //   S = P[end] - PC[c1][end] - PC[c2][end] + f(h)
 // A traverser hand with no compatible positive-reach opponent hand gets
 // exactly 0 (positive-reach masks per card, as in the two-opponent kernels).
+template <class T>
 __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermItem *__restrict__ items,
                                                            int trav) {
-    __shared__ float Rr[1326];
-    __shared__ double Pp[1327];
-    __shared__ double PC[52 * 53];
-    __shared__ int clen[52];
-    __shared__ double wsum[kTermThreads / 32];
-    __shared__ unsigned long long B[52];
-    __shared__ int npos;
+    extern __shared__ __align__(16) char smem[];
+    Carve cv{smem};
+    T *Rr = cv.take<T>(1326);
+    double *Pp = cv.take<double>(1327);
+    double *PC = cv.take<double>(52 * 53);
+    int *clen = cv.take<int>(52);
+    double *wsum = cv.take<double>(kTermThreads / 32);
+    unsigned long long *B = cv.take<unsigned long long>(52);
+    int *npos = cv.take<int>(1);
     const TermItem I = items[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nc = c.ncomb;
-    for (int i = tid; i < nc; i += blockDim.x) Rr[i] = 0.f;
+    for (int i = tid; i < nc; i += blockDim.x) Rr[i] = T(0);
     __syncthreads();
     {
         const int o = I.opp_player[0];
-        const float *r = c.reach + static_cast<size_t>(I.opp_row[0]) * c.HS;
+        const T *r = reach_rows<T>(c) + static_cast<size_t>(I.opp_row[0]) * c.HS;
         const int *pos = c.sd_pos + static_cast<size_t>(o) * c.HS;
         const bool dup = c.dup[o] != 0;
         for (int j = tid; j < c.H[o]; j += blockDim.x) {
@@ -555,7 +627,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
         const short *Pt = c.sd_card_partner + card * 52;
         const int i0 = 2 * lane, i1 = 2 * lane + 1;
         const int q0 = i0 < 52 ? L[i0] : -1, q1 = i1 < 52 ? L[i1] : -1;
-        const float f0 = q0 >= 0 ? Rr[q0] : 0.f, f1 = q1 >= 0 ? Rr[q1] : 0.f;
+        const T f0 = q0 >= 0 ? Rr[q0] : T(0), f1 = q1 >= 0 ? Rr[q1] : T(0);
         const double v0 = f0, v1 = f1;
         const double pair = v0 + v1;
         double incl = pair;
@@ -569,8 +641,8 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
         if (i0 <= len) PC[card * 53 + i0] = ex;
         if (i1 <= len) PC[card * 53 + i1] = ex + v0;
         unsigned long long m = 0ull;
-        if (f0 > 0.f) m |= 1ull << Pt[i0];
-        if (f1 > 0.f) m |= 1ull << Pt[i1];
+        if (f0 > T(0)) m |= 1ull << Pt[i0];
+        if (f1 > T(0)) m |= 1ull << Pt[i1];
         const unsigned lo = __reduce_or_sync(0xffffffffu, static_cast<unsigned>(m));
         const unsigned hi = __reduce_or_sync(0xffffffffu, static_cast<unsigned>(m >> 32));
         if (lane == 0) {
@@ -583,30 +655,31 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
         int n = __popcll(B[lane]) + (lane + 32 < 52 ? __popcll(B[lane + 32]) : 0);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-        if (lane == 0) npos = n / 2;
+        if (lane == 0) *npos = n / 2;
     }
     __syncthreads();
     const int Ht = c.H[trav];
     const int *tpos = c.sd_pos + static_cast<size_t>(trav) * c.HS;
-    float *out = c.val + static_cast<size_t>(I.node) * c.HS;
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
     const double pot = I.pot, bet = I.bet;
+    const int np_ = *npos;
     for (int h = tid; h < c.HS; h += blockDim.x) {
-        float v = 0.f;
+        double v = 0.0;
         const int q = h < Ht ? tpos[h] : -1;
         if (q >= 0) {
             const SdCombo s = c.sd_combo[q];
             const unsigned long long B1 = B[s.c1], B2 = B[s.c2];
-            if (npos - __popcll(B1) - __popcll(B2) + bit(B1, s.c2) > 0) {
+            if (np_ - __popcll(B1) - __popcll(B2) + bit(B1, s.c2) > 0) {
                 const double *p1 = PC + s.c1 * 53, *p2 = PC + s.c2 * 53;
                 const double self = Rr[q];
                 const double W = Pp[s.lo] - p1[s.l1lo] - p2[s.l2lo];
-                const double T = (Pp[s.hi] - Pp[s.lo]) - (p1[s.l1hi] - p1[s.l1lo]) -
-                                 (p2[s.l2hi] - p2[s.l2lo]) + self;
+                const double Tt = (Pp[s.hi] - Pp[s.lo]) - (p1[s.l1hi] - p1[s.l1lo]) -
+                                  (p2[s.l2hi] - p2[s.l2lo]) + self;
                 const double S = Pp[nc] - p1[clen[s.c1]] - p2[clen[s.c2]] + self;
-                v = static_cast<float>(pot * W + 0.5 * pot * T - bet * S);
+                v = pot * W + 0.5 * pot * Tt - bet * S;
             }
         }
-        out[h] = v;
+        store_value(out, h, v);
     }
 }
 
@@ -615,6 +688,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
 // (street_solve.cu:771-823 fold, :936-1002 showdown, :1079-1127 leaf).  Cost
 // is the product of the opponents' range sizes; the planner only routes small
 // cases here.
+template <class T>
 __global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__restrict__ items,
                                                    int nchunk, int trav) {
     const int it = blockIdx.x / nchunk;
@@ -622,10 +696,11 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__r
     const int h = ch * blockDim.x + threadIdx.x;
     if (h >= c.HS) return;
     const TermItem I = items[it];
-    float *out = c.val + static_cast<size_t>(I.node) * c.HS;
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
+    const T *reach = reach_rows<T>(c);
     const int Ht = c.H[trav];
     if (h >= Ht) {
-        out[h] = 0.f;
+        out[h] = T(0);
         return;
     }
     const size_t HS = static_cast<size_t>(c.HS);
@@ -637,17 +712,17 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__r
     if (sd) {
         hs = c.strength[trav * HS + h];
         if (hs == 0) {
-            out[h] = 0.f;
+            out[h] = T(0);
             return;
         }
     }
     int idx[SS_MAX_PLAYERS - 1] = {0, 0, 0, 0, 0};
-    float total = 0.f;
-    const float pot = I.pot, tb = I.bet;
+    T total = T(0);
+    const T pot = I.pot, tb = I.bet;
     for (;;) {
         int cards[SS_MAX_PLAYERS - 1][2];
         unsigned os[SS_MAX_PLAYERS - 1];
-        float prod = 1.0f;
+        T prod = T(1);
         bool ok = true;
         for (int i = 0; i < k && ok; ++i) {
             const int p = I.opp_player[i], o = idx[i];
@@ -663,14 +738,14 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__r
                 ok = false;
                 break;
             }
-            prod *= c.reach[static_cast<size_t>(I.opp_row[i]) * HS + o];
+            prod *= reach[static_cast<size_t>(I.opp_row[i]) * HS + o];
             for (int j = 0; j < i; ++j)
                 if (a0 == cards[j][0] || a0 == cards[j][1] || a1 == cards[j][0] || a1 == cards[j][1]) {
                     ok = false;
                     break;
                 }
         }
-        if (ok && prod > 0.f) {
+        if (ok && prod > T(0)) {
             if (!sd) {
                 total += prod;
             } else {
@@ -681,7 +756,7 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__r
                 } else {
                     int wins = 1;
                     for (int i = 0; i < k; ++i) wins += os[i] == best ? 1 : 0;
-                    total += prod * (pot / static_cast<float>(wins) - tb);
+                    total += prod * (pot / static_cast<T>(wins) - tb);
                 }
             }
         }
@@ -693,7 +768,86 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__r
         }
         if (j < 0) break;
     }
-    out[h] = sd ? total : term_factor(c, I, h) * total;
+    out[h] = sd ? total : static_cast<T>(term_factor(c, I, h)) * total;
+}
+
+// --------------------------------------------------------------------------
+// best response (FP64): exploitability of an average-strategy profile
+// avg[(di * 8 + a) * max_h + h] (the SSOutput layout)
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ double avg_sigma(const float *avg, int di, int a, int h, int max_h, int frozen) {
+    if (frozen >= 0) return a == frozen ? 1.0 : 0.0;
+    return static_cast<double>(avg[(static_cast<size_t>(di) * SS_MAX_ACTIONS + a) * max_h + h]);
+}
+
+// reach of one player under the average strategy
+__global__ void __launch_bounds__(128) k_br_reach(DevCtx c, const ReachItem *__restrict__ items, int nchunk,
+                                                  int H, const float *__restrict__ avg,
+                                                  const int *__restrict__ edge_di, int max_h) {
+    const int it = blockIdx.x / nchunk;
+    const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
+    if (h >= H) return;
+    const ReachItem I = items[it];
+    const size_t HS = static_cast<size_t>(c.HS);
+    const int di = edge_di[I.first_edge];
+    const double pr = c.reach_d[static_cast<size_t>(I.parent_row) * HS + h];
+    for (int a = 0; a < I.na; ++a)
+        c.reach_d[static_cast<size_t>(I.first_edge + a) * HS + h] = pr * avg_sigma(avg, di, a, h, max_h, I.frozen);
+}
+
+// value of the traverser's nodes: mode 0 follows the profile, mode 1 takes
+// the best action (a pure best response per information set; a frozen node
+// keeps its frozen action)
+__global__ void __launch_bounds__(128) k_br_value(DevCtx c, const CfvItem *__restrict__ items, int nchunk,
+                                                  int H, const float *__restrict__ avg,
+                                                  const int *__restrict__ edge_di, int max_h, int mode) {
+    const int it = blockIdx.x / nchunk;
+    const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
+    if (h >= H) return;
+    const CfvItem I = items[it];
+    const size_t HS = static_cast<size_t>(c.HS);
+    const int di = edge_di[I.first_edge];
+    double v = mode == 1 ? -1e300 : 0.0;
+    double vf = 0.0;
+    for (int a = 0; a < I.na; ++a) {
+        double e = 0.0;
+        for (int k = c.fr_off[I.first_edge + a]; k < c.fr_off[I.first_edge + a + 1]; ++k)
+            e += c.val_d[static_cast<size_t>(c.fr_items[k]) * HS + h];
+        if (mode == 1) {
+            v = e > v ? e : v;
+            if (a == I.frozen) vf = e;
+        } else {
+            v += avg_sigma(avg, di, a, h, max_h, I.frozen) * e;
+        }
+    }
+    if (mode == 1 && I.frozen >= 0 && I.frozen < I.na) v = vf;
+    c.val_d[static_cast<size_t>(I.node) * HS + h] = v;
+}
+
+// out = sum over hands h < H of weight(h) * (sum over rows of val_d[row][h]);
+// the weights are the traverser's range (reach_d row weight_row); with
+// skip_blocked, hands touching the board do not count.  One block, fixed
+// reduction order.
+__global__ void __launch_bounds__(1024) k_br_root(DevCtx c, const int *__restrict__ rows, int n, int H,
+                                                  int weight_row, int trav, int skip_blocked, double *out) {
+    __shared__ double part[32];
+    const size_t HS = static_cast<size_t>(c.HS);
+    double acc = 0.0;
+    for (int h = threadIdx.x; h < H; h += blockDim.x) {
+        if (skip_blocked && (c.hand_code[trav * HS + h] & 0x10000)) continue;
+        double s = 0.0;
+        for (int k = 0; k < n; ++k) s += c.val_d[static_cast<size_t>(rows[k]) * HS + h];
+        acc += c.reach_d[static_cast<size_t>(weight_row) * HS + h] * s;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < blockDim.x / 32 ? part[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) *out = v;
+    }
 }
 
 __global__ void k_bump(int *iter) { *iter += 1; }
@@ -766,34 +920,54 @@ cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cuda
     return cudaGetLastError();
 }
 
-cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                         cudaStream_t s) {
+template <class T>
+cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
+                           cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
     switch (kind) {
         case TK_ZERO:
         case TK_LEAF0: {
             const int nc = chunks(c.HS);
-            k_term_fill<<<n * nc, kHandThreads, 0, s>>>(c, items, nc, trav, kind == TK_ZERO);
+            k_term_fill<T><<<n * nc, kHandThreads, 0, s>>>(c, items, nc, trav, kind == TK_ZERO);
             break;
         }
         case TK_CR1:
-            k_term_cr1<<<n, kTermThreads, 0, s>>>(c, items, trav);
+            k_term_cr1<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, items, trav);
             break;
         case TK_CR2:
-            k_term_cr2<<<n, kTermThreads, 0, s>>>(c, items, trav);
+            if (cr2_smem<T>() > 48 * 1024)
+                e = cudaFuncSetAttribute(k_term_cr2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(cr2_smem<T>()));
+            if (e != cudaSuccess) return e;
+            k_term_cr2<T><<<n, kTermThreads, cr2_smem<T>(), s>>>(c, items, trav);
             break;
         case TK_SD1:
-            k_term_sd1<<<n, kTermThreads, 0, s>>>(c, items, trav);
+            if (sd1_smem<T>() > 48 * 1024)
+                e = cudaFuncSetAttribute(k_term_sd1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(sd1_smem<T>()));
+            if (e != cudaSuccess) return e;
+            k_term_sd1<T><<<n, kTermThreads, sd1_smem<T>(), s>>>(c, items, trav);
             break;
         case TK_ENUM: {
             const int nc = (c.HS + 127) / 128;
-            k_term_enum<<<n * nc, 128, 0, s>>>(c, items, nc, trav);
+            k_term_enum<T><<<n * nc, 128, 0, s>>>(c, items, nc, trav);
             break;
         }
         default:
             return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
+                         cudaStream_t s) {
+    return launch_terms_t<float>(c, kind, items, n, trav, s);
+}
+
+cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
+                              cudaStream_t s) {
+    return launch_terms_t<double>(c, kind, items, n, trav, s);
 }
 
 cudaError_t launch_bump(int *iter, cudaStream_t s) {
@@ -822,6 +996,28 @@ cudaError_t launch_avg_strategy(const DevCtx &c, const int *dec_fe, const int *d
     if (num_dec <= 0) return cudaSuccess;
     const int nc = (max_h + 127) / 128;
     k_avg_strategy<<<num_dec * nc, 128, 0, s>>>(c, dec_fe, dec_na, dec_player, nc, max_h, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_br_reach(const DevCtx &c, const ReachItem *items, int n, int H, const float *avg,
+                            const int *edge_di, int max_h, cudaStream_t s) {
+    if (n <= 0 || H <= 0) return cudaSuccess;
+    const int nc = (H + 127) / 128;
+    k_br_reach<<<n * nc, 128, 0, s>>>(c, items, nc, H, avg, edge_di, max_h);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_br_value(const DevCtx &c, const CfvItem *items, int n, int H, const float *avg,
+                            const int *edge_di, int max_h, int mode, cudaStream_t s) {
+    if (n <= 0 || H <= 0) return cudaSuccess;
+    const int nc = (H + 127) / 128;
+    k_br_value<<<n * nc, 128, 0, s>>>(c, items, nc, H, avg, edge_di, max_h, mode);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_br_root(const DevCtx &c, const int *rows, int n, int H, int weight_row, int trav,
+                           int skip_blocked, double *out, cudaStream_t s) {
+    k_br_root<<<1, 1024, 0, s>>>(c, rows, n, H, weight_row, trav, skip_blocked, out);
     return cudaGetLastError();
 }
 

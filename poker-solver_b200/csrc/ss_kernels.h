@@ -13,6 +13,8 @@ struct DevCtx {
     float *S;              // strategy sums      [E][HS]
     float *reach;          // reach per sequence [E + np][HS]
     float *val;            // node values        [N][HS]
+    double *reach_d;       // best response: reach under the average strategy [E + np][HS]
+    double *val_d;         // best response: node values [N + 1][HS]
     const int *fr_off;     // [E + 1]
     const int *fr_items;
     const int *hand_code;  // [np][HS]
@@ -42,7 +44,15 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s);
+cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
+                              cudaStream_t s);
 cudaError_t launch_bump(int *iter, cudaStream_t s);
+cudaError_t launch_br_reach(const DevCtx &c, const ReachItem *items, int n, int H, const float *avg,
+                            const int *edge_di, int max_h, cudaStream_t s);
+cudaError_t launch_br_value(const DevCtx &c, const CfvItem *items, int n, int H, const float *avg,
+                            const int *edge_di, int max_h, int mode, cudaStream_t s);
+cudaError_t launch_br_root(const DevCtx &c, const int *rows, int n, int H, int weight_row, int trav,
+                           int skip_blocked, double *out, cudaStream_t s);
 cudaError_t launch_sum_rows(const DevCtx &c, const int *rows, int n, float *out, int H,
                             cudaStream_t s);
 cudaError_t launch_root_strategy(const DevCtx &c, int first_edge, int na, int frozen, int H,

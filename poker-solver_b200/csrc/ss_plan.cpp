@@ -137,6 +137,7 @@ int build_plan(const Problem &pb, Plan *out) {
     }
     P.root_player = nd[0].player;
     P.root_na = nd[0].num_children;
+    P.starting_pot = pb.starting_pot;
 
     // edges in BFS order
     P.first_edge.assign(N, -1);
