@@ -34,10 +34,11 @@ thread_local std::string g_err;
 
 struct Blob {
     std::vector<char> host;
+    // append bytes at the next 256-byte boundary; a null source reserves zeros
     size_t add(const void *src, size_t bytes) {
         size_t off = (host.size() + 255) & ~static_cast<size_t>(255);
         host.resize(off + bytes);
-        if (bytes) std::memcpy(host.data() + off, src, bytes);
+        if (bytes && src) std::memcpy(host.data() + off, src, bytes);
         return off;
     }
     template <class T>
