@@ -153,6 +153,17 @@ typedef struct {
     double node_hand_updates;     /* num_nodes x sum of hand counts x iterations */
 } SSSolveStats;
 
+/* Served form: continuous batching of solve requests on one GPU. */
+typedef struct {
+    int device;                   /* CUDA device ordinal */
+    double memory_budget_gb;      /* admit requests while their estimated device footprint fits */
+    int block_iterations;         /* iterations between exploitability checks (default 25) */
+    float target_exploitability;  /* retire a request at this exploitability, % of pot (default 0.5) */
+    int max_iterations;           /* ... or after this many iterations (default 1000) */
+    int graph_iterations;         /* iterations per captured CUDA graph (default 25) */
+} SSServerOptions;
+typedef struct SSServer SSServer;
+
 /* A resident subgame: plan, device state and captured CUDA graphs stay on the
  * GPU between calls, so iterations can be added, the state reset or the
  * outputs read without re-uploading anything. */
@@ -294,6 +305,40 @@ int ss_rank7_checksum(unsigned long long *checksum, unsigned long long *category
  * share the array and it keeps the previous call's data (each call rewrites
  * what it reads); calls that overlap on the same GPU race. */
 int ss_solve_gpu_noalloc(SSTreeData *tree_data, int max_iterations, SSOutput *output);
+
+/* EXTENSION (batched form): solve n subgames of any size, street and player
+ * count together -- each kernel launch covers one tree level of every
+ * subgame.  With opts->target_exploitability > 0 each subgame is checked every
+ * opts->check_every iterations and leaves the batch once its FP64
+ * exploitability is at or below the target (or at max_iterations); otherwise
+ * every subgame runs max_iterations.  outputs[i] / stats[i] (stats may be
+ * NULL) are filled as by ss_solve_gpu_ex; free each output with
+ * ss_free_output.  Per subgame, the arithmetic is the same as a solve alone. */
+int ss_batch_solve(SSTreeData *const *trees, int n, int max_iterations, const SSSolveOptions *opts,
+                   SSOutput *outputs, SSSolveStats *stats);
+
+/* EXTENSION (served form): default server options. */
+void ss_server_default_options(SSServerOptions *opts);
+
+/* EXTENSION: start a server (a worker thread driving one batch on the device). */
+int ss_server_create(const SSServerOptions *opts, SSServer **out);
+
+/* EXTENSION: queue a solve request; the tree, ranges, leaf values and frozen
+ * actions are copied, so the caller may free them on return. */
+int ss_server_submit(SSServer *server, const SSTreeData *tree_data, long long *request_id);
+
+/* EXTENSION: 0 = done (fills *output, free it with ss_free_output; *stats and
+ * *latency_ms from submission to retirement, all optional), 1 = still queued
+ * or running, < 0 = failed (the request is dropped). */
+int ss_server_poll(SSServer *server, long long request_id, SSOutput *output, SSSolveStats *stats,
+                   double *latency_ms);
+
+/* EXTENSION: like ss_server_poll but blocks until the request is done. */
+int ss_server_wait(SSServer *server, long long request_id, SSOutput *output, SSSolveStats *stats,
+                   double *latency_ms);
+
+/* EXTENSION: stop the worker and release the server (unfetched results too). */
+void ss_server_destroy(SSServer *server);
 
 /* EXTENSION: message for the last failure on the calling thread ("" if none). */
 const char *ss_last_error(void);

@@ -59,6 +59,10 @@ struct SSSession {
     ssb::Session *impl;
 };
 
+struct SSServer {
+    ssb::Server *impl;
+};
+
 extern "C" {
 
 int ss_build_tree_ex(const int *board, int num_board, int starting_pot, int effective_stack,
@@ -319,6 +323,91 @@ int ss_rank7_batch(const int *cards7, int n, unsigned int *strength_out) {
 int ss_rank7_checksum(unsigned long long *checksum, unsigned long long *category_counts) {
     if (!checksum) return SS_ERR_INVALID;
     return ssb::rank7_checksum(checksum, category_counts);
+}
+
+int ss_batch_solve(SSTreeData *const *trees, int n, int max_iterations, const SSSolveOptions *opts,
+                   SSOutput *outputs, SSSolveStats *stats) {
+    if (!trees || !outputs || n < 0) {
+        ssb::set_error("ss_batch_solve: bad arguments");
+        return SS_ERR_INVALID;
+    }
+    try {
+        std::vector<ssb::Problem> pbs(n);
+        for (int i = 0; i < n; ++i) {
+            int rc = to_problem(trees[i], &pbs[i]);
+            if (rc != SS_OK) return rc;
+        }
+        SSSolveOptions o;
+        ss_default_options(&o);
+        if (opts) o = *opts;
+        ssb::SolveConfig cfg;
+        cfg.device = o.device;
+        cfg.graph_iterations = o.graph_iterations;
+        cfg.target_exploitability = o.target_exploitability;
+        cfg.check_every = o.check_every;
+        cfg.compute_exploitability = o.compute_exploitability;
+        return ssb::batch_solve(pbs, max_iterations, cfg, outputs, stats);
+    } catch (const std::bad_alloc &) {
+        ssb::set_error("out of host memory");
+        return SS_ERR_NOMEM;
+    }
+}
+
+void ss_server_default_options(SSServerOptions *o) {
+    if (!o) return;
+    o->device = 0;
+    o->memory_budget_gb = 40.0;
+    o->block_iterations = 25;
+    o->target_exploitability = 0.5f;
+    o->max_iterations = 1000;
+    o->graph_iterations = 25;
+}
+
+int ss_server_create(const SSServerOptions *opts, SSServer **out) {
+    if (!out) return SS_ERR_INVALID;
+    *out = nullptr;
+    SSServerOptions o;
+    ss_server_default_options(&o);
+    if (opts) o = *opts;
+    try {
+        ssb::Server *s = nullptr;
+        int rc = ssb::server_create(o, &s);
+        if (rc != SS_OK) return rc;
+        *out = new SSServer{s};
+        return SS_OK;
+    } catch (const std::exception &) {
+        ssb::set_error("could not start the server");
+        return SS_ERR_NOMEM;
+    }
+}
+
+int ss_server_submit(SSServer *s, const SSTreeData *td, long long *id) {
+    if (!s || !id) return SS_ERR_INVALID;
+    ssb::Problem pb;
+    int rc = to_problem(td, &pb);
+    if (rc != SS_OK) return rc;
+    try {
+        return ssb::server_submit(s->impl, pb, id);
+    } catch (const std::bad_alloc &) {
+        ssb::set_error("out of host memory");
+        return SS_ERR_NOMEM;
+    }
+}
+
+int ss_server_poll(SSServer *s, long long id, SSOutput *out, SSSolveStats *stats, double *latency_ms) {
+    if (!s) return SS_ERR_INVALID;
+    return ssb::server_poll(s->impl, id, out, stats, latency_ms, 0);
+}
+
+int ss_server_wait(SSServer *s, long long id, SSOutput *out, SSSolveStats *stats, double *latency_ms) {
+    if (!s) return SS_ERR_INVALID;
+    return ssb::server_poll(s->impl, id, out, stats, latency_ms, 1);
+}
+
+void ss_server_destroy(SSServer *s) {
+    if (!s) return;
+    ssb::server_destroy(s->impl);
+    delete s;
 }
 
 const char *ss_last_error(void) { return ssb::last_error(); }

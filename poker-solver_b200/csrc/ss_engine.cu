@@ -15,7 +15,7 @@
 //     a CUDA graph and replayed; the iteration number lives on the device;
 //   * plan, tables and state stay resident in a Session, so a solve can be
 //     extended, reset or read without re-uploading.
-#include "ss_kernels.h"
+#include "ss_session.h"
 
 #include <cuda_runtime.h>
 
@@ -60,24 +60,8 @@ void keep_pool_warm(int device) {
     done[device] = true;
 }
 
-// tuple visits of the enumeration kernel that one solve may spend
-constexpr double kEnumLimitPerIter = 4e9;
-constexpr double kEnumLimitTotal = 2e11;
-
-enum ProfClass { PC_REACH = 0, PC_CFV, PC_FILL, PC_CR1, PC_CR2, PC_SD1, PC_ENUM, PC_OTHER };
 const char *kClassName[SS_PROFILE_CLASSES] = {"reach", "cfv", "term_fill", "term_cr1",
                                              "term_cr2", "term_sd1", "term_enum", "other"};
-
-int term_class(int kind) {
-    switch (kind) {
-        case TK_ZERO:
-        case TK_LEAF0: return PC_FILL;
-        case TK_CR1: return PC_CR1;
-        case TK_CR2: return PC_CR2;
-        case TK_SD1: return PC_SD1;
-        default: return PC_ENUM;
-    }
-}
 
 }  // namespace
 
@@ -93,143 +77,6 @@ const char *last_error() { return g_err.c_str(); }
         }                                                                             \
     } while (0)
 
-class Session {
-  public:
-    Plan P;
-    int device = 0;
-    int graph_iters = 10;
-    int iterations = 0;
-    cudaStream_t stream = nullptr;
-    char *dbase = nullptr;    // static tables
-    float *dstate = nullptr;  // R, S, reach, val
-    float *dleaf = nullptr;
-    float *dsmall = nullptr;  // root strategy snapshot + root values
-    int *diter = nullptr;
-    size_t nR = 0, nReach = 0, nVal = 0, n_rs = 0;
-    int frozen_root = -1;
-    DevCtx c{};
-    const ReachItem *reach_items[SS_MAX_PLAYERS] = {};
-    std::vector<std::pair<int, int>> reach_lv[SS_MAX_PLAYERS];
-    const CfvItem *cfv_items[SS_MAX_PLAYERS] = {};
-    std::vector<std::pair<int, int>> cfv_lv[SS_MAX_PLAYERS];
-    const TermItem *term_items[SS_MAX_PLAYERS][TK_COUNT] = {};
-    const int *root_fr[SS_MAX_PLAYERS] = {};
-    const int *dec_fe = nullptr, *dec_na = nullptr, *dec_pl = nullptr;
-    // per (player, level) / (traverser, kind) minimum bytes, for the profile
-    std::vector<double> reach_bytes[SS_MAX_PLAYERS], cfv_bytes[SS_MAX_PLAYERS];
-    double term_bytes[SS_MAX_PLAYERS][TK_COUNT] = {};
-    cudaGraphExec_t gA = nullptr, gC = nullptr, gB = nullptr;  // G iters, 1 iter, 1 iter + snapshot
-    // best response state (allocated on first use)
-    std::vector<float> host_w;          // range weights [np][HS]
-    double *dbr = nullptr;              // reach_d [E + np][HS], val_d [N + 1][HS]
-    char *dbr_tab = nullptr;            // edge -> decision index, deal item, row list, scalars
-    float *davg_br = nullptr;           // profile in the output layout
-
-    // profiling hook: when set, every launch is preceded by an event record
-    struct Mark {
-        int cls;
-        double bytes;
-        cudaEvent_t ev;
-    };
-    std::vector<Mark> *marks = nullptr;
-
-    ~Session() {
-        if (gA) cudaGraphExecDestroy(gA);
-        if (gB) cudaGraphExecDestroy(gB);
-        if (gC) cudaGraphExecDestroy(gC);
-        if (stream) {
-            if (dbase) cudaFreeAsync(dbase, stream);
-            if (dstate) cudaFreeAsync(dstate, stream);
-            if (dleaf) cudaFreeAsync(dleaf, stream);
-            if (dsmall) cudaFreeAsync(dsmall, stream);
-            if (diter) cudaFreeAsync(diter, stream);
-            if (dbr) cudaFreeAsync(dbr, stream);
-            if (dbr_tab) cudaFreeAsync(dbr_tab, stream);
-            if (davg_br) cudaFreeAsync(davg_br, stream);
-            cudaStreamSynchronize(stream);
-            cudaStreamDestroy(stream);
-        }
-    }
-
-    cudaError_t mark(int cls, double bytes) {
-        if (!marks) return cudaSuccess;
-        Mark m{cls, bytes, nullptr};
-        cudaError_t e = cudaEventCreate(&m.ev);
-        if (e != cudaSuccess) return e;
-        marks->push_back(m);
-        // an external record becomes an event-record node of the captured graph
-        return cudaEventRecordWithFlags(m.ev, stream, cudaEventRecordExternal);
-    }
-
-    cudaError_t reach(int p) {
-        for (size_t l = 0; l < reach_lv[p].size(); ++l) {
-            cudaError_t e = mark(PC_REACH, reach_bytes[p][l]);
-            if (e == cudaSuccess)
-                e = launch_reach(c, reach_items[p] + reach_lv[p][l].first, reach_lv[p][l].second,
-                                 P.H[p], stream);
-            if (e != cudaSuccess) return e;
-        }
-        return cudaSuccess;
-    }
-
-    cudaError_t pass(int t, bool snapshot_root) {
-        cudaError_t e = cudaSuccess;
-        if (snapshot_root) {
-            e = mark(PC_OTHER, 0);
-            if (e == cudaSuccess)
-                e = launch_root_strategy(c, P.first_edge[0], P.root_na, frozen_root,
-                                         P.H[P.root_player], dsmall, stream);
-            if (e != cudaSuccess) return e;
-        }
-        for (int k = 0; k < TK_COUNT; ++k) {
-            const int n = static_cast<int>(P.term[t][k].size());
-            if (n == 0) continue;
-            e = mark(term_class(k), term_bytes[t][k]);
-            if (e == cudaSuccess) e = launch_terms(c, k, term_items[t][k], n, t, stream);
-            if (e != cudaSuccess) return e;
-        }
-        for (size_t l = 0; l < cfv_lv[t].size(); ++l) {
-            e = mark(PC_CFV, cfv_bytes[t][l]);
-            if (e == cudaSuccess)
-                e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.H[t],
-                               stream);
-            if (e != cudaSuccess) return e;
-        }
-        return reach(t);
-    }
-
-    cudaError_t iteration(bool last) {
-        cudaError_t e = mark(PC_OTHER, 0);
-        if (e == cudaSuccess) e = launch_bump(diter, stream);
-        for (int t = 0; t < P.np && e == cudaSuccess; ++t) e = pass(t, last && t == P.np - 1);
-        return e;
-    }
-
-    cudaError_t capture(int iters, bool last, cudaGraphExec_t *exec) {
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return e;
-        cudaError_t body = cudaSuccess;
-        for (int i = 0; i < iters && body == cudaSuccess; ++i) body = iteration(last && i == iters - 1);
-        e = cudaStreamEndCapture(stream, &g);
-        if (body != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return body;
-        }
-        if (e != cudaSuccess) return e;
-        e = cudaGraphInstantiate(exec, g, 0);
-        cudaGraphDestroy(g);
-        return e;
-    }
-
-    int init(const Problem &pb, const SolveConfig &cfg);
-    int exploitability(const float *host_avg, double *pct, double *nash, double *br, double *cur,
-                       double *deal_mass);
-    int reset();
-    int run(int iters);
-    int output(SSOutput *out);
-    int profile(SSKernelProfile *prof);
-};
 
 int Session::init(const Problem &pb, const SolveConfig &cfg) {
     int rc = build_plan(pb, &P);
@@ -372,6 +219,11 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
         c.dup[p] = p < np ? P.dup[p] : 0;
     }
     frozen_root = pb.frozen ? pb.frozen[0] : -1;
+    c.snap = dsmall;
+    c.root_fe = P.first_edge[0];
+    c.root_na = P.root_na;
+    c.root_frozen = frozen_root;
+    c.root_player = P.root_player;
     return reset();
 }
 

@@ -70,6 +70,8 @@ struct alignas(16) ReachItem {
     int na;
     int parent_row;
     int frozen;
+    int sg = 0;               // subgame of a batch (0 for a single subgame)
+    int pad_[3] = {0, 0, 0};
 };
 
 // Bottom-up value and regret update at one traverser decision node; the value
@@ -79,6 +81,8 @@ struct alignas(16) CfvItem {
     int na;
     int frozen;
     int node;
+    int sg = 0;               // subgame of a batch (0 for a single subgame)
+    int pad_[3] = {0, 0, 0};
 };
 
 // Terminal kinds per traverser.
@@ -102,7 +106,7 @@ struct alignas(16) TermItem {
     float payoff;
     float pot;
     float bet;
-    int pad;
+    int sg;                   // subgame of a batch (0 for a single subgame)
     int opp_row[SS_MAX_PLAYERS - 1];
     int opp_player[SS_MAX_PLAYERS - 1];
     int pad2[2];
@@ -191,6 +195,15 @@ void session_destroy(Session *s);
 void *session_stream(Session *s);
 int session_exploitability(Session *s, const float *host_avg, double *pct, double *nash, double *br,
                            double *cur, double *z);
+
+// ss_batch.cu: batched and served forms
+int batch_solve(const std::vector<Problem> &pbs, int max_iterations, const SolveConfig &cfg, SSOutput *outs,
+                SSSolveStats *stats);
+class Server;
+int server_create(const SSServerOptions &o, Server **out);
+int server_submit(Server *s, const Problem &pb, long long *id);
+int server_poll(Server *s, long long id, SSOutput *out, SSSolveStats *stats, double *latency_ms, int wait);
+void server_destroy(Server *s);
 
 // ss_noalloc.cu: solve with all device state in a static device array
 int solve_noalloc(const Problem &pb, int iterations, SSOutput *out);

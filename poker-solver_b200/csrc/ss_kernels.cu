@@ -74,13 +74,15 @@ __device__ __forceinline__ void regret_match4(const float *__restrict__ R, size_
 // reach: reach[first_edge + a] = reach[parent_row] * sigma_a
 // (street_solve.cu:650-683, stored per sequence instead of per node)
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c, const ReachItem *__restrict__ items,
-                                                        int nchunk, int H) {
+__global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                        const ReachItem *__restrict__ items, int nchunk, int H,
+                                                        int p) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
-    if (h0 >= H) return;
     const ReachItem I = items[it];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    if (h0 >= (ctxs ? c.H[p] : H)) return;
     const size_t HS = static_cast<size_t>(c.HS);
     float r[SS_MAX_ACTIONS][4], sig[SS_MAX_ACTIONS][4];
     regret_match4(c.R, HS, I.first_edge, I.na, I.frozen, h0, r, sig);
@@ -109,13 +111,16 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c, const ReachIte
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
 
-__global__ void __launch_bounds__(kCfvThreads) k_cfv(DevCtx c, const CfvItem *__restrict__ items,
-                                                     int nchunk, int H) {
+__global__ void __launch_bounds__(kCfvThreads) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                     const CfvItem *__restrict__ items, int nchunk, int Hl,
+                                                     int trav) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kCfvThreads + threadIdx.x) * 2;
-    if (h0 >= H) return;
     const CfvItem I = items[it];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    const int H = ctxs ? c.H[trav] : Hl;
+    if (h0 >= H) return;
     const size_t HS = static_cast<size_t>(c.HS);
     const float *val = c.val + h0;
     float2 ev[SS_MAX_ACTIONS];
@@ -210,13 +215,15 @@ template <> __device__ __forceinline__ double *val_rows<double>(const DevCtx &c)
 // value rows of terminals with no opponent coupling: zero, or the factor itself
 // (a leaf without a live opponent, street_solve.cu:1062-1065)
 template <class T>
-__global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c, const TermItem *__restrict__ items,
-                                                            int nchunk, int trav, int zero) {
+__global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                            const TermItem *__restrict__ items, int nchunk,
+                                                            int trav, int zero) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
-    if (h0 >= c.HS) return;
     const TermItem I = items[it];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    if (h0 >= c.HS) return;
     const int Ht = c.H[trav];
     T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS + h0;
 #pragma unroll
@@ -259,10 +266,6 @@ __device__ __forceinline__ void zero_matrix(T *M) {
 }
 
 // four consecutive matrix entries (16-byte aligned)
-__device__ __forceinline__ void load4(const float *p, double v[4]) {
-    const float4 x = *reinterpret_cast<const float4 *>(p);
-    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-}
 __device__ __forceinline__ void load4(const double *p, double v[4]) {
     const double2 x = *reinterpret_cast<const double2 *>(p);
     const double2 y = *reinterpret_cast<const double2 *>(p + 2);
@@ -318,8 +321,8 @@ constexpr size_t cr1_smem() {
 // traverser's own combo.  Folds: payoff * mass (street_solve.cu:745-761);
 // leaves: leaf value * mass (:1047-1066).
 template <class T>
-__global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermItem *__restrict__ items,
-                                                           int trav) {
+__global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                           const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
     Carve cv{smem};
     T *M = cv.take<T>(52 * MS);
@@ -328,6 +331,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c, const TermI
     double *F = cv.take<double>(1);
     int *npos = cv.take<int>(1);
     const TermItem I = items[blockIdx.x];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     zero_matrix(M);
     __syncthreads();
@@ -407,8 +411,8 @@ constexpr size_t cr2_smem() {
 // (inclusion-exclusion over shared cards), equal to the reference odometer
 // sum of street_solve.cu:771-823 / :1079-1127 for two opponents.
 template <class T>
-__global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 6 : 2) k_term_cr2(DevCtx c, const TermItem *__restrict__ items,
-                                                              int trav) {
+__global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 6 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                              const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
     Carve cv{smem};
     T *M1 = cv.take<T>(52 * MS);
@@ -419,6 +423,7 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 6 : 2) k_term_c
     ulonglong2 *Bm = cv.take<ulonglong2>(52);   // positive-reach masks of M1 (x) and M2 (y)
     Cr2Scalars *sc = cv.take<Cr2Scalars>(1);
     const TermItem I = items[blockIdx.x];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwarp = blockDim.x / 32;
     zero_matrix(M1);
@@ -562,8 +567,8 @@ constexpr size_t sd1_smem() {
 // A traverser hand with no compatible positive-reach opponent hand gets
 // exactly 0 (positive-reach masks per card, as in the two-opponent kernels).
 template <class T>
-__global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermItem *__restrict__ items,
-                                                           int trav) {
+__global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                           const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
     Carve cv{smem};
     T *Rr = cv.take<T>(1326);
@@ -574,6 +579,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
     unsigned long long *B = cv.take<unsigned long long>(52);
     int *npos = cv.take<int>(1);
     const TermItem I = items[blockIdx.x];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nc = c.ncomb;
     for (int i = tid; i < nc; i += blockDim.x) Rr[i] = T(0);
@@ -689,13 +695,14 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c, const TermI
 // is the product of the opponents' range sizes; the planner only routes small
 // cases here.
 template <class T>
-__global__ void __launch_bounds__(128) k_term_enum(DevCtx c, const TermItem *__restrict__ items,
-                                                   int nchunk, int trav) {
+__global__ void __launch_bounds__(128) k_term_enum(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                   const TermItem *__restrict__ items, int nchunk, int trav) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int h = ch * blockDim.x + threadIdx.x;
-    if (h >= c.HS) return;
     const TermItem I = items[it];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    if (h >= c.HS) return;
     T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
     const T *reach = reach_rows<T>(c);
     const int Ht = c.H[trav];
@@ -850,6 +857,27 @@ __global__ void __launch_bounds__(1024) k_br_root(DevCtx c, const int *__restric
     }
 }
 
+// batched form: advance the iteration counter of every listed subgame
+__global__ void k_bump_many(const DevCtx *__restrict__ ctxs, const int *__restrict__ sgs, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) *const_cast<int *>(ctxs[sgs[i]].iter) += 1;
+}
+
+// batched form: root strategy snapshot (regret matching of the root node)
+// of every listed subgame, one block per subgame, into its ctx.snap
+__global__ void __launch_bounds__(128) k_snapshot_many(const DevCtx *__restrict__ ctxs,
+                                                       const int *__restrict__ sgs) {
+    const DevCtx &c = ctxs[sgs[blockIdx.x]];
+    const int H = c.H[c.root_player];
+    for (int h0 = threadIdx.x * 4; h0 < H; h0 += blockDim.x * 4) {
+        float r[SS_MAX_ACTIONS][4], sig[SS_MAX_ACTIONS][4];
+        regret_match4(c.R, static_cast<size_t>(c.HS), c.root_fe, c.root_na, c.root_frozen, h0, r, sig);
+        for (int a = 0; a < c.root_na; ++a)
+            for (int i = 0; i < 4; ++i)
+                if (h0 + i < H) c.snap[static_cast<size_t>(a) * H + h0 + i] = sig[a][i];
+    }
+}
+
 __global__ void k_bump(int *iter) { *iter += 1; }
 
 // out[h] = sum over rows of val[row][h]
@@ -906,52 +934,54 @@ inline int chunks(int H) { return (H + kHandsPerBlock - 1) / kHandsPerBlock; }
 
 }  // namespace
 
-cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s) {
+cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
+                         const DevCtx *ctxs, int player) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = chunks(H);
-    k_reach<<<n * nc, kHandThreads, 0, s>>>(c, items, nc, H);
+    k_reach<<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, H, player);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s) {
+cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s,
+                       const DevCtx *ctxs, int trav) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
-    k_cfv<<<n * nc, kCfvThreads, 0, s>>>(c, items, nc, H);
+    k_cfv<<<n * nc, kCfvThreads, 0, s>>>(c, ctxs, items, nc, H, trav);
     return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                           cudaStream_t s) {
+                           cudaStream_t s, const DevCtx *ctxs) {
     if (n <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     switch (kind) {
         case TK_ZERO:
         case TK_LEAF0: {
             const int nc = chunks(c.HS);
-            k_term_fill<T><<<n * nc, kHandThreads, 0, s>>>(c, items, nc, trav, kind == TK_ZERO);
+            k_term_fill<T><<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, trav, kind == TK_ZERO);
             break;
         }
         case TK_CR1:
-            k_term_cr1<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, items, trav);
+            k_term_cr1<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
         case TK_CR2:
             if (cr2_smem<T>() > 48 * 1024)
                 e = cudaFuncSetAttribute(k_term_cr2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(cr2_smem<T>()));
             if (e != cudaSuccess) return e;
-            k_term_cr2<T><<<n, kTermThreads, cr2_smem<T>(), s>>>(c, items, trav);
+            k_term_cr2<T><<<n, kTermThreads, cr2_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
         case TK_SD1:
             if (sd1_smem<T>() > 48 * 1024)
                 e = cudaFuncSetAttribute(k_term_sd1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(sd1_smem<T>()));
             if (e != cudaSuccess) return e;
-            k_term_sd1<T><<<n, kTermThreads, sd1_smem<T>(), s>>>(c, items, trav);
+            k_term_sd1<T><<<n, kTermThreads, sd1_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
         case TK_ENUM: {
             const int nc = (c.HS + 127) / 128;
-            k_term_enum<T><<<n * nc, 128, 0, s>>>(c, items, nc, trav);
+            k_term_enum<T><<<n * nc, 128, 0, s>>>(c, ctxs, items, nc, trav);
             break;
         }
         default:
@@ -961,13 +991,13 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
 }
 
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                         cudaStream_t s) {
-    return launch_terms_t<float>(c, kind, items, n, trav, s);
+                         cudaStream_t s, const DevCtx *ctxs) {
+    return launch_terms_t<float>(c, kind, items, n, trav, s, ctxs);
 }
 
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                               cudaStream_t s) {
-    return launch_terms_t<double>(c, kind, items, n, trav, s);
+    return launch_terms_t<double>(c, kind, items, n, trav, s, nullptr);
 }
 
 cudaError_t launch_bump(int *iter, cudaStream_t s) {
@@ -1018,6 +1048,18 @@ cudaError_t launch_br_value(const DevCtx &c, const CfvItem *items, int n, int H,
 cudaError_t launch_br_root(const DevCtx &c, const int *rows, int n, int H, int weight_row, int trav,
                            int skip_blocked, double *out, cudaStream_t s) {
     k_br_root<<<1, 1024, 0, s>>>(c, rows, n, H, weight_row, trav, skip_blocked, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bump_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_bump_many<<<(n + 127) / 128, 128, 0, s>>>(ctxs, sgs, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_snapshot_many<<<n, 128, 0, s>>>(ctxs, sgs);
     return cudaGetLastError();
 }
 

@@ -24,12 +24,15 @@ struct DevCtx {
     const short *sd_card_list;   // [52][52]
     const short *sd_card_partner;// [52][52]
     const float *leaf_values;
-    const int *iter;       // current CFR iteration (device counter)
+    const int *iter;       // current CFR iteration (device counter, one per subgame)
     int HS;
     int np;
     int ncomb;
     int H[SS_MAX_PLAYERS];
     int dup[SS_MAX_PLAYERS];     // range holds some combo more than once
+    // root strategy snapshot (batched form: one launch covers many subgames)
+    float *snap;
+    int root_fe, root_na, root_frozen, root_player;
 };
 
 // threads per block of the per-hand kernels; each thread covers 4 hands
@@ -40,13 +43,21 @@ constexpr int kCfvThreads = 128;
 // threads per block of the per-terminal kernels
 constexpr int kTermThreads = 256;
 
-cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s);
-cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s);
+// With ctxs (a device array) every item reads the context of its subgame
+// (item.sg) and covers that subgame's hands of `player` / `trav`; without,
+// all items use c and cover H hands.  H also sizes the grid (the largest hand
+// count of the launch).
+cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
+                         const DevCtx *ctxs = nullptr, int player = -1);
+cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s,
+                       const DevCtx *ctxs = nullptr, int trav = -1);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                         cudaStream_t s);
+                         cudaStream_t s, const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                               cudaStream_t s);
 cudaError_t launch_bump(int *iter, cudaStream_t s);
+cudaError_t launch_bump_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s);
+cudaError_t launch_snapshot_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s);
 cudaError_t launch_br_reach(const DevCtx &c, const ReachItem *items, int n, int H, const float *avg,
                             const int *edge_di, int max_h, cudaStream_t s);
 cudaError_t launch_br_value(const DevCtx &c, const CfvItem *items, int n, int H, const float *avg,

@@ -201,3 +201,80 @@ def read_output(out, num_hands):
         "root_player": rp,
         "root_num_actions": na,
     }
+
+
+# ---------------------------------------------------------------------------
+# batched and served forms through the C ABI
+# ---------------------------------------------------------------------------
+
+def batch_solve(subgames, iterations, target=None, check_every=25, graph_iterations=10, device=0):
+    """Solve AbiSubgames together (ss_batch_solve); returns (rc, [result dicts])."""
+    lib = subgames[0].lib
+    n = len(subgames)
+    TreeP = ctypes.POINTER(ssg.tree_struct(subgames[0].max_hands_cap))
+    trees = (TreeP * n)(*[ctypes.pointer(sg.td) for sg in subgames])
+    outs = (ssg.SSOutput * n)()
+    stats = (ssg.SSSolveStats * n)()
+    opts = ssg.SSSolveOptions(device, graph_iterations, -1.0 if target is None else float(target),
+                              check_every, 0)
+    lib.ss_batch_solve.restype = ctypes.c_int
+    rc = lib.ss_batch_solve(trees, n, iterations, ctypes.byref(opts), outs, stats)
+    if rc != 0:
+        return rc, None
+    res = []
+    for i, sg in enumerate(subgames):
+        r = read_output(outs[i], sg.nh)
+        r["stats"] = {k: getattr(stats[i], k) for k, _ in ssg.SSSolveStats._fields_}
+        lib.ss_free_output(ctypes.byref(outs[i]))
+        res.append(r)
+    return 0, res
+
+
+class SSServerOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("memory_budget_gb", ctypes.c_double),
+                ("block_iterations", ctypes.c_int), ("target_exploitability", ctypes.c_float),
+                ("max_iterations", ctypes.c_int), ("graph_iterations", ctypes.c_int)]
+
+
+class Server:
+    """Continuous-batching solve server (ss_server_*)."""
+
+    def __init__(self, lib, **kw):
+        self.lib = lib
+        opts = SSServerOptions()
+        lib.ss_server_default_options(ctypes.byref(opts))
+        for k, v in kw.items():
+            setattr(opts, k, v)
+        self.h = ctypes.c_void_p()
+        lib.ss_server_create.restype = ctypes.c_int
+        lib.ss_server_submit.restype = ctypes.c_int
+        lib.ss_server_poll.restype = ctypes.c_int
+        lib.ss_server_wait.restype = ctypes.c_int
+        lib.ss_server_destroy.argtypes = [ctypes.c_void_p]
+        rc = lib.ss_server_create(ctypes.byref(opts), ctypes.byref(self.h))
+        if rc != 0:
+            raise RuntimeError(f"ss_server_create failed ({rc}): {ssg.last_error(lib)}")
+
+    def submit(self, sg):
+        rid = ctypes.c_longlong()
+        rc = self.lib.ss_server_submit(self.h, ctypes.byref(sg.td), ctypes.byref(rid))
+        if rc != 0:
+            raise RuntimeError(f"ss_server_submit failed ({rc}): {ssg.last_error(self.lib)}")
+        return rid.value
+
+    def wait(self, rid, num_hands):
+        out, stats, lat = ssg.SSOutput(), ssg.SSSolveStats(), ctypes.c_double()
+        rc = self.lib.ss_server_wait(self.h, ctypes.c_longlong(rid), ctypes.byref(out), ctypes.byref(stats),
+                                     ctypes.byref(lat))
+        if rc != 0:
+            raise RuntimeError(f"request {rid} failed ({rc}): {ssg.last_error(self.lib)}")
+        r = read_output(out, num_hands)
+        r["stats"] = {k: getattr(stats, k) for k, _ in ssg.SSSolveStats._fields_}
+        r["latency_ms"] = lat.value
+        self.lib.ss_free_output(ctypes.byref(out))
+        return r
+
+    def close(self):
+        if self.h:
+            self.lib.ss_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
