@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--iterations", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="plain,batched,served",
+                    help="comma list of plain (the headline), batched, served")
+    ap.add_argument("--batch-size", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=100.0, help="served form: requests per second")
+    ap.add_argument("--duration", type=float, default=3.0, help="served form: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -340,6 +345,107 @@ def run_ours(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
+# batched and served forms on the request mix
+# ---------------------------------------------------------------------------
+
+TARGET = 0.5      # % of pot
+CHECK = 25        # iterations between exploitability checks
+MAX_ITERS = 1000
+
+
+def pct(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(round(q / 100.0 * (len(v) - 1))))]
+
+
+def run_batched(n, seed, device):
+    """n mixed requests solved to <= 0.5% pot exploitability: one per call
+    (plain form, ss_solve_gpu_ex with the same stopping rule) and all
+    together (ss_batch_solve); wall time from host buffers to host outputs."""
+    import workloads as wl
+    subs = wl.mix_subgames(n, seed)
+    sg0 = subs[0]
+    rc, _ = sg0.solve(CHECK, target=TARGET, check_every=CHECK)  # warm the library / pool
+    t0 = time.perf_counter()
+    plain = []
+    for sg in subs:
+        rc, r = sg.solve(MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
+        if rc != 0:
+            raise RuntimeError(f"plain solve failed ({rc})")
+        plain.append(r["stats"])
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rc, res = wl.batch_solve(subs, MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
+    t_batch = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(f"batch solve failed ({rc})")
+    its = [r["stats"]["iterations_run"] for r in res]
+    expl = [r["stats"]["exploitability_pct"] for r in res]
+    nodes = [sg.td.num_nodes for sg in subs]
+    for sg in subs:
+        sg.free()
+    return {"subgames": n, "target_pct": TARGET, "check_every": CHECK,
+            "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch,
+            "speedup_vs_plain": t_plain / t_batch,
+            "iterations_p50": pct(its, 50), "iterations_max": max(its),
+            "exploitability_max_pct": max(expl),
+            "plain_iterations_p50": pct([p["iterations_run"] for p in plain], 50),
+            "tree_nodes": {"min": min(nodes), "p50": pct(nodes, 50), "max": max(nodes)},
+            "mix": "80% river (2p) / 15% turn (2-3p) / 5% flop (2p), full ranges, 0-70% zero weights"}
+
+
+def run_served(rate, duration, seed, device):
+    """Poisson arrivals at `rate` for `duration` seconds into the server
+    (continuous batching, retirement at <= 0.5% pot); latency = submission
+    to retirement.  The plain form's service time of the same requests
+    (one solve per call, no queueing) is reported beside it."""
+    import workloads as wl
+    rng = np.random.default_rng(seed + 7)
+    n = max(8, int(rate * duration))
+    subs = wl.mix_subgames(n, seed + 1)
+    lib = subs[0].lib
+    gaps = rng.exponential(1.0 / rate, n)
+    srv = wl.Server(lib, device=device, block_iterations=CHECK, target_exploitability=TARGET,
+                    max_iterations=MAX_ITERS, memory_budget_gb=40.0)
+    ids = [None] * n
+    t_start = time.perf_counter()
+
+    def feeder():
+        t = t_start
+        for i, sg in enumerate(subs):
+            t += gaps[i]
+            d = t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids[i] = srv.submit(sg)
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    lat, its = [], []
+    for i, sg in enumerate(subs):
+        while ids[i] is None:
+            time.sleep(0.0005)
+        r = srv.wait(ids[i], sg.nh)
+        lat.append(r["latency_ms"])
+        its.append(r["stats"]["iterations_run"])
+    th.join()
+    wall = time.perf_counter() - t_start
+    srv.close()
+    service = []
+    for sg in subs[:min(n, 64)]:
+        t0 = time.perf_counter()
+        rc, _ = sg.solve(MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
+        service.append((time.perf_counter() - t0) * 1e3)
+    for sg in subs:
+        sg.free()
+    return {"rate_per_s": rate, "requests": n, "solves_per_s": n / wall,
+            "latency_p50_ms": pct(lat, 50), "latency_p99_ms": pct(lat, 99),
+            "iterations_p50": pct(its, 50),
+            "plain_service_p50_ms": pct(service, 50), "plain_service_p99_ms": pct(service, 99),
+            "plain_solves_per_s": 1e3 * len(service) / sum(service)}
+
+
+# ---------------------------------------------------------------------------
 # the reference on the host cores
 # ---------------------------------------------------------------------------
 
@@ -435,7 +541,13 @@ def main():
                 print(json.dumps(line))
         return 0
 
+    forms = set(args.forms.split(","))
     res = run_ours(args, world, rank, local)
+    batched = served = None
+    if rank == 0 and world == 1 and "batched" in forms:
+        batched = run_batched(args.batch_size, args.seed, local)
+    if rank == 0 and world == 1 and "served" in forms:
+        served = run_served(args.rate, args.duration, args.seed, local)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = reference_cpu(args.seed, budget_s=20.0)
@@ -460,6 +572,7 @@ def main():
             "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
+            "batched": batched, "served": served,
         }
         print(json.dumps(line))
     try:

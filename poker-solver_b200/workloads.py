@@ -162,10 +162,10 @@ class AbiSubgame:
         nd = np.ctypeslib.as_array(self.td.node_depth, shape=(n,)).copy()
         return nodes, ch, lo, nd
 
-    def solve(self, iterations, graph_iterations=10, device=0, target=None):
+    def solve(self, iterations, graph_iterations=10, device=0, target=None, check_every=50):
         out = ssg.SSOutput()
         stats = ssg.SSSolveStats()
-        opts = ssg.SSSolveOptions(device, graph_iterations, -1.0 if target is None else target, 50, 0)
+        opts = ssg.SSSolveOptions(device, graph_iterations, -1.0 if target is None else target, check_every, 0)
         rc = self.lib.ss_solve_gpu_ex(ctypes.byref(self.td), iterations, ctypes.byref(opts),
                                       ctypes.byref(out), ctypes.byref(stats))
         if rc != 0:
@@ -278,3 +278,44 @@ class Server:
         if self.h:
             self.lib.ss_server_destroy(self.h)
             self.h = ctypes.c_void_p()
+
+
+# ---------------------------------------------------------------------------
+# request mix of the batched / served forms
+# ---------------------------------------------------------------------------
+
+BET_SETS = [[0.5, 1.0], [0.33, 0.75], [1.0], [0.5], [0.33, 0.75, 1.5], [0.75]]
+
+
+def mix_config(rng, river=0.8, turn=0.15):
+    """One seeded request of the serving mix: 80% river (2 players),
+    15% turn (2-3 players, continuation leaves), 5% flop (2 players,
+    continuation leaves); all non-board combos with U(0,1) weights, a
+    U(0, 0.7) fraction zeroed; random bet set and raise cap (so tree sizes
+    spread from tens to thousands of nodes)."""
+    u = rng.random()
+    street = "river" if u < river else ("turn" if u < river + turn else "flop")
+    nb = {"river": 5, "turn": 4, "flop": 3}[street]
+    np_ = 2 if street != "turn" else int(rng.integers(2, 4))
+    board = [int(c) for c in rng.permutation(52)[:nb]]
+    sizes = BET_SETS[int(rng.integers(len(BET_SETS)))]
+    if np_ == 3:
+        sizes = sizes[:1]
+    raises = int(rng.integers(1, 4)) if street == "river" else int(rng.integers(1, 3))
+    pot = int(rng.integers(50, 400))
+    cfg = dict(board=board, pot=pot, stack=int(pot * rng.uniform(2, 8)), bet_sizes=sizes,
+               max_raises=raises, num_players=np_, seed=int(rng.integers(1 << 30)),
+               leaf_sigma=0.3 * pot, name=f"{street}{np_}")
+    cfg["hands"], cfg["weights"] = make_ranges(rng, board, np_, None, zero_frac=float(rng.uniform(0, 0.7)))
+    return cfg
+
+
+def mix_subgames(n, seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        cfg = mix_config(rng)
+        sg = AbiSubgame(cfg, max_hands=ssg.SS_MAX_HANDS_WIDE)
+        sg.set_leaf_values(leaf_values_for(cfg, sg.num_leaves))
+        out.append(sg)
+    return out
