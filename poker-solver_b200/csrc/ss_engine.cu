@@ -147,6 +147,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     const size_t o_fr_off = b.add(P.fr_off);
     const size_t o_fr_items = b.add(P.fr_items);
     const size_t o_code = b.add(P.hand_code);
+    const size_t o_pair = b.add(P.pair_idx);
     const size_t o_sdpos = b.add(P.sd_pos);
     const size_t o_str = b.add(P.strength);
     const size_t o_sdc = b.add(P.sd_combo);
@@ -204,6 +205,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.fr_off = reinterpret_cast<const int *>(dbase + o_fr_off);
     c.fr_items = reinterpret_cast<const int *>(dbase + o_fr_items);
     c.hand_code = reinterpret_cast<const int *>(dbase + o_code);
+    c.pair_idx = reinterpret_cast<const short *>(dbase + o_pair);
     c.sd_pos = reinterpret_cast<const int *>(dbase + o_sdpos);
     c.strength = reinterpret_cast<const unsigned *>(dbase + o_str);
     c.sd_combo = reinterpret_cast<const SdCombo *>(dbase + o_sdc);
@@ -214,6 +216,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.HS = P.HS;
     c.np = np;
     c.ncomb = P.ncomb;
+    c.deck = P.deck;
     for (int p = 0; p < SS_MAX_PLAYERS; ++p) {
         c.H[p] = p < np ? P.H[p] : 0;
         c.dup[p] = p < np ? P.dup[p] : 0;

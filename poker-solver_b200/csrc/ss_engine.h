@@ -98,6 +98,12 @@ enum TermKind : int {
 
 // One terminal for one traverser.  factor: payoff for folds; leaf_off >= 0
 // selects leaf_values[leaf_off + h] instead.  Showdowns use pot / bet.
+// Two-opponent terminals whose counted opponents sit on the same reach rows
+// (the traverser's own continuation choices below one opponent pair) form a
+// group: consecutive items, the first with gextra = number of followers, the
+// followers with follow = 1.  A zeroed item is a group of one.  Groups hold
+// at most kTermGroupMax items.
+constexpr int kTermGroupMax = 16;
 struct alignas(16) TermItem {
     int node;
     int kind_detail;          // TK_ENUM: 0 fold, 1 leaf, 2 showdown
@@ -109,7 +115,8 @@ struct alignas(16) TermItem {
     int sg;                   // subgame of a batch (0 for a single subgame)
     int opp_row[SS_MAX_PLAYERS - 1];
     int opp_player[SS_MAX_PLAYERS - 1];
-    int pad2[2];
+    int gextra;               // group leader: number of following items in its group
+    int follow;               // 1: member of the group led by an earlier item
 };
 
 // Showdown tables for one board: every non-board 2-card combo ranked by the
@@ -146,8 +153,12 @@ struct Plan {
     std::vector<int> root_fr[SS_MAX_PLAYERS];
     // per traverser, per TermKind: terminal items
     std::vector<TermItem> term[SS_MAX_PLAYERS][TK_COUNT];
-    // hand tables, [np][HS]: c0 | c1 << 8 | board_blocked << 16; -1 padding
+    // hand tables, [np][HS]: c0 | c1 << 8 | board_blocked << 16 | d0 << 20 | d1 << 26,
+    // d = dense card index (rank among the deck's non-board cards, 63 for a
+    // board card); -1 padding
     std::vector<int> hand_code;
+    int deck = 0;                      // number of non-board cards
+    std::vector<short> pair_idx;       // [np][52][52] range index of each dense-card pair, -1 if none
     // showdown tables (river only)
     int ncomb = 0;
     std::vector<SdCombo> sd_combo;     // [ncomb]

@@ -275,6 +275,13 @@ __device__ __forceinline__ void load4(const float *p, float v[4]) {
     const float4 x = *reinterpret_cast<const float4 *>(p);
     v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
 }
+__device__ __forceinline__ void store4(double *p, const double v[4]) {
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void store4(float *p, const float v[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
 
 // Row pass over a combo matrix, one warp per card row r: the row sum u(r) in
 // FP64 and the 64-bit mask of the row's positive cells.  The masks give the
@@ -380,122 +387,427 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevC
     }
 }
 
-// Per-card aggregates of the two-opponent closed form, packed so a hand
-// needs two 16-byte shared loads per card.
-struct alignas(16) CardAgg {
+// Per-card terms of the two-opponent closed form over the dense deck (the
+// non-board cards, renumbered 0 .. deck-1): FP64 sums and integer counts of
+// positive-reach cells, packed so a hand reads a few 16/32-byte entries per
+// card.  Entry 52 stays zero and stands for a board card of the traverser.
+struct alignas(16) Cr2Card {
     double u1, u2;      // per-card reach sums of opponents 1 and 2
-    double w, d;        // (M2 u1 + M1 u2)(c), sum_b M1[c][b] M2[c][b]
+    double g;           // u1 u2 + w - 2 d, w = (M2 u1 + M1 u2)(c), d = sum_b M1[c][b] M2[c][b]
+    double d;
 };
-struct alignas(16) CardCnt {
-    int u1, u2, w, d;   // the same on the 0/1 positive-reach matrices
+struct alignas(16) Cr2Cnt {
+    int n1, n2;         // positive-reach cells of the card's row in M1, M2
+    int pad0, pad1;
 };
+// block scalars: F_i = sum u_i / 2, QD = D - Q with Q = sum u1 u2, D = sum d / 2,
+// and the same on the 0/1 positive-reach matrices
 struct Cr2Scalars {
-    double F1, F2, Q, D;
-    long long IF1, IF2, IQ, ID;
+    double F1, F2, QD;
+    int IF1, IF2, IQD, pad;
 };
+constexpr int kCr2Off = 52;   // index of the zero per-card entry
+constexpr int kMaxHS = 1344;  // largest row stride: 1326 combos rounded up to 32
 
+// dynamic shared memory of the two-opponent kernel for row stride HS: M1, M2,
+// P (whose space first stages the two opponents' reach rows), the first
+// terminal's leaf row, per-card terms, staged group items
 template <class T>
-constexpr size_t cr2_smem() {
-    return 3 * 52 * MS * sizeof(T) + 52 * sizeof(CardAgg) + 52 * sizeof(CardCnt) + 52 * 16 +
-           sizeof(Cr2Scalars) + 64;
+constexpr size_t cr2_smem(int HS) {
+    return 3 * 52 * MS * sizeof(T) + static_cast<size_t>(HS) * 4 + 53 * sizeof(Cr2Card) + 53 * sizeof(Cr2Cnt) +
+           53 * 16 + 5 * 48 * 4 + sizeof(Cr2Scalars) + 3 * kTermGroupMax * 4 + 8 * 16;
 }
 
-// Two counted opponents (1, 2) with combo matrices M1, M2, per-card sums
-// u_i = M_i 1, d(c) = sum_b M1[c][b] M2[c][b], w = M2 u1 + M1 u2,
-// P = M1 M2, F_i = sum u_i / 2, Q = sum u1 u2, D = sum d / 2.  For a traverser
-// hand (a, b), m_i = M_i[a][b], A_i = F_i - u_i(a) - u_i(b) + m_i, the mass of
-// opponent pairs disjoint from each other and from (a, b) is
+// asynchronous global -> shared copies (cp.async): 16-byte chunks and 4-byte words
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// One opponent's staged reach as a symmetric matrix over the dense deck:
+// M[a][b] = M[b][a] = reach of the hand {a, b}; board-blocked hands never
+// count (street_solve.cu:755-757).  This form serves ranges that hold some
+// combo twice (accumulated atomically into a cleared matrix).
+template <class T>
+__device__ __forceinline__ void scatter_dense(const int *__restrict__ code, int Ho, const T *r, T *M) {
+    for (int j = threadIdx.x; j < Ho; j += blockDim.x) {
+        const int hc = __ldg(code + j);
+        if (hc & 0x10000) continue;
+        const int a = (hc >> 20) & 63, b = (hc >> 26) & 63;
+        const T x = r[j];
+        atomicAdd(&M[a * MS + b], x);
+        atomicAdd(&M[b * MS + a], x);
+    }
+}
+
+// The same matrices gathered instead (ranges without a repeated combo): each
+// thread fills 4-column chunks of rows 0 .. Dp-1 through the player's table of
+// range indices per dense-card pair, so every cell is written once, with
+// conflict-free 16-byte stores and no clearing pass.  Cells outside rows and
+// columns 0 .. Dp-1 are left unset; nothing reads them.
+template <class T>
+__device__ __forceinline__ void gather_dense(const short *__restrict__ tab, const T *r, T *M, int Dp) {
+    const int chunk = threadIdx.x & 15, c0 = chunk * 4;
+    if (c0 >= Dp) return;
+    for (int row = threadIdx.x >> 4; row < Dp; row += kTermThreads / 16) {
+        const short4 ix = __ldg(reinterpret_cast<const short4 *>(tab + row * 52 + c0));
+        T v[4];
+        v[0] = ix.x >= 0 ? r[ix.x] : T(0);
+        v[1] = ix.y >= 0 ? r[ix.y] : T(0);
+        v[2] = ix.z >= 0 ? r[ix.z] : T(0);
+        v[3] = ix.w >= 0 ? r[ix.w] : T(0);
+        store4(M + row * MS + c0, v);
+    }
+}
+
+// The fields of a subgame context that the two-opponent kernel reads, copied
+// into registers.  (A reference bound to either the kernel parameter or a
+// batch entry would give the parameter a generic address, and every field
+// read would then go through local memory.)
+template <class T>
+struct Cr2View {
+    const T *reach;
+    T *val;
+    const int *code_t, *code0, *code1;   // hand codes of the traverser and the two opponents
+    const short *tab0, *tab1;            // dense-pair tables of the two opponents
+    const float *leaf;
+    int HS, deck, Ht, H0, H1;
+    bool dup;
+};
+template <class T>
+__device__ __forceinline__ Cr2View<T> cr2_view(const DevCtx &c, int trav, int o0, int o1) {
+    Cr2View<T> v;
+    v.reach = reach_rows<T>(c);
+    v.val = val_rows<T>(c);
+    v.code_t = c.hand_code + static_cast<size_t>(trav) * c.HS;
+    v.code0 = c.hand_code + static_cast<size_t>(o0) * c.HS;
+    v.code1 = c.hand_code + static_cast<size_t>(o1) * c.HS;
+    v.tab0 = c.pair_idx + static_cast<size_t>(o0) * 52 * 52;
+    v.tab1 = c.pair_idx + static_cast<size_t>(o1) * 52 * 52;
+    v.leaf = c.leaf_values;
+    v.HS = c.HS;
+    v.deck = c.deck;
+    v.Ht = c.H[trav];
+    v.H0 = c.H[o0];
+    v.H1 = c.H[o1];
+    v.dup = (c.dup[o0] | c.dup[o1]) != 0;
+    return v;
+}
+
+// TF32 split of the tensor-core product below: x = hi + lo, hi = x truncated
+// to TF32 (10 explicit mantissa bits), lo = the exact FP32 remainder rounded
+// to TF32 (half away from zero on the bit pattern).  hi*hi + hi*lo + lo*hi
+// then carries about 21 significant bits, close to the FP32 product.
+__device__ __forceinline__ void split_tf32(float x, unsigned &hi, unsigned &lo) {
+    hi = __float_as_uint(x) & 0xffffe000u;                                        // truncated: x - hi is exact
+    lo = (__float_as_uint(x - __uint_as_float(hi)) + 0x1000u) & 0xffffe000u;     // rounded remainder
+}
+// d += a b, one m16n8k8 TF32 tile (A row-major 16x8, B column-major 8x8)
+__device__ __forceinline__ void mma_tf32(float d[4], const unsigned a[4], const unsigned b[2]) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// P = M1 M2 over a dense deck of at most 48 cards on the tensor cores: warp w
+// (0..5) owns rows 16 (w / 2) .. +15 and columns 24 (w % 2) .. +23 (three
+// 8-column tiles); six k-steps of 8.  Operand fragments are read from the
+// FP32 matrices in shared memory (row stride 52 keeps the A-fragment loads
+// free of bank conflicts) and split into TF32 pairs in registers.
+// Also leaves rsum[h][r] = sum of row r over column half h and csum[s][c] =
+// sum of column c over row strip s (FP32, deterministic order).
+__device__ __forceinline__ void product_mma48(const float *M1, const float *M2, float *P, float *rsum, float *csum,
+                                              int warp, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = (warp >> 1) * 16, n0 = (warp & 1) * 24;
+    float acc[3][4] = {};
+#pragma unroll
+    for (int k0 = 0; k0 < 48; k0 += 8) {
+        unsigned ah[4], al[4];
+        split_tf32(M1[(m0 + g) * MS + k0 + t], ah[0], al[0]);
+        split_tf32(M1[(m0 + g + 8) * MS + k0 + t], ah[1], al[1]);
+        split_tf32(M1[(m0 + g) * MS + k0 + t + 4], ah[2], al[2]);
+        split_tf32(M1[(m0 + g + 8) * MS + k0 + t + 4], ah[3], al[3]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int n = n0 + j * 8 + g;
+            unsigned bh[2], bl[2];
+            split_tf32(M2[(k0 + t) * MS + n], bh[0], bl[0]);
+            split_tf32(M2[(k0 + t + 4) * MS + n], bh[1], bl[1]);
+            mma_tf32(acc[j], al, bh);
+            mma_tf32(acc[j], ah, bl);
+            mma_tf32(acc[j], ah, bh);
+        }
+    }
+    float ra = 0.f, rb = 0.f;   // this lane's share of rows m0 + g and m0 + g + 8
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int n = n0 + j * 8 + 2 * t;
+        *reinterpret_cast<float2 *>(&P[(m0 + g) * MS + n]) = make_float2(acc[j][0], acc[j][1]);
+        *reinterpret_cast<float2 *>(&P[(m0 + g + 8) * MS + n]) = make_float2(acc[j][2], acc[j][3]);
+        ra += acc[j][0] + acc[j][1];
+        rb += acc[j][2] + acc[j][3];
+    }
+    // row sums over this warp's 24 columns and column sums over its 16 rows
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+        ra += __shfl_xor_sync(0xffffffffu, ra, o);
+        rb += __shfl_xor_sync(0xffffffffu, rb, o);
+    }
+    if (t == 0) {
+        rsum[(warp & 1) * 48 + m0 + g] = ra;
+        rsum[(warp & 1) * 48 + m0 + g + 8] = rb;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float c0 = acc[j][0] + acc[j][2], c1 = acc[j][1] + acc[j][3];
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) {
+            c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+            c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+        }
+        if (g == 0) {
+            csum[(warp >> 1) * 48 + n0 + j * 8 + 2 * t] = c0;
+            csum[(warp >> 1) * 48 + n0 + j * 8 + 2 * t + 1] = c1;
+        }
+    }
+}
+
+// column sums and positive-cell masks of M1 (s < Dp) or M2 (s >= Dp): four
+// independent partial sums in T (Dp is a multiple of 4; FP32 keeps the
+// relative error near 1e-7), added in FP64 in a fixed order
+template <class T>
+__device__ __forceinline__ void column_stats(const T *M1, const T *M2, int s, int Dp, Cr2Card *card,
+                                             ulonglong2 *Bm) {
+    const bool second = s >= Dp;
+    const int col = second ? s - Dp : s;
+    const T *M = (second ? M2 : M1) + col;
+    T u[4] = {T(0), T(0), T(0), T(0)};
+    unsigned long long B = 0ull;
+    for (int r = 0; r < Dp; r += 4) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const T x = M[(r + i) * MS];
+            u[i] += x;
+            B |= static_cast<unsigned long long>(x > T(0)) << (r + i);
+        }
+    }
+    const double tot = (static_cast<double>(u[0]) + static_cast<double>(u[1])) +
+                       (static_cast<double>(u[2]) + static_cast<double>(u[3]));
+    if (second) {
+        card[col].u2 = tot;
+        Bm[col].y = B;
+    } else {
+        card[col].u1 = tot;
+        Bm[col].x = B;
+    }
+}
+
+// 4x4 tile (rows i0.., columns j0..) of P = M1 M2; M1 is symmetric, so row k
+// of M1 is its column k.
+template <class T>
+__device__ __forceinline__ void product_tile(const T *M1, const T *M2, T *P, int i0, int j0, int Dp) {
+    T acc[4][4] = {};
+#pragma unroll 4
+    for (int k = 0; k < Dp; ++k) {
+        T xs[4], ys[4];
+        load4(&M1[k * MS + i0], xs);
+        load4(&M2[k * MS + j0], ys);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += xs[i] * ys[j];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) P[(i0 + i) * MS + j0 + j] = acc[i][j];
+}
+
+// Number of opponent pairs with positive reach that are disjoint from each
+// other and from the traverser hand (a, b): the two-opponent formula on the
+// 0/1 positive-reach matrices, whose entries are the bits of the card masks
+// (row c of M_i = bits of Bm[c]).  The per-card term ng(c) = n1 n2 + nw - 2 nd
+// with nw(c) = (I2 n1 + I1 n2)(c) is summed here over the set bits, since the
+// count is only needed for the few hands whose mass is near zero.
+__device__ __forceinline__ int card_ng(const ulonglong2 *Bm, const Cr2Cnt *cnt, int c) {
+    const ulonglong2 Bc = Bm[c];
+    int nw = 0;
+    for (unsigned long long m = Bc.y; m; m &= m - 1) nw += cnt[__ffsll(static_cast<long long>(m)) - 1].n1;
+    for (unsigned long long m = Bc.x; m; m &= m - 1) nw += cnt[__ffsll(static_cast<long long>(m)) - 1].n2;
+    return cnt[c].n1 * cnt[c].n2 + nw - 2 * __popcll(Bc.x & Bc.y);
+}
+__device__ __noinline__ int pair_count(const ulonglong2 *Bm, const Cr2Cnt *cnt, int a, int b, int IF1, int IF2,
+                                      int IQD) {
+    const ulonglong2 Ba = Bm[a], Bb = Bm[b];
+    const int n1a = cnt[a].n1, n1b = cnt[b].n1, n2a = cnt[a].n2, n2b = cnt[b].n2;
+    const int j1 = bit(Ba.x, b), j2 = bit(Ba.y, b);
+    return (IF1 - n1a - n1b + j1) * (IF2 - n2a - n2b + j2) + IQD + card_ng(Bm, cnt, a) + card_ng(Bm, cnt, b) -
+           j2 * (n1a + n1b) - j1 * (n2a + n2b) + 3 * j1 * j2 - (__popcll(Ba.x & Bb.y) + __popcll(Bb.x & Ba.y));
+}
+
+// Two counted opponents (1, 2) with combo matrices M1, M2 over the dense
+// deck, per-card sums u_i = M_i 1, d(c) = sum_b M1[c][b] M2[c][b],
+// w = M2 u1 + M1 u2, P = M1 M2, F_i = sum u_i / 2, Q = sum u1 u2, D = sum d / 2.
+// For a traverser hand (a, b), m_i = M_i[a][b], A_i = F_i - u_i(a) - u_i(b) + m_i,
+// the mass of opponent pairs disjoint from each other and from (a, b) is
 //   A1 A2 - Q + u1(a)u2(a) + u1(b)u2(b) + w(a) + w(b)
 //   - m2 (u1(a) + u1(b)) - m1 (u2(a) + u2(b)) - 2 (d(a) + d(b)) + 3 m1 m2
 //   - P[a][b] - P[b][a] + D
 // (inclusion-exclusion over shared cards), equal to the reference odometer
 // sum of street_solve.cu:771-823 / :1079-1127 for two opponents.
+//
+// Exact zeros: the reference only adds positive reach products, so a hand
+// with no compatible positive-reach pair gets exactly 0.  Every term above is
+// at most a few F1 F2 in size and the product P carries FP32 accuracy, so a
+// computed mass above 1e-4 F1 F2 cannot come from an empty set of pairs; at or
+// below it the kernel counts the compatible positive-reach pairs exactly (the
+// same formula on the 0/1 positive-reach matrices, via 64-bit card masks) and
+// writes 0 when there are none.
+//
+// One block per group of terminals sharing both opponents' reach rows: the
+// masses are computed once and multiplied by each terminal's factor.
+// Phases: cp.async staging of both reach rows and the first leaf row; gather
+// (or clear + scatter for ranges that repeat a combo); P (tensor cores)
+// alongside per-column sums and masks; per-card FP64 terms and block scalars;
+// per-hand mass and one output row per terminal.
 template <class T>
-__global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 6 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
+__global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                               const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
+    const TermItem *I0 = items + blockIdx.x;
+    if (I0->follow) return;   // written by the block of its group's first item
+    const int ng = I0->gextra + 1;
+    const int o0 = I0->opp_player[0], o1 = I0->opp_player[1];
+    const Cr2View<T> V = ctxs ? cr2_view<T>(ctxs[I0->sg], trav, o0, o1) : cr2_view<T>(c0, trav, o0, o1);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int HS = V.HS;
+    const int Dp = (V.deck + 3) & ~3;
     Carve cv{smem};
     T *M1 = cv.take<T>(52 * MS);
     T *M2 = cv.take<T>(52 * MS);
     T *P = cv.take<T>(52 * MS);
-    CardAgg *agg = cv.take<CardAgg>(52);
-    CardCnt *cnt = cv.take<CardCnt>(52);
-    ulonglong2 *Bm = cv.take<ulonglong2>(52);   // positive-reach masks of M1 (x) and M2 (y)
+    float *leaf0 = cv.take<float>(HS);
+    Cr2Card *card = cv.take<Cr2Card>(53);
+    Cr2Cnt *cnt = cv.take<Cr2Cnt>(53);
+    ulonglong2 *Bm = cv.take<ulonglong2>(53);   // positive-cell masks of M1 (x) and M2 (y) per card
+    float *rsum = cv.take<float>(2 * 48);       // tensor-core path: partial row / column sums of P
+    float *csum = cv.take<float>(3 * 48);
     Cr2Scalars *sc = cv.take<Cr2Scalars>(1);
-    const TermItem I = items[blockIdx.x];
-    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nwarp = blockDim.x / 32;
-    zero_matrix(M1);
-    zero_matrix(M2);
-    __syncthreads();
-    scatter_combo(c, I.opp_player[0], I.opp_row[0], M1);
-    scatter_combo(c, I.opp_player[1], I.opp_row[1], M2);
-    __syncthreads();
-    for (int r = warp; r < 52; r += nwarp) {
-        double s1, s2, a0, a1, e0, e1;
-        unsigned long long b1, b2;
-        row_stats(M1, r, lane, &s1, &b1, &a0, &a1);
-        row_stats(M2, r, lane, &s2, &b2, &e0, &e1);
-        const double sd = warp_sum(a0 * e0 + a1 * e1);
-        if (lane == 0) {
-            agg[r].u1 = s1;
-            agg[r].u2 = s2;
-            agg[r].d = sd;
-            Bm[r] = make_ulonglong2(b1, b2);
-            cnt[r].u1 = __popcll(b1);
-            cnt[r].u2 = __popcll(b2);
-            cnt[r].d = __popcll(b1 & b2);
+    int *gnode = cv.take<int>(kTermGroupMax);
+    int *gleaf = cv.take<int>(kTermGroupMax);
+    float *gpay = cv.take<float>(kTermGroupMax);
+    T *r1 = P, *r2 = P + HS;                    // staged reach rows (P is written after the scatter)
+
+    // staging: both opponents' reach rows (16-byte chunks; rows start on
+    // 128-byte boundaries) and the first terminal's leaf row (4-byte words)
+    {
+        const T *s1 = V.reach + static_cast<size_t>(I0->opp_row[0]) * HS;
+        const T *s2 = V.reach + static_cast<size_t>(I0->opp_row[1]) * HS;
+        constexpr int per = 16 / sizeof(T);
+        for (int q = tid * per; q < HS; q += kTermThreads * per) {
+            cp_async16(r1 + q, s1 + q);
+            cp_async16(r2 + q, s2 + q);
+        }
+        const int lo = I0->leaf_off;
+        if (lo >= 0) {
+            const float *src = V.leaf + lo;
+            for (int h = tid; h < V.Ht; h += kTermThreads) cp_async4(leaf0 + h, src + h);
+        }
+        if (tid < ng) {
+            const TermItem &I = I0[tid];
+            gnode[tid] = I.node;
+            gleaf[tid] = I.leaf_off;
+            gpay[tid] = I.payoff;
         }
     }
+    if (V.dup) {
+        zero_matrix(M1);
+        zero_matrix(M2);
+    }
+    cp_async_wait_all();
     __syncthreads();
-    if (tid < 169) {
-        // P = M1 M2 in 4x4 tiles; M1 is symmetric, so row b of M1 is column b
-        const int i0 = (tid / 13) * 4, j0 = (tid % 13) * 4;
-        T acc[4][4] = {};
-        for (int b = 0; b < 52; ++b) {
-            T xs[4], ys[4];
-            load4(&M1[b * MS + i0], xs);
-            load4(&M2[b * MS + j0], ys);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] += xs[i] * ys[j];
+    if (V.dup) {
+        scatter_dense(V.code0, V.H0, r1, M1);
+        scatter_dense(V.code1, V.H1, r2, M2);
+    } else {
+        gather_dense(V.tab0, r1, M1, Dp);
+        gather_dense(V.tab1, r2, M2, Dp);
+    }
+    __syncthreads();
+
+    // phase A: P = M1 M2 (tensor cores when the deck fits 48 cards, else
+    // 4x4 SIMT tiles); per-column reach sums and positive-cell masks
+    bool mma = false;
+    if constexpr (sizeof(T) == 4) mma = Dp <= 48;
+    if (mma) {
+        if constexpr (sizeof(T) == 4) {
+            if (warp < 6) product_mma48(M1, M2, P, rsum, csum, warp, lane);
         }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) P[(i0 + i) * MS + j0 + j] = acc[i][j];
-    } else if (tid < 169 + 52) {
-        const int col = tid - 169;
-        double s = 0.0;
-        int n = 0;
-        for (int b = 0; b < 52; ++b) {
-            const CardAgg g = agg[b];
-            s += g.u1 * static_cast<double>(M2[b * MS + col]) + g.u2 * static_cast<double>(M1[b * MS + col]);
-            const ulonglong2 m = Bm[b];
-            n += bit(m.y, col) * cnt[b].u1 + bit(m.x, col) * cnt[b].u2;
+        // columns: warps 6-7 take 0..63, warp 0 (after its MMA tiles) 64..95
+        const int s = tid >= 6 * 32 ? tid - 6 * 32 : tid < 32 ? 64 + tid : 2 * 52;
+        if (s < 2 * Dp) column_stats(M1, M2, s, Dp, card, Bm);
+    } else {
+        const int nt = Dp >> 2;
+        if (tid < nt * nt) product_tile(M1, M2, P, (tid / nt) * 4, (tid % nt) * 4, Dp);
+        const int s = kTermThreads - 1 - tid;
+        if (s < 2 * Dp) column_stats(M1, M2, s, Dp, card, Bm);
+    }
+    __syncthreads();
+
+    // phase B: per-card terms (w from the row and column sums of P, d from its
+    // diagonal: P = M1 M2 with symmetric M1, M2 gives rowsum = M1 u2,
+    // colsum = M2 u1, P[c][c] = d(c)); entries beyond the deck are zeroed;
+    // the last warp forms the block scalars
+    if (tid < Dp) {
+        const int col = tid;
+        double w;
+        if (mma) {
+            w = (static_cast<double>(rsum[col]) + static_cast<double>(rsum[48 + col])) +
+                ((static_cast<double>(csum[col]) + static_cast<double>(csum[48 + col])) +
+                 static_cast<double>(csum[96 + col]));
+        } else {
+            w = 0.0;
+            for (int b = 0; b < Dp; ++b)
+                w += static_cast<double>(P[col * MS + b]) + static_cast<double>(P[b * MS + col]);
         }
-        agg[col].w = s;
-        cnt[col].w = n;
-    } else if (warp == nwarp - 1) {
-        double a1 = 0, a2 = 0, q = 0, e = 0;
-        long long n1 = 0, n2 = 0, nq = 0, nd = 0;
-        for (int k = lane; k < 52; k += 32) {
-            const CardAgg g = agg[k];
-            a1 += g.u1;
-            a2 += g.u2;
-            q += g.u1 * g.u2;
-            e += g.d;
-            const CardCnt m = cnt[k];
-            n1 += m.u1;
-            n2 += m.u2;
-            nq += static_cast<long long>(m.u1) * m.u2;
-            nd += m.d;
+        const double d = P[col * MS + col];
+        const double u1 = card[col].u1, u2 = card[col].u2;
+        card[col].g = u1 * u2 + w - 2.0 * d;
+        card[col].d = d;
+        const ulonglong2 Bc = Bm[col];
+        cnt[col] = Cr2Cnt{__popcll(Bc.x), __popcll(Bc.y), 0, 0};
+    } else if (tid <= kCr2Off) {
+        card[tid] = Cr2Card{0.0, 0.0, 0.0, 0.0};
+        cnt[tid] = Cr2Cnt{0, 0, 0, 0};
+        Bm[tid] = make_ulonglong2(0ull, 0ull);
+    } else if (warp == kTermThreads / 32 - 1) {
+        double a1 = 0.0, a2 = 0.0, qq = 0.0, e = 0.0;
+        int n1 = 0, n2 = 0, nq = 0, nd = 0;
+        for (int k = lane; k < Dp; k += 32) {
+            const double u1 = card[k].u1, u2 = card[k].u2;
+            a1 += u1;
+            a2 += u2;
+            qq += u1 * u2;
+            e += static_cast<double>(P[k * MS + k]);
+            const ulonglong2 B = Bm[k];
+            const int p1 = __popcll(B.x), p2 = __popcll(B.y);
+            n1 += p1;
+            n2 += p2;
+            nq += p1 * p2;
+            nd += __popcll(B.x & B.y);
         }
         a1 = warp_sum(a1);
         a2 = warp_sum(a2);
-        q = warp_sum(q);
+        qq = warp_sum(qq);
         e = warp_sum(e);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -504,49 +816,41 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 6 : 2) k_term_c
             nq += __shfl_xor_sync(0xffffffffu, nq, o);
             nd += __shfl_xor_sync(0xffffffffu, nd, o);
         }
-        if (lane == 0) {
-            sc->F1 = 0.5 * a1;
-            sc->F2 = 0.5 * a2;
-            sc->Q = q;
-            sc->D = 0.5 * e;
-            sc->IF1 = n1 / 2;
-            sc->IF2 = n2 / 2;
-            sc->IQ = nq;
-            sc->ID = nd / 2;
-        }
+        if (lane == 0) *sc = Cr2Scalars{0.5 * a1, 0.5 * a2, 0.5 * e - qq, n1 / 2, n2 / 2, nd / 2 - nq, 0};
     }
     __syncthreads();
+
+    // phase C: card-removal mass of every traverser hand, written out as
+    // factor x mass for every terminal of the group
     const Cr2Scalars S = *sc;
-    const int Ht = c.H[trav];
-    const int *tc = c.hand_code + static_cast<size_t>(trav) * c.HS;
-    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
-    for (int h = tid; h < c.HS; h += blockDim.x) {
+    const double zmin = 1e-4 * S.F1 * S.F2;
+    const bool none = !(S.F1 > 0.0 && S.F2 > 0.0);   // an opponent without positive reach: all zero
+    const int Ht = V.Ht;
+    const int *__restrict__ tc = V.code_t;
+    const bool leaf_first = gleaf[0] >= 0;
+    const float gp0 = gpay[0];
+    T *out0 = V.val + static_cast<size_t>(gnode[0]) * HS;
+    for (int h = tid; h < HS; h += kTermThreads) {
         double v = 0.0;
-        if (h < Ht) {
-            const int hc = tc[h];
-            const int a = hc & 0xff, b = (hc >> 8) & 0xff;
-            const ulonglong2 Ba = Bm[a], Bb = Bm[b];
-            const CardCnt na = cnt[a], nb = cnt[b];
-            const long long j1 = bit(Ba.x, b), j2 = bit(Ba.y, b);
-            const long long JA1 = S.IF1 - na.u1 - nb.u1 + j1, JA2 = S.IF2 - na.u2 - nb.u2 + j2;
-            const long long live = JA1 * JA2 - S.IQ + static_cast<long long>(na.u1) * na.u2 +
-                                   static_cast<long long>(nb.u1) * nb.u2 + na.w + nb.w -
-                                   j2 * (na.u1 + nb.u1) - j1 * (na.u2 + nb.u2) - 2 * (na.d + nb.d) +
-                                   3 * j1 * j2 - (__popcll(Ba.x & Bb.y) + __popcll(Bb.x & Ba.y)) + S.ID;
-            if (live > 0) {
-                const CardAgg ga = agg[a], gb = agg[b];
-                const double m1 = M1[a * MS + b], m2 = M2[a * MS + b];
-                const double A1 = S.F1 - ga.u1 - gb.u1 + m1;
-                const double A2 = S.F2 - ga.u2 - gb.u2 + m2;
-                const double z = A1 * A2 - S.Q + ga.u1 * ga.u2 + gb.u1 * gb.u2 + ga.w + gb.w -
-                                 m2 * (ga.u1 + gb.u1) - m1 * (ga.u2 + gb.u2) - 2.0 * (ga.d + gb.d) +
-                                 3.0 * m1 * m2 -
-                                 (static_cast<double>(P[a * MS + b]) + static_cast<double>(P[b * MS + a])) +
-                                 S.D;
-                v = static_cast<double>(term_factor(c, I, h)) * z;
-            }
+        if (h < Ht && !none) {
+            const int hc = __ldg(tc + h);
+            const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
+            const bool on = (a < kCr2Off) && (b < kCr2Off);
+            const Cr2Card ga = card[a], gb = card[b];
+            const double m1 = on ? static_cast<double>(M1[a * MS + b]) : 0.0;
+            const double m2 = on ? static_cast<double>(M2[a * MS + b]) : 0.0;
+            const double pp = on ? static_cast<double>(P[a * MS + b] + P[b * MS + a]) : 0.0;
+            const double A1 = S.F1 - ga.u1 - gb.u1 + m1;
+            const double A2 = S.F2 - ga.u2 - gb.u2 + m2;
+            v = A1 * A2 + S.QD + ga.g + gb.g - m2 * (ga.u1 + gb.u1) - m1 * (ga.u2 + gb.u2) + 3.0 * m1 * m2 - pp;
+            if (fabs(v) <= zmin && pair_count(Bm, cnt, a, b, S.IF1, S.IF2, S.IQD) <= 0) v = 0.0;
         }
-        store_value(out, h, v);
+        const float f0 = h >= Ht ? 0.f : leaf_first ? leaf0[h] : gp0;
+        out0[h] = static_cast<T>(static_cast<double>(f0) * v);
+        for (int g = 1; g < ng; ++g) {
+            const float f = h >= Ht ? 0.f : gleaf[g] >= 0 ? __ldg(V.leaf + gleaf[g] + h) : gpay[g];
+            V.val[static_cast<size_t>(gnode[g]) * HS + h] = static_cast<T>(static_cast<double>(f) * v);
+        }
     }
 }
 
@@ -965,13 +1269,18 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
         case TK_CR1:
             k_term_cr1<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
-        case TK_CR2:
-            if (cr2_smem<T>() > 48 * 1024)
+        case TK_CR2: {
+            // c.HS: the row stride (the largest of a batch); the staging of two
+            // reach rows in the product's space needs HS <= kMaxHS
+            if (c.HS > kMaxHS) return cudaErrorInvalidValue;
+            const size_t sm = cr2_smem<T>(c.HS);
+            if (sm > 48 * 1024)
                 e = cudaFuncSetAttribute(k_term_cr2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(cr2_smem<T>()));
+                                         static_cast<int>(cr2_smem<T>(kMaxHS)));
             if (e != cudaSuccess) return e;
-            k_term_cr2<T><<<n, kTermThreads, cr2_smem<T>(), s>>>(c, ctxs, items, trav);
+            k_term_cr2<T><<<n, kTermThreads, sm, s>>>(c, ctxs, items, trav);
             break;
+        }
         case TK_SD1:
             if (sd1_smem<T>() > 48 * 1024)
                 e = cudaFuncSetAttribute(k_term_sd1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

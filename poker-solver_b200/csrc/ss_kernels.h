@@ -18,6 +18,7 @@ struct DevCtx {
     const int *fr_off;     // [E + 1]
     const int *fr_items;
     const int *hand_code;  // [np][HS]
+    const short *pair_idx; // [np][52][52] range index of each dense-card pair, -1 if none
     const int *sd_pos;     // [np][HS]
     const unsigned *strength;    // [np][HS]
     const SdCombo *sd_combo;     // [ncomb]
@@ -28,6 +29,7 @@ struct DevCtx {
     int HS;
     int np;
     int ncomb;
+    int deck;              // number of non-board cards (dense card indices 0 .. deck-1)
     int H[SS_MAX_PLAYERS];
     int dup[SS_MAX_PLAYERS];     // range holds some combo more than once
     // root strategy snapshot (batched form: one launch covers many subgames)

@@ -251,12 +251,15 @@ int build_plan(const Problem &pb, Plan *out) {
     for (int b = 0; b < nb && b < 5; ++b)
         if (board[b] >= 0 && board[b] < 52) on_board[board[b]] = true;
     const size_t HS = static_cast<size_t>(P.HS);
+    int dense[52];
+    P.deck = 0;
+    for (int x = 0; x < 52; ++x) dense[x] = on_board[x] ? 63 : P.deck++;
     P.hand_code.assign(static_cast<size_t>(np) * HS, -1);
     for (int p = 0; p < np; ++p)
         for (int h = 0; h < P.H[p]; ++h) {
             const int a = pb.hands[p][2 * h], b = pb.hands[p][2 * h + 1];
             const int blocked = (on_board[a] || on_board[b]) ? 1 : 0;
-            P.hand_code[p * HS + h] = a | (b << 8) | (blocked << 16);
+            P.hand_code[p * HS + h] = a | (b << 8) | (blocked << 16) | (dense[a] << 20) | (dense[b] << 26);
         }
 
     // terminal work lists per traverser
@@ -312,6 +315,26 @@ int build_plan(const Problem &pb, Plan *out) {
                 P.enum_work += w;
             }
             P.term[t][kind].push_back(it);
+        }
+    }
+
+    // two-opponent terminals sharing both opponents' reach rows share their
+    // card-removal mass: order them by the row pair and mark the groups
+    for (int t = 0; t < np; ++t) {
+        std::vector<TermItem> &v = P.term[t][TK_CR2];
+        std::stable_sort(v.begin(), v.end(), [](const TermItem &u, const TermItem &w) {
+            if (u.opp_row[0] != w.opp_row[0]) return u.opp_row[0] < w.opp_row[0];
+            return u.opp_row[1] < w.opp_row[1];
+        });
+        for (size_t i = 0; i < v.size();) {
+            size_t j = i + 1;
+            while (j < v.size() && j - i < static_cast<size_t>(kTermGroupMax) &&
+                   v[j].opp_row[0] == v[i].opp_row[0] && v[j].opp_row[1] == v[i].opp_row[1] &&
+                   v[j].opp_player[0] == v[i].opp_player[0] && v[j].opp_player[1] == v[i].opp_player[1])
+                ++j;
+            v[i].gextra = static_cast<int>(j - i - 1);
+            for (size_t m = i + 1; m < j; ++m) v[m].follow = 1;
+            i = j;
         }
     }
 
@@ -391,6 +414,19 @@ int build_plan(const Problem &pb, Plan *out) {
             if (seen[a * 52 + b]++) P.dup[p] = 1;
         }
     }
+
+    // per player: the range index of each dense-card pair (both orders), -1
+    // where the range has no such hand (or it touches the board); the
+    // two-opponent kernel gathers its combo matrices through it
+    P.pair_idx.assign(static_cast<size_t>(np) * 52 * 52, static_cast<short>(-1));
+    for (int p = 0; p < np; ++p)
+        for (int h = 0; h < P.H[p]; ++h) {
+            const int hc = P.hand_code[p * HS + h];
+            if (hc & 0x10000) continue;
+            const int a = (hc >> 20) & 63, b = (hc >> 26) & 63;
+            P.pair_idx[(static_cast<size_t>(p) * 52 + a) * 52 + b] = static_cast<short>(h);
+            P.pair_idx[(static_cast<size_t>(p) * 52 + b) * 52 + a] = static_cast<short>(h);
+        }
 
     double hsum = 0;
     for (int p = 0; p < np; ++p) hsum += P.H[p];
