@@ -121,7 +121,7 @@ class Batch {
   private:
     struct Launch {
         int type;   // 0 bump, 1 snapshot, 2 terminals, 3 cfv, 4 reach
-        int kind;   // terminal kind
+        int kind;   // terminal kind; value/regret launches: number of long items (at the end)
         int t;      // traverser / player
         size_t off; // item offset in dlists
         int n;
@@ -142,8 +142,8 @@ class Batch {
                 return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
                                     stream, dctx);
             case 3:
-                return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.H, stream, dctx,
-                                  L.t);
+                return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.kind, L.H, stream,
+                                  dctx, L.t);
             default:
                 return launch_reach(cmax, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H, stream,
                                     dctx, L.t);
@@ -211,19 +211,25 @@ class Batch {
             for (int i : act)
                 if (subs[i]->P.np > t) lv = std::max(lv, subs[i]->P.cfv_levels[t].size());
             for (size_t l = 0; l < lv; ++l) {
-                std::vector<CfvItem> items;
+                // every subgame's short items, then every subgame's long ones
+                std::vector<CfvItem> items, longs;
                 int H = 0;
                 for (int i : act) {
                     const Plan &P = subs[i]->P;
                     if (P.np <= t || l >= P.cfv_levels[t].size()) continue;
-                    for (CfvItem it : P.cfv_levels[t][l]) {
+                    const auto &v = P.cfv_levels[t][l];
+                    const size_t n_short = v.size() - static_cast<size_t>(P.cfv_nlong[t][l]);
+                    for (size_t j = 0; j < v.size(); ++j) {
+                        CfvItem it = v[j];
                         it.sg = i;
-                        items.push_back(it);
+                        (j < n_short ? items : longs).push_back(it);
                     }
                     H = std::max(H, P.H[t]);
                 }
+                const int n_long = static_cast<int>(longs.size());
+                items.insert(items.end(), longs.begin(), longs.end());
                 if (!items.empty())
-                    seq.push_back({3, 0, t, put(items.data(), items.size() * sizeof(CfvItem)),
+                    seq.push_back({3, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
                                    static_cast<int>(items.size()), H});
             }
             lv = 0;

@@ -85,6 +85,10 @@ struct alignas(16) CfvItem {
     int pad_[3] = {0, 0, 0};
 };
 
+// A value/regret item whose edges' frontiers hold at least this many rows in
+// total is long: several warps share each of its hand chunks.
+constexpr int kCfvLongFrontier = 48;
+
 // Terminal kinds per traverser.
 enum TermKind : int {
     TK_ZERO = 0,     // value 0 (folded traverser at showdown, leaves without leaf values)
@@ -146,8 +150,10 @@ struct Plan {
     std::vector<int> edge_node;        // [E]
     // per player: reach levels (top-down)
     std::vector<std::vector<ReachItem>> reach_levels[SS_MAX_PLAYERS];
-    // per traverser: cfv levels (bottom-up order)
+    // per traverser: cfv levels (bottom-up order); within a level the items
+    // with long frontiers come last, cfv_nlong of them
     std::vector<std::vector<CfvItem>> cfv_levels[SS_MAX_PLAYERS];
+    std::vector<int> cfv_nlong[SS_MAX_PLAYERS];
     std::vector<int> fr_off;           // [E + 1]
     std::vector<int> fr_items;         // val rows (= node ids)
     std::vector<int> root_fr[SS_MAX_PLAYERS];

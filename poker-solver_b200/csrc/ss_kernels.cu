@@ -81,12 +81,21 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
     const ReachItem I = items[it];
-    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
-    if (h0 >= (ctxs ? c.H[p] : H)) return;
-    const size_t HS = static_cast<size_t>(c.HS);
+    // context fields in registers (a reference to either the parameter or a
+    // batch entry would send every field read through local memory)
+    float *R, *reach;
+    int HSi, Hp;
+    if (ctxs) {
+        const DevCtx &c = ctxs[I.sg];
+        R = c.R, reach = c.reach, HSi = c.HS, Hp = c.H[p];
+    } else {
+        R = c0.R, reach = c0.reach, HSi = c0.HS, Hp = H;
+    }
+    if (h0 >= Hp) return;
+    const size_t HS = static_cast<size_t>(HSi);
     float r[SS_MAX_ACTIONS][4], sig[SS_MAX_ACTIONS][4];
-    regret_match4(c.R, HS, I.first_edge, I.na, I.frozen, h0, r, sig);
-    const float4 pr = ld4(c.reach + static_cast<size_t>(I.parent_row) * HS + h0);
+    regret_match4(R, HS, I.first_edge, I.na, I.frozen, h0, r, sig);
+    const float4 pr = ld4(reach + static_cast<size_t>(I.parent_row) * HS + h0);
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
@@ -95,7 +104,7 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
             o.y = pr.y * sig[a][1];
             o.z = pr.z * sig[a][2];
             o.w = pr.w * sig[a][3];
-            st4(c.reach + static_cast<size_t>(I.first_edge + a) * HS + h0, o);
+            st4(reach + static_cast<size_t>(I.first_edge + a) * HS + h0, o);
         }
     }
 }
@@ -104,59 +113,98 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
 // cfv: value, regret and strategy-sum update at traverser nodes
 // (street_solve.cu:1155-1175): v = sum_a sigma_a ev_a; r_a = (r_a + (ev_a - v))
 // * t/(t+1); s_a += t * sigma_a; ev_a = sum of val over frontier(edge a).
-// Each thread owns 2 hands.  Edge values are gathered first (four frontier
-// rows in flight at a time), then the regrets are loaded and matched, which
-// keeps the live state to the edge values and regrets.
+// Each lane owns 2 hands, each warp 64 consecutive hands.  S == 1: the four
+// warps of a block take four hand chunks and walk whole frontiers, eight row
+// loads in flight.  S > 1 (items with long frontiers, which are few): the S
+// warps of a block share one hand chunk and each sums every S-th frontier
+// row; warp 0 adds the S partial sums in a fixed order and updates.
 // --------------------------------------------------------------------------
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
+// a float2 load kept as a separate L1-cached access (not merged with an
+// earlier load of the same address, so the value need not stay in registers)
+__device__ __forceinline__ float2 ld2_l1(const float *p) {
+    float2 v;
+    asm volatile("ld.global.ca.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void add2(float2 &a, float2 b) {
+    a.x += b.x;
+    a.y += b.y;
+}
 
-__global__ void __launch_bounds__(kCfvThreads) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
+// context fields of the value/regret kernel, copied into registers (see Cr2View)
+struct CfvView {
+    float *R, *S, *val;
+    const int *fr_off, *fr_items, *iter;
+    int HS, H;
+};
+__device__ __forceinline__ CfvView cfv_view(const DevCtx &c, int H) {
+    return CfvView{c.R, c.S, c.val, c.fr_off, c.fr_items, c.iter, c.HS, H};
+}
+
+template <int S>
+__global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                      const CfvItem *__restrict__ items, int nchunk, int Hl,
                                                      int trav) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
-    const int h0 = (ch * kCfvThreads + threadIdx.x) * 2;
     const CfvItem I = items[it];
-    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
-    const int H = ctxs ? c.H[trav] : Hl;
-    if (h0 >= H) return;
-    const size_t HS = static_cast<size_t>(c.HS);
-    const float *val = c.val + h0;
+    const CfvView V = ctxs ? cfv_view(ctxs[I.sg], ctxs[I.sg].H[trav]) : cfv_view(c0, Hl);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h0 = (S == 1 ? ch * (kCfvThreads / 32) + warp : ch) * 64 + lane * 2;
+    const bool act = h0 < V.H;
+    if (S == 1 && !act) return;
+    const size_t HS = static_cast<size_t>(V.HS);
+    const float *val = V.val + h0;
+    const int *__restrict__ fr = V.fr_items;
     float2 ev[SS_MAX_ACTIONS];
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
             float2 e = make_float2(0.f, 0.f);
-            int k = c.fr_off[I.first_edge + a];
-            const int k1 = c.fr_off[I.first_edge + a + 1];
-            for (; k + 4 <= k1; k += 4) {
-                const int n0 = c.fr_items[k], n1 = c.fr_items[k + 1];
-                const int n2 = c.fr_items[k + 2], n3 = c.fr_items[k + 3];
-                const float2 x0 = ld2(val + static_cast<size_t>(n0) * HS);
-                const float2 x1 = ld2(val + static_cast<size_t>(n1) * HS);
-                const float2 x2 = ld2(val + static_cast<size_t>(n2) * HS);
-                const float2 x3 = ld2(val + static_cast<size_t>(n3) * HS);
-                e.x += x0.x; e.y += x0.y;
-                e.x += x1.x; e.y += x1.y;
-                e.x += x2.x; e.y += x2.y;
-                e.x += x3.x; e.y += x3.y;
-            }
-            for (; k < k1; ++k) {
-                const float2 x = ld2(val + static_cast<size_t>(c.fr_items[k]) * HS);
-                e.x += x.x; e.y += x.y;
+            if (act) {
+                int k = V.fr_off[I.first_edge + a] + (S == 1 ? 0 : warp);
+                const int k1 = V.fr_off[I.first_edge + a + 1];
+                for (; k + 7 * S < k1; k += 8 * S) {
+                    float2 x[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) x[i] = ld2(val + static_cast<size_t>(__ldg(fr + k + i * S)) * HS);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) add2(e, x[i]);
+                }
+                for (; k < k1; k += S) add2(e, ld2(val + static_cast<size_t>(__ldg(fr + k)) * HS));
             }
             ev[a] = e;
         }
     }
-    float2 r[SS_MAX_ACTIONS];
+    if constexpr (S > 1) {
+        __shared__ float2 part[S][SS_MAX_ACTIONS][32];
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+            if (a < I.na) part[warp][a][lane] = ev[a];
+        __syncthreads();
+        if (warp != 0 || !act) return;
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+            if (a < I.na) {
+                float2 e = part[0][a][lane];
+#pragma unroll
+                for (int w = 1; w < S; ++w) add2(e, part[w][a][lane]);
+                ev[a] = e;
+            }
+        }
+    }
+    // the regrets are read three times (sum, value, update) instead of being
+    // held in registers; the rereads hit L1
+    const float *Rh = V.R + static_cast<size_t>(I.first_edge) * HS + h0;
     float s0 = 0.f, s1 = 0.f;
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
-            r[a] = ld2(c.R + static_cast<size_t>(I.first_edge + a) * HS + h0);
-            s0 += r[a].x > 0.f ? r[a].x : 0.f;
-            s1 += r[a].y > 0.f ? r[a].y : 0.f;
+            const float2 r = ld2_l1(Rh + a * HS);
+            s0 += r.x > 0.f ? r.x : 0.f;
+            s1 += r.y > 0.f ? r.y : 0.f;
         }
     }
     const float uni = 1.0f / static_cast<float>(I.na);
@@ -170,28 +218,30 @@ __global__ void __launch_bounds__(kCfvThreads) k_cfv(DevCtx c0, const DevCtx *__
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
-            v0 += sigma(a, r[a].x, s0, inv0) * ev[a].x;
-            v1 += sigma(a, r[a].y, s1, inv1) * ev[a].y;
+            const float2 r = ld2_l1(Rh + a * HS);
+            v0 += sigma(a, r.x, s0, inv0) * ev[a].x;
+            v1 += sigma(a, r.y, s1, inv1) * ev[a].y;
         }
     }
-    const int t = *c.iter;
+    const int t = *V.iter;
     const float d = static_cast<float>(t) / (static_cast<float>(t) + 1.0f);
     const float w = static_cast<float>(t);
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
         if (a < I.na) {
             const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
-            const float2 sm = ld2(c.S + off);
+            const float2 r = ld2_l1(Rh + a * HS);
+            const float2 sm = ld2(V.S + off);
             float2 nr, ns;
-            nr.x = (r[a].x + (ev[a].x - v0)) * d;
-            nr.y = (r[a].y + (ev[a].y - v1)) * d;
-            ns.x = sm.x + w * sigma(a, r[a].x, s0, inv0);
-            ns.y = sm.y + w * sigma(a, r[a].y, s1, inv1);
-            st2(c.R + off, nr);
-            st2(c.S + off, ns);
+            nr.x = (r.x + (ev[a].x - v0)) * d;
+            nr.y = (r.y + (ev[a].y - v1)) * d;
+            ns.x = sm.x + w * sigma(a, r.x, s0, inv0);
+            ns.y = sm.y + w * sigma(a, r.y, s1, inv1);
+            st2(V.R + off, nr);
+            st2(V.S + off, ns);
         }
     }
-    st2(c.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0, v1));
+    st2(V.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0, v1));
 }
 
 // --------------------------------------------------------------------------
@@ -1246,11 +1296,19 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s,
+cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
                        const DevCtx *ctxs, int trav) {
     if (n <= 0 || H <= 0) return cudaSuccess;
-    const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
-    k_cfv<<<n * nc, kCfvThreads, 0, s>>>(c, ctxs, items, nc, H, trav);
+    n_long = n_long < 0 ? 0 : n_long > n ? n : n_long;
+    const int n_short = n - n_long;
+    if (n_short > 0) {
+        const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
+        k_cfv<1><<<n_short * nc, kCfvThreads, 0, s>>>(c, ctxs, items, nc, H, trav);
+    }
+    if (n_long > 0) {
+        const int nc = (H + 63) / 64;
+        k_cfv<kCfvThreads / 32><<<n_long * nc, kCfvThreads, 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
+    }
     return cudaGetLastError();
 }
 

@@ -51,7 +51,8 @@ constexpr int kTermThreads = 256;
 // count of the launch).
 cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
                          const DevCtx *ctxs = nullptr, int player = -1);
-cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int H, cudaStream_t s,
+// The last n_long items (long frontiers) run with four warps per hand chunk.
+cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
                        const DevCtx *ctxs = nullptr, int trav = -1);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s, const DevCtx *ctxs = nullptr);

@@ -251,9 +251,9 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
             for (int k = 0; k < TK_COUNT; ++k)
                 NA_CK(launch_terms(c, k, reinterpret_cast<const TermItem *>(base + o_term[t][k]),
                                    static_cast<int>(P.term[t][k].size()), t, s0));
-            for (auto &lv : cfv_lv[t])
-                NA_CK(launch_cfv(c, reinterpret_cast<const CfvItem *>(base + o_cfv[t]) + lv.first, lv.second,
-                                 P.H[t], s0));
+            for (size_t l = 0; l < cfv_lv[t].size(); ++l)
+                NA_CK(launch_cfv(c, reinterpret_cast<const CfvItem *>(base + o_cfv[t]) + cfv_lv[t][l].first,
+                                 cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t], s0));
             NA_CK(reach(t));
         }
     }

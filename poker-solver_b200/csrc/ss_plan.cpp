@@ -242,6 +242,15 @@ int build_plan(const Problem &pb, Plan *out) {
             it.node = x;
             P.cfv_levels[t][h].push_back(it);
         }
+        P.cfv_nlong[t].assign(P.cfv_levels[t].size(), 0);
+        for (size_t l = 0; l < P.cfv_levels[t].size(); ++l) {
+            auto &v = P.cfv_levels[t][l];
+            auto is_short = [&](const CfvItem &it) {
+                return P.fr_off[it.first_edge + it.na] - P.fr_off[it.first_edge] < kCfvLongFrontier;
+            };
+            auto mid = std::stable_partition(v.begin(), v.end(), is_short);
+            P.cfv_nlong[t][l] = static_cast<int>(v.end() - mid);
+        }
     }
 
     // board and hand tables

@@ -130,8 +130,8 @@ class Session {
         for (size_t l = 0; l < cfv_lv[t].size(); ++l) {
             e = mark(PC_CFV, cfv_bytes[t][l]);
             if (e == cudaSuccess)
-                e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.H[t],
-                               stream);
+                e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.cfv_nlong[t][l],
+                               P.H[t], stream);
             if (e != cudaSuccess) return e;
         }
         return reach(t);
