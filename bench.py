@@ -313,12 +313,15 @@ def run_ours(args, world, rank, local):
     if not peak:
         peak = 6650.0
     d = classes[dom]
+    # per launch: algorithmic bytes and average event-timed duration (their
+    # ratio equals bytes per iteration over time per iteration)
+    n_launch = max(1, d["launches"])
     achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else 0.0
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
         if dom in tr.get("classes", {}):
-            traffic = tr["classes"][dom].get("dram_bytes_per_iteration")
+            traffic = tr["classes"][dom].get("dram_bytes_per_launch")
     except Exception:
         pass
 
@@ -333,8 +336,9 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(args.steps * (args.iterations * launches_per_iter + reach_launches)),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "bytes_per_iteration": d["bytes"],
-                     "kernel_ms_per_iteration": d["ms"]},
+                     "traffic": traffic, "bytes_per_launch": d["bytes"] / n_launch,
+                     "launch_ms": d["ms"] / n_launch, "launches_per_iteration": d["launches"],
+                     "bytes_per_iteration": d["bytes"], "kernel_ms_per_iteration": d["ms"]},
         "profile": {k: {"ms": round(v["ms"], 4), "launches": v["launches"],
                         "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
                     for k, v in classes.items() if v["launches"]},

@@ -205,7 +205,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.fr_off = reinterpret_cast<const int *>(dbase + o_fr_off);
     c.fr_items = reinterpret_cast<const int *>(dbase + o_fr_items);
     c.hand_code = reinterpret_cast<const int *>(dbase + o_code);
-    c.pair_idx = reinterpret_cast<const short *>(dbase + o_pair);
+    c.pair_idx = reinterpret_cast<const int *>(dbase + o_pair);
     c.sd_pos = reinterpret_cast<const int *>(dbase + o_sdpos);
     c.strength = reinterpret_cast<const unsigned *>(dbase + o_str);
     c.sd_combo = reinterpret_cast<const SdCombo *>(dbase + o_sdc);

@@ -164,7 +164,7 @@ struct Plan {
     // board card); -1 padding
     std::vector<int> hand_code;
     int deck = 0;                      // number of non-board cards
-    std::vector<short> pair_idx;       // [np][52][52] range index of each dense-card pair, -1 if none
+    std::vector<int> pair_idx;         // [np][52][52] range index of each dense-card pair, HS if none
     // showdown tables (river only)
     int ncomb = 0;
     std::vector<SdCombo> sd_combo;     // [ncomb]

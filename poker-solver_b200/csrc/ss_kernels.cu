@@ -499,20 +499,17 @@ __device__ __forceinline__ void scatter_dense(const int *__restrict__ code, int 
 
 // The same matrices gathered instead (ranges without a repeated combo): each
 // thread fills 4-column chunks of rows 0 .. Dp-1 through the player's table of
-// range indices per dense-card pair, so every cell is written once, with
-// conflict-free 16-byte stores and no clearing pass.  Cells outside rows and
-// columns 0 .. Dp-1 are left unset; nothing reads them.
+// range indices per dense-card pair (missing pairs index the zero kept after
+// the staged row), so every cell is written once, with 16-byte stores and no
+// clearing pass.  Cells outside rows and columns 0 .. Dp-1 are left unset;
+// nothing reads them.
 template <class T>
-__device__ __forceinline__ void gather_dense(const short *__restrict__ tab, const T *r, T *M, int Dp) {
+__device__ __forceinline__ void gather_dense(const int *__restrict__ tab, const T *r, T *M, int Dp) {
     const int chunk = threadIdx.x & 15, c0 = chunk * 4;
     if (c0 >= Dp) return;
     for (int row = threadIdx.x >> 4; row < Dp; row += kTermThreads / 16) {
-        const short4 ix = __ldg(reinterpret_cast<const short4 *>(tab + row * 52 + c0));
-        T v[4];
-        v[0] = ix.x >= 0 ? r[ix.x] : T(0);
-        v[1] = ix.y >= 0 ? r[ix.y] : T(0);
-        v[2] = ix.z >= 0 ? r[ix.z] : T(0);
-        v[3] = ix.w >= 0 ? r[ix.w] : T(0);
+        const int4 ix = __ldg(reinterpret_cast<const int4 *>(tab + row * 52 + c0));
+        const T v[4] = {r[ix.x], r[ix.y], r[ix.z], r[ix.w]};
         store4(M + row * MS + c0, v);
     }
 }
@@ -526,7 +523,7 @@ struct Cr2View {
     const T *reach;
     T *val;
     const int *code_t, *code0, *code1;   // hand codes of the traverser and the two opponents
-    const short *tab0, *tab1;            // dense-pair tables of the two opponents
+    const int *tab0, *tab1;              // dense-pair tables of the two opponents
     const float *leaf;
     int HS, deck, Ht, H0, H1;
     bool dup;
@@ -755,7 +752,8 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     int *gnode = cv.take<int>(kTermGroupMax);
     int *gleaf = cv.take<int>(kTermGroupMax);
     float *gpay = cv.take<float>(kTermGroupMax);
-    T *r1 = P, *r2 = P + HS;                    // staged reach rows (P is written after the scatter)
+    // staged reach rows, each followed by a zero (P is written after the gather)
+    T *r1 = P, *r2 = P + HS + 16 / sizeof(T);
 
     // staging: both opponents' reach rows (16-byte chunks; rows start on
     // 128-byte boundaries) and the first terminal's leaf row (4-byte words)
@@ -777,6 +775,10 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
             gnode[tid] = I.node;
             gleaf[tid] = I.leaf_off;
             gpay[tid] = I.payoff;
+        }
+        if (tid == 0) {
+            r1[HS] = T(0);
+            r2[HS] = T(0);
         }
     }
     if (V.dup) {

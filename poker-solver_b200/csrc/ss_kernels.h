@@ -18,7 +18,7 @@ struct DevCtx {
     const int *fr_off;     // [E + 1]
     const int *fr_items;
     const int *hand_code;  // [np][HS]
-    const short *pair_idx; // [np][52][52] range index of each dense-card pair, -1 if none
+    const int *pair_idx;   // [np][52][52] range index of each dense-card pair, HS if none
     const int *sd_pos;     // [np][HS]
     const unsigned *strength;    // [np][HS]
     const SdCombo *sd_combo;     // [ncomb]

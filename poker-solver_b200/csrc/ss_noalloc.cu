@@ -171,7 +171,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     const size_t o_fr_off = up(P.fr_off.data(), P.fr_off.size() * sizeof(int));
     const size_t o_fr_items = up(P.fr_items.data(), P.fr_items.size() * sizeof(int));
     const size_t o_code = up(P.hand_code.data(), P.hand_code.size() * sizeof(int));
-    const size_t o_pair = up(P.pair_idx.data(), P.pair_idx.size() * sizeof(short));
+    const size_t o_pair = up(P.pair_idx.data(), P.pair_idx.size() * sizeof(int));
     const size_t o_sdpos = up(P.sd_pos.data(), P.sd_pos.size() * sizeof(int));
     const size_t o_str = up(P.strength.data(), P.strength.size() * sizeof(uint32_t));
     const size_t o_sdc = up(P.sd_combo.data(), P.sd_combo.size() * sizeof(SdCombo));
@@ -211,7 +211,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     c.fr_off = reinterpret_cast<const int *>(base + o_fr_off);
     c.fr_items = reinterpret_cast<const int *>(base + o_fr_items);
     c.hand_code = reinterpret_cast<const int *>(base + o_code);
-    c.pair_idx = reinterpret_cast<const short *>(base + o_pair);
+    c.pair_idx = reinterpret_cast<const int *>(base + o_pair);
     c.sd_pos = reinterpret_cast<const int *>(base + o_sdpos);
     c.strength = reinterpret_cast<const unsigned *>(base + o_str);
     c.sd_combo = reinterpret_cast<const SdCombo *>(base + o_sdc);

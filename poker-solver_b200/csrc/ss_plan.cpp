@@ -424,17 +424,18 @@ int build_plan(const Problem &pb, Plan *out) {
         }
     }
 
-    // per player: the range index of each dense-card pair (both orders), -1
-    // where the range has no such hand (or it touches the board); the
-    // two-opponent kernel gathers its combo matrices through it
-    P.pair_idx.assign(static_cast<size_t>(np) * 52 * 52, static_cast<short>(-1));
+    // per player: the range index of each dense-card pair (both orders), HS
+    // where the range has no such hand (or it touches the board) -- the
+    // two-opponent kernel keeps a zero after each staged reach row -- so it
+    // gathers its combo matrices through this table without tests
+    P.pair_idx.assign(static_cast<size_t>(np) * 52 * 52, P.HS);
     for (int p = 0; p < np; ++p)
         for (int h = 0; h < P.H[p]; ++h) {
             const int hc = P.hand_code[p * HS + h];
             if (hc & 0x10000) continue;
             const int a = (hc >> 20) & 63, b = (hc >> 26) & 63;
-            P.pair_idx[(static_cast<size_t>(p) * 52 + a) * 52 + b] = static_cast<short>(h);
-            P.pair_idx[(static_cast<size_t>(p) * 52 + b) * 52 + a] = static_cast<short>(h);
+            P.pair_idx[(static_cast<size_t>(p) * 52 + a) * 52 + b] = h;
+            P.pair_idx[(static_cast<size_t>(p) * 52 + b) * 52 + a] = h;
         }
 
     double hsum = 0;
