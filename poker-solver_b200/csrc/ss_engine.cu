@@ -61,7 +61,7 @@ void keep_pool_warm(int device) {
 }
 
 const char *kClassName[SS_PROFILE_CLASSES] = {"reach", "cfv", "term_fill", "term_cr1",
-                                             "term_cr2", "term_sd1", "term_enum", "other"};
+                                             "term_cr2", "term_sd", "term_enum", "other"};
 
 }  // namespace
 
@@ -153,6 +153,8 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     const size_t o_sdc = b.add(P.sd_combo);
     const size_t o_sdl = b.add(P.sd_card_list);
     const size_t o_sdp = b.add(P.sd_card_partner);
+    const size_t o_ph = b.add(P.pos_hand);
+    const size_t o_seg = b.add(P.sd_seg);
     std::vector<int> dfe, dna, dpl;
     for (int x : P.dec_nodes) {
         dfe.push_back(P.first_edge[x]);
@@ -211,6 +213,9 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.sd_combo = reinterpret_cast<const SdCombo *>(dbase + o_sdc);
     c.sd_card_list = reinterpret_cast<const short *>(dbase + o_sdl);
     c.sd_card_partner = reinterpret_cast<const short *>(dbase + o_sdp);
+    c.pos_hand = reinterpret_cast<const int *>(dbase + o_ph);
+    c.sd_seg = reinterpret_cast<const int *>(dbase + o_seg);
+    for (int p = 0; p <= SS_MAX_PLAYERS; ++p) c.sd_seg_off[p] = P.sd_seg_off[p];
     c.leaf_values = dleaf;
     c.iter = diter;
     c.HS = P.HS;

@@ -97,7 +97,8 @@ enum TermKind : int {
     TK_CR2 = 3,      // fold / leaf with two counted opponents
     TK_SD1 = 4,      // showdown against one live opponent
     TK_ENUM = 5,     // anything else: exact tuple enumeration (small ranges only)
-    TK_COUNT = 6
+    TK_SD2 = 6,      // three-way showdown (two live opponents), ranges without repeated combos
+    TK_COUNT = 7
 };
 
 // One terminal for one traverser.  factor: payoff for folds; leaf_off >= 0
@@ -132,6 +133,7 @@ struct alignas(16) SdCombo {
     int lo, hi;
     short c1, c2;
     short l1lo, l1hi, l2lo, l2hi;
+    unsigned char d1, d2;     // dense indices of c1, c2 (rank among the non-board cards)
 };
 
 // ---------------------------------------------------------------------------
@@ -171,6 +173,13 @@ struct Plan {
     std::vector<short> sd_card_list;   // [52][52] rank positions of the combos holding each card
     std::vector<short> sd_card_partner;// [52][52] the other card of each of those combos
     std::vector<int> sd_pos;           // [np][HS], -1 if blocked / padding
+    std::vector<int> pos_hand;         // [np][ncomb] hand index at each rank position, -1 if none
+    // per player, the rank axis cut into segments for the three-way showdown
+    // sweep: {lo, hi, holds a hand of the player, 0}; a segment is one tie
+    // group holding some of the player's hands, or a run of groups holding
+    // none.  Player p's segments are sd_seg[sd_seg_off[p] .. sd_seg_off[p+1]).
+    std::vector<int> sd_seg;           // 4 ints per segment
+    int sd_seg_off[SS_MAX_PLAYERS + 1] = {};
     std::vector<uint32_t> strength;    // [np][HS], 0 if blocked / padding
     int dup[SS_MAX_PLAYERS] = {};      // range holds some combo more than once
     double enum_work = 0;              // tuple visits per iteration on TK_ENUM

@@ -911,9 +911,9 @@ constexpr size_t sd1_smem() {
     return 1326 * sizeof(T) + 1327 * 8 + 52 * 53 * 8 + 52 * 4 + (kTermThreads / 32) * 8 + 52 * 8 + 64;
 }
 
-// Showdown against one live opponent (street_solve.cu:886-903): with W, T, S
-// the opponent reach on compatible hands that are weaker, tied and in total,
-// value = pot W + pot/2 T - bet S.  Combos are ranked once per board; the
+// Showdown against one live opponent (street_solve.cu:886-903): with W, T, L
+// the opponent reach on compatible hands that are weaker, tied and stronger,
+// value = (pot - bet) W + (pot/2 - bet) T - bet L.  Combos are ranked once per board; the
 // block builds the opponent's reach in rank order, its prefix sums P and
 // per-card prefix sums PC[c], and then for a traverser combo (c1, c2) with
 // tie group [lo, hi):
@@ -1023,7 +1023,11 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
     const int Ht = c.H[trav];
     const int *tpos = c.sd_pos + static_cast<size_t>(trav) * c.HS;
     T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
-    const double pot = I.pot, bet = I.bet;
+    // payoff per class with the reference's float coefficients (win pot - bet,
+    // tie pot * 0.5 - bet, loss -bet): a coefficient that is exactly 0 drops
+    // its class exactly, as in the reference's sum
+    const double cw = static_cast<double>(I.pot - I.bet), ct = static_cast<double>(I.pot * 0.5f - I.bet);
+    const double cl = -static_cast<double>(I.bet);
     const int np_ = *npos;
     for (int h = tid; h < c.HS; h += blockDim.x) {
         double v = 0.0;
@@ -1037,11 +1041,315 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
                 const double W = Pp[s.lo] - p1[s.l1lo] - p2[s.l2lo];
                 const double Tt = (Pp[s.hi] - Pp[s.lo]) - (p1[s.l1hi] - p1[s.l1lo]) -
                                   (p2[s.l2hi] - p2[s.l2lo]) + self;
-                const double S = Pp[nc] - p1[clen[s.c1]] - p2[clen[s.c2]] + self;
-                v = pot * W + 0.5 * pot * Tt - bet * S;
+                const double L = (Pp[nc] - Pp[s.hi]) - (p1[clen[s.c1]] - p1[s.l1hi]) - (p2[clen[s.c2]] - p2[s.l2hi]);
+                v = cw * W + ct * Tt + cl * L;
             }
         }
         store_value(out, h, v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Three-way showdown (two live opponents), street_solve.cu:936-1002: the
+// traverser (strength s) against opponents 1, 2 on disjoint hands o1, o2
+// wins pot / (1 + number of opponents tying s) - bet if neither opponent is
+// stronger, else loses bet.  With D(X, Y) the mass of opponent pairs
+// (o1 in X, o2 in Y) disjoint from each other and from the hand, and L / E
+// the opponents' hands weaker than / tying s, the classes are W2 = D(L, L)
+// (win), T1 = D(E, L) + D(L, E) (two-way tie), T2 = D(E, E) (three-way tie)
+// and the rest of Z = D(all, all) (loss).
+// D(X, Y) is the two-opponent card-removal closed form on matrices holding
+// only X's and Y's hands.  The kernel sweeps the combos in rank order and
+// keeps that form's aggregates (P = M1 M2, u_i, w, d, F_i, Q, D; FP64) for
+// the opponents' hands added so far; per tie group of the traverser's hands
+// it reads A = D(L, L) before the group, B = D(L+E, L) after adding
+// opponent 1's group hands and C = D(L+E, L+E) after opponent 2's, and sums
+// D(L, E) directly over opponent 2's group hands (each term an exact
+// four-card removal for opponent 1).  With Z read after the sweep:
+//   W2 = A, T1 = (B - A) + D(L, E), T2 = (C - B) - D(L, E), lose = Z - C,
+//   value = (pot - bet) W2 + (pot/2 - bet) T1 + (pot/3 - bet) T2 - bet lose.
+// Adding a hand changes one row and column of P and every w entry, so each
+// phase gives threads fixed ownership (P columns or rows, w entries, the
+// scalars, matrix cells) and loops over the phase's hands: no atomics, a
+// fixed summation order.  One block per terminal.
+// ---------------------------------------------------------------------------
+constexpr int SD2_S = 49;   // row stride of the sweep's 47-card matrices (odd: conflict-free columns)
+
+template <class T>
+constexpr size_t sd2_smem(int HS, int ncomb) {
+    return SD2_S * SD2_S * 8 + 2 * SD2_S * SD2_S * sizeof(T) + 4 * 64 * 8 + 8 * 8 + static_cast<size_t>(HS) * 32 +
+           2 * static_cast<size_t>(ncomb) * sizeof(T) + 53 * sizeof(ulonglong2) + 53 * sizeof(Cr2Cnt) +
+           sizeof(Cr2Scalars) + 16 * 16;
+}
+
+struct Sd2State {
+    double *P, *u1, *u2, *w, *d, *sc;   // sc: F1, F2, Q, D
+};
+
+// D(., .) of the hand (a, b) on the current sweep state (the two-opponent
+// closed form, see k_term_cr2)
+// Written with explicit round-to-nearest operations (no contraction into
+// FMAs), so two evaluations on the same state agree bit for bit wherever they
+// are inlined: the class masses below are differences of such evaluations and
+// must come out exactly 0 when the class is empty and the states coincide.
+template <class T>
+__device__ __forceinline__ double sd2_mass(const Sd2State &st, const T *M1, const T *M2, int a, int b) {
+    const double u1a = st.u1[a], u1b = st.u1[b], u2a = st.u2[a], u2b = st.u2[b];
+    const double m1 = static_cast<double>(M1[a * SD2_S + b]), m2 = static_cast<double>(M2[a * SD2_S + b]);
+    const double pp = __dadd_rn(st.P[a * SD2_S + b], st.P[b * SD2_S + a]);
+    const double ga = __dsub_rn(__dadd_rn(__dmul_rn(u1a, u2a), st.w[a]), __dmul_rn(2.0, st.d[a]));
+    const double gb = __dsub_rn(__dadd_rn(__dmul_rn(u1b, u2b), st.w[b]), __dmul_rn(2.0, st.d[b]));
+    const double A1 = __dadd_rn(__dsub_rn(__dsub_rn(st.sc[0], u1a), u1b), m1);
+    const double A2 = __dadd_rn(__dsub_rn(__dsub_rn(st.sc[1], u2a), u2b), m2);
+    double z = __dmul_rn(A1, A2);
+    z = __dadd_rn(z, __dsub_rn(st.sc[3], st.sc[2]));
+    z = __dadd_rn(z, __dadd_rn(ga, gb));
+    z = __dsub_rn(z, __dmul_rn(m2, __dadd_rn(u1a, u1b)));
+    z = __dsub_rn(z, __dmul_rn(m1, __dadd_rn(u2a, u2b)));
+    z = __dadd_rn(z, __dmul_rn(3.0, __dmul_rn(m1, m2)));
+    return __dsub_rn(z, pp);
+}
+
+// Add the hands of opponent `who` (0 or 1) at rank positions [lo, hi) to the
+// sweep state.  R: that opponent's reach by rank position; Mo: that
+// opponent's matrix, Mx: the other's; uo / ux: their card sums.
+template <class T>
+__device__ __forceinline__ void sd2_add(const Sd2State &st, const SdCombo *__restrict__ cb, const T *R, T *Mo,
+                                        const T *Mx, double *uo, const double *ux, int who, int lo, int hi) {
+    const int tid = threadIdx.x;
+    if (tid < SD2_S) {
+        // P = M1 M2: opponent 1's hand {x, y} adds to rows x, y (thread = column);
+        // opponent 2's adds to columns x, y (thread = row)
+        const int j = tid;
+        for (int q = lo; q < hi; ++q) {
+            const double r = static_cast<double>(R[q]);
+            if (r == 0.0) continue;
+            const int x = cb[q].d1, y = cb[q].d2;
+            if (who == 0) {
+                st.P[x * SD2_S + j] += r * static_cast<double>(Mx[y * SD2_S + j]);
+                st.P[y * SD2_S + j] += r * static_cast<double>(Mx[x * SD2_S + j]);
+            } else {
+                st.P[j * SD2_S + x] += r * static_cast<double>(Mx[j * SD2_S + y]);
+                st.P[j * SD2_S + y] += r * static_cast<double>(Mx[j * SD2_S + x]);
+            }
+        }
+    } else if (tid >= 64 && tid < 64 + SD2_S) {
+        // w = M2 u1 + M1 u2: the card sums of this opponent change at x, y,
+        // its matrix at (x, y)
+        const int c = tid - 64;
+        double acc = 0.0;
+        for (int q = lo; q < hi; ++q) {
+            const double r = static_cast<double>(R[q]);
+            if (r == 0.0) continue;
+            const int x = cb[q].d1, y = cb[q].d2;
+            acc += r * (static_cast<double>(Mx[c * SD2_S + x]) + static_cast<double>(Mx[c * SD2_S + y]));
+            if (c == x) acc += r * ux[y];
+            if (c == y) acc += r * ux[x];
+        }
+        st.w[c] += acc;
+    } else if (tid == 128) {
+        double F = st.sc[who], Q = st.sc[2], D = st.sc[3];
+        for (int q = lo; q < hi; ++q) {
+            const double r = static_cast<double>(R[q]);
+            if (r == 0.0) continue;
+            const int x = cb[q].d1, y = cb[q].d2;
+            const double m = static_cast<double>(Mx[x * SD2_S + y]);
+            Q += r * (ux[x] + ux[y]);
+            D += r * m;
+            st.d[x] += r * m;
+            st.d[y] += r * m;
+            uo[x] += r;
+            uo[y] += r;
+            F += r;
+        }
+        st.sc[who] = F;
+        st.sc[2] = Q;
+        st.sc[3] = D;
+    } else if (tid >= 160) {
+        for (int q = lo + tid - 160; q < hi; q += kTermThreads - 160) {
+            const T r = R[q];
+            if (r == T(0)) continue;
+            const int x = cb[q].d1, y = cb[q].d2;
+            Mo[x * SD2_S + y] = r;
+            Mo[y * SD2_S + x] = r;
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                           const TermItem *__restrict__ items, int trav) {
+    extern __shared__ __align__(16) char smem[];
+    const TermItem I = items[blockIdx.x];
+    const int o1 = I.opp_player[0], o2 = I.opp_player[1];
+    const T *reach;
+    T *val;
+    const int *pos_hand, *seg, *sd_pos;
+    const SdCombo *cb;
+    int HS, nc, Ht, s0, s1;
+    {
+        const DevCtx &c = ctxs ? ctxs[I.sg] : c0;   // read once into registers below
+        reach = reach_rows<T>(c);
+        val = val_rows<T>(c);
+        pos_hand = c.pos_hand;
+        seg = c.sd_seg;
+        sd_pos = c.sd_pos;
+        cb = c.sd_combo;
+        HS = c.HS;
+        nc = c.ncomb;
+        Ht = c.H[trav];
+        s0 = c.sd_seg_off[trav];
+        s1 = c.sd_seg_off[trav + 1];
+    }
+    const int tid = threadIdx.x, lane = tid & 31;
+    Carve cv{smem};
+    Sd2State st;
+    st.P = cv.take<double>(SD2_S * SD2_S);
+    T *M1 = cv.take<T>(SD2_S * SD2_S);
+    T *M2 = cv.take<T>(SD2_S * SD2_S);
+    st.u1 = cv.take<double>(64);
+    st.u2 = cv.take<double>(64);
+    st.w = cv.take<double>(64);
+    st.d = cv.take<double>(64);
+    st.sc = cv.take<double>(8);
+    double *cls = cv.take<double>(4 * HS);   // per traverser hand: A, D(L, E), B, C
+    T *R1 = cv.take<T>(nc);
+    T *R2 = cv.take<T>(nc);
+    ulonglong2 *Bm = cv.take<ulonglong2>(53);
+    Cr2Cnt *cnt = cv.take<Cr2Cnt>(53);
+    Cr2Scalars *sc2 = cv.take<Cr2Scalars>(1);
+
+    // opponents' reach by rank position; everything else starts at zero
+    {
+        const T *ra = reach + static_cast<size_t>(I.opp_row[0]) * HS;
+        const T *rb = reach + static_cast<size_t>(I.opp_row[1]) * HS;
+        const int *pa = pos_hand + static_cast<size_t>(o1) * nc, *pb = pos_hand + static_cast<size_t>(o2) * nc;
+        for (int q = tid; q < nc; q += kTermThreads) {
+            const int ha = __ldg(pa + q), hb = __ldg(pb + q);
+            R1[q] = ha >= 0 ? ra[ha] : T(0);
+            R2[q] = hb >= 0 ? rb[hb] : T(0);
+        }
+        for (int i = tid; i < SD2_S * SD2_S; i += kTermThreads) {
+            st.P[i] = 0.0;
+            M1[i] = T(0);
+            M2[i] = T(0);
+        }
+        if (tid < 64) {
+            st.u1[tid] = 0.0;
+            st.u2[tid] = 0.0;
+            st.w[tid] = 0.0;
+            st.d[tid] = 0.0;
+        }
+        if (tid < 8) st.sc[tid] = 0.0;
+    }
+    __syncthreads();
+
+    const int *ph_t = pos_hand + static_cast<size_t>(trav) * nc;
+    for (int si = s0; si < s1; ++si) {
+        const int lo = __ldg(seg + 4 * si), hi = __ldg(seg + 4 * si + 1), has = __ldg(seg + 4 * si + 2);
+        if (has) {
+            // opponents' hands weaker than the group: A, and D(L, E) summed
+            // over opponent 2's group hands (opponent 1 avoiding four cards)
+            for (int q = lo + tid; q < hi; q += kTermThreads) {
+                const int h = __ldg(ph_t + q);
+                if (h < 0) continue;
+                const int a = cb[q].d1, b = cb[q].d2;
+                const double A = sd2_mass(st, M1, M2, a, b);
+                const double F1 = st.sc[0], u1a = st.u1[a], u1b = st.u1[b];
+                const double m1ab = static_cast<double>(M1[a * SD2_S + b]);
+                double dle = 0.0;
+                for (int q2 = lo; q2 < hi; ++q2) {
+                    const double r = static_cast<double>(R2[q2]);
+                    if (r == 0.0) continue;
+                    const int x = cb[q2].d1, y = cb[q2].d2;
+                    if (x == a || x == b || y == a || y == b) continue;
+                    const double avoid = F1 - u1a - u1b - st.u1[x] - st.u1[y] + m1ab +
+                                         static_cast<double>(M1[a * SD2_S + x]) + static_cast<double>(M1[a * SD2_S + y]) +
+                                         static_cast<double>(M1[b * SD2_S + x]) + static_cast<double>(M1[b * SD2_S + y]) +
+                                         static_cast<double>(M1[x * SD2_S + y]);
+                    dle += r * avoid;
+                }
+                cls[4 * h] = A;
+                cls[4 * h + 1] = dle;
+            }
+            __syncthreads();
+        }
+        sd2_add(st, cb, R1, M1, M2, st.u1, st.u2, 0, lo, hi);
+        __syncthreads();
+        if (has) {
+            for (int q = lo + tid; q < hi; q += kTermThreads) {
+                const int h = __ldg(ph_t + q);
+                if (h >= 0) cls[4 * h + 2] = sd2_mass(st, M1, M2, cb[q].d1, cb[q].d2);
+            }
+            __syncthreads();
+        }
+        sd2_add(st, cb, R2, M2, M1, st.u2, st.u1, 1, lo, hi);
+        __syncthreads();
+        if (has) {
+            for (int q = lo + tid; q < hi; q += kTermThreads) {
+                const int h = __ldg(ph_t + q);
+                if (h >= 0) cls[4 * h + 3] = sd2_mass(st, M1, M2, cb[q].d1, cb[q].d2);
+            }
+            __syncthreads();
+        }
+    }
+
+    // all hands added: Z, and the exact positive-pair count for hands whose
+    // mass is within the error bound of zero (masks over the 47-card matrices)
+    if (tid < 2 * 64) {
+        const int col = tid & 63;
+        const T *M = tid < 64 ? M1 : M2;
+        unsigned long long B = 0ull;
+        if (col < SD2_S - 2)
+            for (int r = 0; r < SD2_S - 2; ++r) B |= static_cast<unsigned long long>(M[r * SD2_S + col] > T(0)) << r;
+        if (col <= kCr2Off) {
+            if (tid < 64)
+                Bm[col].x = B;
+            else
+                Bm[col].y = B;
+        }
+    }
+    __syncthreads();
+    if (tid <= kCr2Off) cnt[tid] = Cr2Cnt{__popcll(Bm[tid].x), __popcll(Bm[tid].y), 0, 0};
+    __syncthreads();
+    if (tid < 32) {
+        int n1 = 0, n2 = 0, nq = 0, nd = 0;
+        for (int k = lane; k <= kCr2Off; k += 32) {
+            n1 += cnt[k].n1;
+            n2 += cnt[k].n2;
+            nq += cnt[k].n1 * cnt[k].n2;
+            nd += __popcll(Bm[k].x & Bm[k].y);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+            nq += __shfl_xor_sync(0xffffffffu, nq, o);
+            nd += __shfl_xor_sync(0xffffffffu, nd, o);
+        }
+        if (lane == 0) *sc2 = Cr2Scalars{0.0, 0.0, 0.0, n1 / 2, n2 / 2, nd / 2 - nq, 0};
+    }
+    __syncthreads();
+    const Cr2Scalars S2 = *sc2;
+    const double zmin = 1e-4 * st.sc[0] * st.sc[1];
+    // payoff per class with the reference's float coefficients (pot / winners
+    // - bet, or -bet): a coefficient that is exactly 0 drops its class exactly
+    const double cw = static_cast<double>(I.pot - I.bet), c1 = static_cast<double>(I.pot / 2.0f - I.bet);
+    const double c2 = static_cast<double>(I.pot / 3.0f - I.bet), cl = -static_cast<double>(I.bet);
+    const int *tp = sd_pos + static_cast<size_t>(trav) * HS;
+    T *out = val + static_cast<size_t>(I.node) * HS;
+    for (int h = tid; h < HS; h += kTermThreads) {
+        double v = 0.0;
+        const int q = h < Ht ? __ldg(tp + h) : -1;
+        if (q >= 0) {
+            const int a = cb[q].d1, b = cb[q].d2;
+            const double Z = sd2_mass(st, M1, M2, a, b);
+            const double A = cls[4 * h], dle = cls[4 * h + 1], B = cls[4 * h + 2], C = cls[4 * h + 3];
+            const double W2 = A, T1 = (B - A) + dle, T2 = (C - B) - dle, L = Z - C;
+            v = cw * W2 + c1 * T1 + c2 * T2 + cl * L;
+            if (fabs(Z) <= zmin && pair_count(Bm, cnt, a, b, S2.IF1, S2.IF2, S2.IQD) <= 0) v = 0.0;
+        }
+        out[h] = static_cast<T>(v);
     }
 }
 
@@ -1348,6 +1656,13 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             if (e != cudaSuccess) return e;
             k_term_sd1<T><<<n, kTermThreads, sd1_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
+        case TK_SD2: {
+            const size_t sm = sd2_smem<T>(c.HS, c.ncomb);
+            e = cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+            if (e != cudaSuccess) return e;
+            k_term_sd2<T><<<n, kTermThreads, sm, s>>>(c, ctxs, items, trav);
+            break;
+        }
         case TK_ENUM: {
             const int nc = (c.HS + 127) / 128;
             k_term_enum<T><<<n * nc, 128, 0, s>>>(c, ctxs, items, nc, trav);

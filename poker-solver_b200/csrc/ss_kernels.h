@@ -24,6 +24,9 @@ struct DevCtx {
     const SdCombo *sd_combo;     // [ncomb]
     const short *sd_card_list;   // [52][52]
     const short *sd_card_partner;// [52][52]
+    const int *pos_hand;         // [np][ncomb] hand index at each rank position, -1 if none
+    const int *sd_seg;           // three-way showdown sweep segments, 4 ints each
+    int sd_seg_off[SS_MAX_PLAYERS + 1];
     const float *leaf_values;
     const int *iter;       // current CFR iteration (device counter, one per subgame)
     int HS;

@@ -271,6 +271,18 @@ int build_plan(const Problem &pb, Plan *out) {
             P.hand_code[p * HS + h] = a | (b << 8) | (blocked << 16) | (dense[a] << 20) | (dense[b] << 26);
         }
 
+    // ranges holding the same combo twice need atomic accumulation in the
+    // terminal kernels' combo tables
+    for (int p = 0; p < np; ++p) {
+        std::vector<char> seen(52 * 52, 0);
+        P.dup[p] = 0;
+        for (int h = 0; h < P.H[p]; ++h) {
+            int a = pb.hands[p][2 * h], b = pb.hands[p][2 * h + 1];
+            if (a > b) std::swap(a, b);
+            if (seen[a * 52 + b]++) P.dup[p] = 1;
+        }
+    }
+
     // terminal work lists per traverser
     bool need_sd = false;
     P.enum_work = 0;
@@ -313,7 +325,10 @@ int build_plan(const Problem &pb, Plan *out) {
                     it.pot = static_cast<float>(n.pot);
                     it.bet = static_cast<float>(n.bets[t]);
                     it.kind_detail = 2;
-                    kind = k == 1 ? TK_SD1 : TK_ENUM;
+                    kind = k == 1 ? TK_SD1
+                           : (k == 2 && !P.dup[t] && !P.dup[it.opp_player[0]] && !P.dup[it.opp_player[1]])
+                               ? TK_SD2
+                               : TK_ENUM;
                     need_sd = true;
                 }
             }
@@ -353,6 +368,9 @@ int build_plan(const Problem &pb, Plan *out) {
     P.sd_card_list.assign(52 * 52, -1);
     P.sd_card_partner.assign(52 * 52, -1);
     P.sd_pos.assign(static_cast<size_t>(np) * HS, -1);
+    P.pos_hand.clear();
+    P.sd_seg.clear();
+    for (int p = 0; p <= SS_MAX_PLAYERS; ++p) P.sd_seg_off[p] = 0;
     P.strength.assign(static_cast<size_t>(np) * HS, 0u);
     if (need_sd) {
         if (nb != 5) {
@@ -410,18 +428,31 @@ int build_plan(const Problem &pb, Plan *out) {
                 P.sd_pos[p * HS + h] = q;
                 P.strength[p * HS + h] = combos[q].s;
             }
-    }
-
-    // ranges holding the same combo twice need atomic accumulation in the
-    // terminal kernels' combo tables
-    for (int p = 0; p < np; ++p) {
-        std::vector<char> seen(52 * 52, 0);
-        P.dup[p] = 0;
-        for (int h = 0; h < P.H[p]; ++h) {
-            int a = pb.hands[p][2 * h], b = pb.hands[p][2 * h + 1];
-            if (a > b) std::swap(a, b);
-            if (seen[a * 52 + b]++) P.dup[p] = 1;
+        for (int q = 0; q < nc; ++q) {
+            P.sd_combo[q].d1 = static_cast<unsigned char>(dense[combos[q].a]);
+            P.sd_combo[q].d2 = static_cast<unsigned char>(dense[combos[q].b]);
         }
+        P.pos_hand.assign(static_cast<size_t>(np) * nc, -1);
+        for (int p = 0; p < np; ++p)
+            for (int h = 0; h < P.H[p]; ++h)
+                if (P.sd_pos[p * HS + h] >= 0) P.pos_hand[static_cast<size_t>(p) * nc + P.sd_pos[p * HS + h]] = h;
+        P.sd_seg.clear();
+        for (int p = 0; p < np; ++p) {
+            P.sd_seg_off[p] = static_cast<int>(P.sd_seg.size() / 4);
+            for (int q = 0; q < nc;) {
+                const int hi = P.sd_combo[q].hi;
+                bool has = false;
+                for (int r = q; r < hi; ++r) has = has || P.pos_hand[static_cast<size_t>(p) * nc + r] >= 0;
+                const size_t ns = P.sd_seg.size();
+                const bool own = ns / 4 > static_cast<size_t>(P.sd_seg_off[p]);   // a segment of player p exists
+                if (!has && own && P.sd_seg[ns - 2] == 0)
+                    P.sd_seg[ns - 3] = hi;  // extend the previous run of groups without the player's hands
+                else
+                    P.sd_seg.insert(P.sd_seg.end(), {q, hi, has ? 1 : 0, 0});
+                q = hi;
+            }
+        }
+        P.sd_seg_off[np] = static_cast<int>(P.sd_seg.size() / 4);
     }
 
     // per player: the range index of each dense-card pair (both orders), HS

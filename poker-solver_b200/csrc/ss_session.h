@@ -27,7 +27,8 @@ inline int term_class(int kind) {
         case TK_LEAF0: return PC_FILL;
         case TK_CR1: return PC_CR1;
         case TK_CR2: return PC_CR2;
-        case TK_SD1: return PC_SD1;
+        case TK_SD1:
+        case TK_SD2: return PC_SD1;
         default: return PC_ENUM;
     }
 }
