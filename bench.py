@@ -395,7 +395,7 @@ def run_batched(n, seed, device):
             "exploitability_max_pct": max(expl),
             "plain_iterations_p50": pct([p["iterations_run"] for p in plain], 50),
             "tree_nodes": {"min": min(nodes), "p50": pct(nodes, 50), "max": max(nodes)},
-            "mix": "80% river (2p) / 15% turn (2-3p) / 5% flop (2p), full ranges, 0-70% zero weights"}
+            "mix": "80% river (70% 2p, 30% 3p) / 15% turn (2-3p) / 5% flop (2p), full ranges, 0-70% zero weights"}
 
 
 def run_served(rate, duration, seed, device):

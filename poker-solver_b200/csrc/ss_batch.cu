@@ -169,7 +169,10 @@ class Batch {
         for (int i = 0; i < K; ++i)
             if (subs[i]) {
                 ctx[i] = subs[i]->c;
+                // launch-time sizes (grids, dynamic shared memory) come from
+                // cmax: the largest row stride and rank table of the batch
                 cmax.HS = std::max(cmax.HS, subs[i]->c.HS);
+                cmax.ncomb = std::max(cmax.ncomb, subs[i]->c.ncomb);
             }
         // merged lists, in launch order
         std::vector<char> blob;

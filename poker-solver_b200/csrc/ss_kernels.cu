@@ -738,6 +738,8 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int HS = V.HS;
     const int Dp = (V.deck + 3) & ~3;
+    // shared memory was provisioned for c0's row stride (the largest of a batch)
+    if (HS > c0.HS || V.deck > 52) return;
     Carve cv{smem};
     T *M1 = cv.take<T>(52 * MS);
     T *M2 = cv.take<T>(52 * MS);
@@ -1201,6 +1203,9 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
         s0 = c.sd_seg_off[trav];
         s1 = c.sd_seg_off[trav + 1];
     }
+    // the launch provisioned shared memory for c0's row stride and rank table
+    // (the largest of a batch); a block needing more must not run
+    if (HS > c0.HS || nc > c0.ncomb) return;
     const int tid = threadIdx.x, lane = tid & 31;
     Carve cv{smem};
     Sd2State st;

@@ -287,16 +287,19 @@ class Server:
 BET_SETS = [[0.5, 1.0], [0.33, 0.75], [1.0], [0.5], [0.33, 0.75, 1.5], [0.75]]
 
 
-def mix_config(rng, river=0.8, turn=0.15):
-    """One seeded request of the serving mix: 80% river (2 players),
-    15% turn (2-3 players, continuation leaves), 5% flop (2 players,
-    continuation leaves); all non-board combos with U(0,1) weights, a
-    U(0, 0.7) fraction zeroed; random bet set and raise cap (so tree sizes
-    spread from tens to thousands of nodes)."""
+def mix_config(rng, river=0.8, turn=0.15, river3=0.3):
+    """One seeded request of the serving mix: 80% river (2 players, or 3 with
+    probability river3), 15% turn (2-3 players, continuation leaves), 5% flop
+    (2 players, continuation leaves); all non-board combos with U(0,1)
+    weights, a U(0, 0.7) fraction zeroed; random bet set and raise cap (so
+    tree sizes spread from tens to thousands of nodes)."""
     u = rng.random()
     street = "river" if u < river else ("turn" if u < river + turn else "flop")
     nb = {"river": 5, "turn": 4, "flop": 3}[street]
-    np_ = 2 if street != "turn" else int(rng.integers(2, 4))
+    if street == "river":
+        np_ = 3 if rng.random() < river3 else 2
+    else:
+        np_ = 2 if street == "flop" else int(rng.integers(2, 4))
     board = [int(c) for c in rng.permutation(52)[:nb]]
     sizes = BET_SETS[int(rng.integers(len(BET_SETS)))]
     if np_ == 3:

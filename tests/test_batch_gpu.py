@@ -22,6 +22,11 @@ def mixed_subgames():
         sg = wl.AbiSubgame(cfg, max_hands=200)
         sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
         subs.append(sg)
+    # a 3-player river (three-way showdowns)
+    cfg = wl.config("river6", seed=47, num_players=3, bet_sizes=[1.0], max_raises=1)
+    cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(47), cfg["board"], 3, 50)
+    sg = wl.AbiSubgame(cfg, max_hands=200)
+    subs.append(sg)
     # a heads-up turn with continuation leaves
     cfg = wl.config("hu_river", seed=46, num_hands=40)
     cfg["board"] = cfg["board"][:4]
