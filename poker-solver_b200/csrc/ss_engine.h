@@ -98,7 +98,8 @@ enum TermKind : int {
     TK_SD1 = 4,      // showdown against one live opponent
     TK_ENUM = 5,     // anything else: exact tuple enumeration (small ranges only)
     TK_SD2 = 6,      // three-way showdown (two live opponents), ranges without repeated combos
-    TK_COUNT = 7
+    TK_CR1D = 7,     // TK_CR1 against a range that holds some combo more than once
+    TK_COUNT = 8
 };
 
 // One terminal for one traverser.  factor: payoff for folds; leaf_off >= 0

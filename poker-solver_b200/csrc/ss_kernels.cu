@@ -376,9 +376,11 @@ constexpr size_t cr1_smem() {
 // One counted opponent: mass(h) = F - u(c1) - u(c2) + f(h), F the opponent's
 // total reach, u(c) its reach on hands holding card c, f(h) its reach on the
 // traverser's own combo.  Folds: payoff * mass (street_solve.cu:745-761);
-// leaves: leaf value * mass (:1047-1066).
+// leaves: leaf value * mass (:1047-1066).  This form scatters the opponent's
+// reach into a cleared 52x52 matrix (atomically), so it serves ranges that
+// hold some combo more than once; k_term_cr1 below covers the others.
 template <class T>
-__global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevCtx *__restrict__ ctxs,
+__global__ void __launch_bounds__(kTermThreads) k_term_cr1_dup(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                            const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
     Carve cv{smem};
@@ -898,6 +900,123 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
             const double A2 = S.F2 - ga.u2 - gb.u2 + m2;
             v = A1 * A2 + S.QD + ga.g + gb.g - m2 * (ga.u1 + gb.u1) - m1 * (ga.u2 + gb.u2) + 3.0 * m1 * m2 - pp;
             if (fabs(v) <= zmin && pair_count(Bm, cnt, a, b, S.IF1, S.IF2, S.IQD) <= 0) v = 0.0;
+        }
+        const float f0 = h >= Ht ? 0.f : leaf_first ? leaf0[h] : gp0;
+        out0[h] = static_cast<T>(static_cast<double>(f0) * v);
+        for (int g = 1; g < ng; ++g) {
+            const float f = h >= Ht ? 0.f : gleaf[g] >= 0 ? __ldg(V.leaf + gleaf[g] + h) : gpay[g];
+            V.val[static_cast<size_t>(gnode[g]) * HS + h] = static_cast<T>(static_cast<double>(f) * v);
+        }
+    }
+}
+
+template <class T>
+constexpr size_t cr1_gather_smem(int HS) {
+    return (static_cast<size_t>(HS) + 4) * sizeof(T) + static_cast<size_t>(HS) * 4 + 64 * 8 + 64 * 4 +
+           3 * kTermGroupMax * 4 + 2 * 16 + 8 * 16;
+}
+
+// One counted opponent over the dense deck, for ranges without a repeated
+// combo: u(c) and f(h) are read from the staged reach row through the
+// opponent's pair table (row c of the table lists the opponent's hands
+// holding card c), so no matrix is built.  Exact zeros: the number of
+// compatible positive-reach opponent hands N - n(a) - n(b) + [f(h) > 0]
+// decides a value of exactly 0.  One block per group of terminals sharing the
+// opponent's reach row (the traverser's own continuation choices).
+template <class T>
+__global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                           const TermItem *__restrict__ items, int trav) {
+    extern __shared__ __align__(16) char smem[];
+    const TermItem *I0 = items + blockIdx.x;
+    if (I0->follow) return;   // written by the block of its group's first item
+    const int ng = I0->gextra + 1;
+    const int o = I0->opp_player[0];
+    const Cr2View<T> V = ctxs ? cr2_view<T>(ctxs[I0->sg], trav, o, o) : cr2_view<T>(c0, trav, o, o);
+    const int HS = V.HS;
+    if (HS > c0.HS || V.deck > 52) return;   // shared memory was provisioned for c0's row stride
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int Dp = (V.deck + 3) & ~3;
+    Carve cv{smem};
+    T *r = cv.take<T>(HS + 4);                 // staged reach row, r[HS] = 0 for missing pairs
+    float *leaf0 = cv.take<float>(HS);
+    double *u = cv.take<double>(64);
+    int *nz = cv.take<int>(64);
+    int *gnode = cv.take<int>(kTermGroupMax);
+    int *gleaf = cv.take<int>(kTermGroupMax);
+    float *gpay = cv.take<float>(kTermGroupMax);
+    {
+        const T *src = V.reach + static_cast<size_t>(I0->opp_row[0]) * HS;
+        constexpr int per = 16 / sizeof(T);
+        for (int q = tid * per; q < HS; q += kTermThreads * per) cp_async16(r + q, src + q);
+        const int lo = I0->leaf_off;
+        if (lo >= 0) {
+            const float *ls = V.leaf + lo;
+            for (int h = tid; h < V.Ht; h += kTermThreads) cp_async4(leaf0 + h, ls + h);
+        }
+        if (tid < ng) {
+            const TermItem &I = I0[tid];
+            gnode[tid] = I.node;
+            gleaf[tid] = I.leaf_off;
+            gpay[tid] = I.payoff;
+        }
+        if (tid == 0) r[HS] = T(0);
+        if (tid < 64) {
+            u[tid] = 0.0;
+            nz[tid] = 0;
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // per card c: u(c) and the count of positive-reach hands holding c, four
+    // lanes per card (a quarter of the table row each, shuffles in a fixed order)
+    {
+        const int col = tid >> 2, part = tid & 3, q = Dp >> 2;
+        double s = 0.0;
+        int n = 0;
+        if (col < Dp) {
+            const int *row = V.tab0 + col * 52 + part * q;
+            for (int b = 0; b < q; ++b) {
+                const T x = r[__ldg(row + b)];
+                s += static_cast<double>(x);
+                n += x > T(0) ? 1 : 0;
+            }
+        }
+#pragma unroll
+        for (int k = 1; k < 4; k <<= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, k);
+            n += __shfl_xor_sync(0xffffffffu, n, k);
+        }
+        if (part == 0 && col < Dp) {
+            u[col] = s;
+            nz[col] = n;
+        }
+    }
+    __syncthreads();
+    double F;
+    int N;
+    {
+        double s = (lane < Dp ? u[lane] : 0.0) + (lane + 32 < Dp ? u[lane + 32] : 0.0);
+        int n = (lane < Dp ? nz[lane] : 0) + (lane + 32 < Dp ? nz[lane + 32] : 0);
+        s = warp_sum(s);
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) n += __shfl_xor_sync(0xffffffffu, n, k);
+        F = 0.5 * s;
+        N = n / 2;
+    }
+    const int Ht = V.Ht;
+    const int *__restrict__ tc = V.code_t;
+    const bool leaf_first = gleaf[0] >= 0;
+    const float gp0 = gpay[0];
+    T *out0 = V.val + static_cast<size_t>(gnode[0]) * HS;
+    for (int h = tid; h < HS; h += kTermThreads) {
+        double v = 0.0;
+        if (h < Ht) {
+            const int hc = __ldg(tc + h);
+            const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
+            const bool on = (a < kCr2Off) && (b < kCr2Off);
+            const T f = on ? r[__ldg(V.tab0 + a * 52 + b)] : T(0);
+            const int live = N - nz[a] - nz[b] + (f > T(0) ? 1 : 0);
+            if (live > 0) v = F - u[a] - u[b] + static_cast<double>(f);
         }
         const float f0 = h >= Ht ? 0.f : leaf_first ? leaf0[h] : gp0;
         out0[h] = static_cast<T>(static_cast<double>(f0) * v);
@@ -1639,8 +1758,17 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             k_term_fill<T><<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, trav, kind == TK_ZERO);
             break;
         }
-        case TK_CR1:
-            k_term_cr1<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, ctxs, items, trav);
+        case TK_CR1: {
+            const size_t sm = cr1_gather_smem<T>(c.HS);
+            if (sm > 48 * 1024)
+                e = cudaFuncSetAttribute(k_term_cr1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(cr1_gather_smem<T>(kMaxHS)));
+            if (e != cudaSuccess) return e;
+            k_term_cr1<T><<<n, kTermThreads, sm, s>>>(c, ctxs, items, trav);
+            break;
+        }
+        case TK_CR1D:
+            k_term_cr1_dup<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
         case TK_CR2: {
             // c.HS: the row stride (the largest of a batch); the staging of two

@@ -309,14 +309,14 @@ int build_plan(const Problem &pb, Plan *out) {
                 it.payoff = (n.player == t) ? static_cast<float>(n.pot - n.bets[t])
                                             : -static_cast<float>(n.bets[t]);
                 it.kind_detail = 0;
-                kind = k == 0 ? TK_LEAF0 : k == 1 ? TK_CR1 : k == 2 ? TK_CR2 : TK_ENUM;
+                kind = k == 0 ? TK_LEAF0 : k == 1 ? (P.dup[it.opp_player[0]] ? TK_CR1D : TK_CR1) : k == 2 ? TK_CR2 : TK_ENUM;
             } else if (n.type == SS_NODE_LEAF) {
                 if (pb.leaf_values && n.leaf_idx >= 0) {
                     for (int o = 0; o < np; ++o)
                         if (o != t && n.active_players[o]) add_opp(o);
                     it.leaf_off = (n.leaf_idx * np + t) * P.max_h;
                     it.kind_detail = 1;
-                    kind = k == 0 ? TK_LEAF0 : k == 1 ? TK_CR1 : k == 2 ? TK_CR2 : TK_ENUM;
+                    kind = k == 0 ? TK_LEAF0 : k == 1 ? (P.dup[it.opp_player[0]] ? TK_CR1D : TK_CR1) : k == 2 ? TK_CR2 : TK_ENUM;
                 }
             } else {  // showdown
                 if (pb.is_river && n.active_players[t]) {
@@ -342,25 +342,26 @@ int build_plan(const Problem &pb, Plan *out) {
         }
     }
 
-    // two-opponent terminals sharing both opponents' reach rows share their
-    // card-removal mass: order them by the row pair and mark the groups
-    for (int t = 0; t < np; ++t) {
-        std::vector<TermItem> &v = P.term[t][TK_CR2];
-        std::stable_sort(v.begin(), v.end(), [](const TermItem &u, const TermItem &w) {
-            if (u.opp_row[0] != w.opp_row[0]) return u.opp_row[0] < w.opp_row[0];
-            return u.opp_row[1] < w.opp_row[1];
-        });
-        for (size_t i = 0; i < v.size();) {
-            size_t j = i + 1;
-            while (j < v.size() && j - i < static_cast<size_t>(kTermGroupMax) &&
-                   v[j].opp_row[0] == v[i].opp_row[0] && v[j].opp_row[1] == v[i].opp_row[1] &&
-                   v[j].opp_player[0] == v[i].opp_player[0] && v[j].opp_player[1] == v[i].opp_player[1])
-                ++j;
-            v[i].gextra = static_cast<int>(j - i - 1);
-            for (size_t m = i + 1; m < j; ++m) v[m].follow = 1;
-            i = j;
+    // one- and two-opponent terminals sharing their opponents' reach rows
+    // share their card-removal mass: order them by the rows and mark groups
+    for (int t = 0; t < np; ++t)
+        for (int kind : {TK_CR1, TK_CR2}) {
+            std::vector<TermItem> &v = P.term[t][kind];
+            std::stable_sort(v.begin(), v.end(), [](const TermItem &u, const TermItem &w) {
+                if (u.opp_row[0] != w.opp_row[0]) return u.opp_row[0] < w.opp_row[0];
+                return u.opp_row[1] < w.opp_row[1];
+            });
+            for (size_t i = 0; i < v.size();) {
+                size_t j = i + 1;
+                while (j < v.size() && j - i < static_cast<size_t>(kTermGroupMax) &&
+                       v[j].opp_row[0] == v[i].opp_row[0] && v[j].opp_row[1] == v[i].opp_row[1] &&
+                       v[j].opp_player[0] == v[i].opp_player[0] && v[j].opp_player[1] == v[i].opp_player[1])
+                    ++j;
+                v[i].gextra = static_cast<int>(j - i - 1);
+                for (size_t m = i + 1; m < j; ++m) v[m].follow = 1;
+                i = j;
+            }
         }
-    }
 
     // showdown tables: every non-board combo ranked on the 5-card board
     P.ncomb = 0;

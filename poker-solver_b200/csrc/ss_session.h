@@ -25,7 +25,8 @@ inline int term_class(int kind) {
     switch (kind) {
         case TK_ZERO:
         case TK_LEAF0: return PC_FILL;
-        case TK_CR1: return PC_CR1;
+        case TK_CR1:
+        case TK_CR1D: return PC_CR1;
         case TK_CR2: return PC_CR2;
         case TK_SD1:
         case TK_SD2: return PC_SD1;

@@ -194,3 +194,21 @@ def test_against_reference_gpu_build():
     theirs = ref.solve(td, H, W, nh, 4)
     ref.free(td)
     strict(ours, theirs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,seed,nh,over", [
+    ("hu_river", 51, 30, {}),
+    ("turn3", 52, 10, SMALL_TURN),
+])
+def test_ranges_repeating_a_combo(oracle, name, seed, nh, over):
+    """A range may list the same combo twice (the C ABI allows it; the
+    reference's kernels just loop over both hands): the scatter forms of the
+    card-removal kernels accumulate both."""
+    cfg = wl.config(name, seed=seed, num_hands=nh, **over)
+    for p in range(cfg["num_players"]):
+        cfg["hands"][p] = np.concatenate([cfg["hands"][p], cfg["hands"][p][:3]])
+        cfg["weights"][p] = np.concatenate([cfg["weights"][p], cfg["weights"][p][:3] * 0.5]).astype(np.float32)
+    ours, lv = solve(cfg, 3)
+    r32, _ = oracle_pair(oracle, cfg, 3, lv)
+    strict(ours, r32)
