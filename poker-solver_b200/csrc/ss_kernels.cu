@@ -158,13 +158,54 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
     const size_t HS = static_cast<size_t>(V.HS);
     const float *val = V.val + h0;
     const int *__restrict__ fr = V.fr_items;
+    // the regret and strategy-sum rows are needed after the frontier sums:
+    // start bringing them into L1 now (no registers held)
+    if (act && (S == 1 || warp == 0)) {
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+            if (a < I.na) {
+                const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(V.R + off));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(V.S + off));
+            }
+        }
+    }
     float2 ev[SS_MAX_ACTIONS];
 #pragma unroll
-    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-        if (a < I.na) {
-            float2 e = make_float2(0.f, 0.f);
-            if (act) {
-                int k = V.fr_off[I.first_edge + a] + (S == 1 ? 0 : warp);
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) ev[a] = make_float2(0.f, 0.f);
+    if constexpr (S == 1) {
+        // the frontiers of all edges are one contiguous run of rows: walk it
+        // eight rows at a time across edge boundaries (short frontiers, one
+        // row per edge at the lowest level, would otherwise leave one load in
+        // flight); each row adds to its edge in row order
+        const int fe = I.first_edge;
+        int bnd[SS_MAX_ACTIONS];
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
+        const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
+        for (int k = k0; k < kend; k += 8) {
+            float2 x[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                x[i] = k + i < kend ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS) : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (k + i < kend) {
+                    int e = 0;
+#pragma unroll
+                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
+#pragma unroll
+                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+                        if (e == a) add2(ev[a], x[i]);
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+            if (a < I.na && act) {
+                float2 e = make_float2(0.f, 0.f);
+                int k = V.fr_off[I.first_edge + a] + warp;
                 const int k1 = V.fr_off[I.first_edge + a + 1];
                 for (; k + 7 * S < k1; k += 8 * S) {
                     float2 x[8];
@@ -174,8 +215,8 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
                     for (int i = 0; i < 8; ++i) add2(e, x[i]);
                 }
                 for (; k < k1; k += S) add2(e, ld2(val + static_cast<size_t>(__ldg(fr + k)) * HS));
+                ev[a] = e;
             }
-            ev[a] = e;
         }
     }
     if constexpr (S > 1) {
