@@ -89,6 +89,12 @@ struct alignas(16) CfvItem {
 // total is long: several warps share each of its hand chunks.
 constexpr int kCfvLongFrontier = 48;
 
+// A three-way showdown's rank-order sweep is cut into at most this many runs
+// of tie groups, each swept by its own block from a directly computed state.
+constexpr int kSd2Chunks = 16;
+// target number of segments per run
+constexpr int kSd2SegsPerChunk = 24;
+
 // Terminal kinds per traverser.
 enum TermKind : int {
     TK_ZERO = 0,     // value 0 (folded traverser at showdown, leaves without leaf values)
@@ -181,6 +187,10 @@ struct Plan {
     // none.  Player p's segments are sd_seg[sd_seg_off[p] .. sd_seg_off[p+1]).
     std::vector<int> sd_seg;           // 4 ints per segment
     int sd_seg_off[SS_MAX_PLAYERS + 1] = {};
+    // per player, the segments cut into kSd2Chunks runs swept by separate
+    // blocks: run k = segments [sd_chunk[p*(kSd2Chunks+1)+k], ...[k+1]) (empty
+    // runs at the end when the player has few segments)
+    std::vector<int> sd_chunk;
     std::vector<uint32_t> strength;    // [np][HS], 0 if blocked / padding
     int dup[SS_MAX_PLAYERS] = {};      // range holds some combo more than once
     double enum_work = 0;              // tuple visits per iteration on TK_ENUM

@@ -1241,7 +1241,7 @@ template <class T>
 constexpr size_t sd2_smem(int HS, int ncomb) {
     return SD2_S * SD2_S * 8 + 2 * SD2_S * SD2_S * sizeof(T) + 4 * 64 * 8 + 8 * 8 + static_cast<size_t>(HS) * 32 +
            2 * static_cast<size_t>(ncomb) * sizeof(T) + 53 * sizeof(ulonglong2) + 53 * sizeof(Cr2Cnt) +
-           sizeof(Cr2Scalars) + 16 * 16;
+           sizeof(Cr2Scalars) + 16 + 16 * 16;
 }
 
 struct Sd2State {
@@ -1338,11 +1338,101 @@ __device__ __forceinline__ void sd2_add(const Sd2State &st, const SdCombo *__res
     }
 }
 
+// The sweep state for the opponents' hands at rank positions [0, qend),
+// computed directly (not by adding them one tie group at a time): the two
+// matrices, P = M1 M2 as FP64 4x4 tiles over the 48-card box, the card sums,
+// d, w and the scalars, each summed in a fixed order.  The caller syncs
+// before and after.
+template <class T>
+__device__ void sd2_direct_state(const Sd2State &st, T *M1, T *M2, const T *R1, const T *R2,
+                                 const SdCombo *__restrict__ cb, int qend) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < SD2_S * SD2_S; i += kTermThreads) {
+        M1[i] = T(0);
+        M2[i] = T(0);
+        st.P[i] = 0.0;
+    }
+    __syncthreads();
+    for (int q = tid; q < qend; q += kTermThreads) {
+        const int x = cb[q].d1, y = cb[q].d2;
+        const T r1 = R1[q], r2 = R2[q];
+        if (r1 != T(0)) {
+            M1[x * SD2_S + y] = r1;
+            M1[y * SD2_S + x] = r1;
+        }
+        if (r2 != T(0)) {
+            M2[x * SD2_S + y] = r2;
+            M2[y * SD2_S + x] = r2;
+        }
+    }
+    __syncthreads();
+    if (tid < 144) {
+        const int i0 = (tid / 12) * 4, j0 = (tid % 12) * 4;
+        double acc[4][4] = {};
+        for (int k = 0; k < 48; ++k) {
+            double xs[4], ys[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                xs[i] = static_cast<double>(M1[(i0 + i) * SD2_S + k]);
+                ys[i] = static_cast<double>(M2[k * SD2_S + j0 + i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] += xs[i] * ys[j];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) st.P[(i0 + i) * SD2_S + j0 + j] = acc[i][j];
+    } else if (tid >= 160 && tid < 160 + SD2_S) {
+        const int c = tid - 160;
+        double u1 = 0.0, u2 = 0.0, d = 0.0;
+        for (int r = 0; r < SD2_S; ++r) {
+            const double x1 = static_cast<double>(M1[r * SD2_S + c]), x2 = static_cast<double>(M2[r * SD2_S + c]);
+            u1 += x1;
+            u2 += x2;
+            d += x1 * x2;
+        }
+        st.u1[c] = u1;
+        st.u2[c] = u2;
+        st.d[c] = d;
+    }
+    __syncthreads();
+    if (tid < SD2_S) {
+        const int c = tid;
+        double w = 0.0;
+        for (int b = 0; b < SD2_S; ++b)
+            w += static_cast<double>(M2[c * SD2_S + b]) * st.u1[b] + static_cast<double>(M1[c * SD2_S + b]) * st.u2[b];
+        st.w[c] = w;
+    } else if (warp == kTermThreads / 32 - 1) {
+        double f1 = 0.0, f2 = 0.0, q = 0.0, e = 0.0;
+        for (int c = lane; c < SD2_S; c += 32) {
+            f1 += st.u1[c];
+            f2 += st.u2[c];
+            q += st.u1[c] * st.u2[c];
+            e += st.d[c];
+        }
+        f1 = warp_sum(f1);
+        f2 = warp_sum(f2);
+        q = warp_sum(q);
+        e = warp_sum(e);
+        if (lane == 0) {
+            st.sc[0] = 0.5 * f1;
+            st.sc[1] = 0.5 * f2;
+            st.sc[2] = q;
+            st.sc[3] = 0.5 * e;
+        }
+    }
+    __syncthreads();
+}
+
 template <class T>
 __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                            const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
-    const TermItem I = items[blockIdx.x];
+    const TermItem I = items[blockIdx.x / kSd2Chunks];
+    const int chunk = blockIdx.x % kSd2Chunks;
     const int o1 = I.opp_player[0], o2 = I.opp_player[1];
     const T *reach;
     T *val;
@@ -1360,12 +1450,14 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
         HS = c.HS;
         nc = c.ncomb;
         Ht = c.H[trav];
-        s0 = c.sd_seg_off[trav];
-        s1 = c.sd_seg_off[trav + 1];
+        const int *ch = c.sd_chunk + static_cast<size_t>(trav) * (kSd2Chunks + 1);
+        s0 = ch[chunk];
+        s1 = ch[chunk + 1];
     }
     // the launch provisioned shared memory for c0's row stride and rank table
     // (the largest of a batch); a block needing more must not run
     if (HS > c0.HS || nc > c0.ncomb) return;
+    if (s0 >= s1) return;   // an unused run (the player has few tie groups)
     const int tid = threadIdx.x, lane = tid & 31;
     Carve cv{smem};
     Sd2State st;
@@ -1383,31 +1475,36 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
     ulonglong2 *Bm = cv.take<ulonglong2>(53);
     Cr2Cnt *cnt = cv.take<Cr2Cnt>(53);
     Cr2Scalars *sc2 = cv.take<Cr2Scalars>(1);
+    int *last_pos = cv.take<int>(4);
 
-    // opponents' reach by rank position; everything else starts at zero
+    // opponents' reach by rank position, and the last position holding
+    // positive reach of either opponent
+    if (tid == 0) *last_pos = -1;
+    if (tid < 64) {
+        st.u1[tid] = 0.0;
+        st.u2[tid] = 0.0;
+        st.w[tid] = 0.0;
+        st.d[tid] = 0.0;
+    }
+    __syncthreads();
     {
         const T *ra = reach + static_cast<size_t>(I.opp_row[0]) * HS;
         const T *rb = reach + static_cast<size_t>(I.opp_row[1]) * HS;
         const int *pa = pos_hand + static_cast<size_t>(o1) * nc, *pb = pos_hand + static_cast<size_t>(o2) * nc;
+        int lp = -1;
         for (int q = tid; q < nc; q += kTermThreads) {
             const int ha = __ldg(pa + q), hb = __ldg(pb + q);
-            R1[q] = ha >= 0 ? ra[ha] : T(0);
-            R2[q] = hb >= 0 ? rb[hb] : T(0);
+            const T x = ha >= 0 ? ra[ha] : T(0), y = hb >= 0 ? rb[hb] : T(0);
+            R1[q] = x;
+            R2[q] = y;
+            if (x > T(0) || y > T(0)) lp = q;
         }
-        for (int i = tid; i < SD2_S * SD2_S; i += kTermThreads) {
-            st.P[i] = 0.0;
-            M1[i] = T(0);
-            M2[i] = T(0);
-        }
-        if (tid < 64) {
-            st.u1[tid] = 0.0;
-            st.u2[tid] = 0.0;
-            st.w[tid] = 0.0;
-            st.d[tid] = 0.0;
-        }
-        if (tid < 8) st.sc[tid] = 0.0;
+        atomicMax(last_pos, lp);
     }
     __syncthreads();
+    // this run starts from the state of every hand ranked below it
+    const int run_lo = __ldg(seg + 4 * s0), run_hi = __ldg(seg + 4 * (s1 - 1) + 1);
+    sd2_direct_state(st, M1, M2, R1, R2, cb, run_lo);
 
     const int *ph_t = pos_hand + static_cast<size_t>(trav) * nc;
     for (int si = s0; si < s1; ++si) {
@@ -1459,8 +1556,10 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
         }
     }
 
-    // all hands added: Z, and the exact positive-pair count for hands whose
-    // mass is within the error bound of zero (masks over the 47-card matrices)
+    // all hands added (directly, unless this run ends the rank order): Z, and
+    // the exact positive-pair count for hands whose mass is within the error
+    // bound of zero (masks over the 47-card matrices)
+    if (run_hi < nc) sd2_direct_state(st, M1, M2, R1, R2, cb, nc);
     if (tid < 2 * 64) {
         const int col = tid & 63;
         const T *M = tid < 64 ? M1 : M2;
@@ -1503,14 +1602,21 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
     const double c2 = static_cast<double>(I.pot / 3.0f - I.bet), cl = -static_cast<double>(I.bet);
     const int *tp = sd_pos + static_cast<size_t>(trav) * HS;
     T *out = val + static_cast<size_t>(I.node) * HS;
+    const int lastp = *last_pos;
     for (int h = tid; h < HS; h += kTermThreads) {
         double v = 0.0;
         const int q = h < Ht ? __ldg(tp + h) : -1;
+        // hands of this run's tie groups; the first run also writes the hands
+        // without a rank position (and the padding)
+        if (q >= 0 ? (q < run_lo || q >= run_hi) : chunk != 0) continue;
         if (q >= 0) {
             const int a = cb[q].d1, b = cb[q].d2;
             const double Z = sd2_mass(st, M1, M2, a, b);
             const double A = cls[4 * h], dle = cls[4 * h + 1], B = cls[4 * h + 2], C = cls[4 * h + 3];
-            const double W2 = A, T1 = (B - A) + dle, T2 = (C - B) - dle, L = Z - C;
+            // no positive-reach opponent hand ranked above the group: the loss
+            // class is empty, exactly (Z and C may come from different runs)
+            const double L = cb[q].hi > lastp ? 0.0 : Z - C;
+            const double W2 = A, T1 = (B - A) + dle, T2 = (C - B) - dle;
             v = cw * W2 + c1 * T1 + c2 * T2 + cl * L;
             if (fabs(Z) <= zmin && pair_count(Bm, cnt, a, b, S2.IF1, S2.IF2, S2.IQD) <= 0) v = 0.0;
         }
@@ -1782,7 +1888,8 @@ cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long,
     }
     if (n_long > 0) {
         const int nc = (H + 63) / 64;
-        k_cfv<kCfvThreads / 32><<<n_long * nc, kCfvThreads, 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
+        static_assert(32 * kCfvSplit == kCfvThreads, "the split form fills one block of kCfvThreads");
+        k_cfv<kCfvSplit><<<n_long * nc, kCfvThreads, 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
     }
     return cudaGetLastError();
 }
@@ -1834,7 +1941,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             const size_t sm = sd2_smem<T>(c.HS, c.ncomb);
             e = cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
             if (e != cudaSuccess) return e;
-            k_term_sd2<T><<<n, kTermThreads, sm, s>>>(c, ctxs, items, trav);
+            k_term_sd2<T><<<n * kSd2Chunks, kTermThreads, sm, s>>>(c, ctxs, items, trav);
             break;
         }
         case TK_ENUM: {

@@ -26,6 +26,7 @@ struct DevCtx {
     const short *sd_card_partner;// [52][52]
     const int *pos_hand;         // [np][ncomb] hand index at each rank position, -1 if none
     const int *sd_seg;           // three-way showdown sweep segments, 4 ints each
+    const int *sd_chunk;         // [np][kSd2Chunks + 1] runs of segments
     int sd_seg_off[SS_MAX_PLAYERS + 1];
     const float *leaf_values;
     const int *iter;       // current CFR iteration (device counter, one per subgame)
@@ -45,6 +46,8 @@ constexpr int kHandThreads = 64;
 constexpr int kHandsPerBlock = kHandThreads * 4;
 // threads per block of the value/regret kernel (2 hands each)
 constexpr int kCfvThreads = 128;
+// warps that share one hand chunk of a value/regret item with a long frontier
+constexpr int kCfvSplit = 4;
 // threads per block of the per-terminal kernels
 constexpr int kTermThreads = 256;
 
@@ -54,7 +57,7 @@ constexpr int kTermThreads = 256;
 // count of the launch).
 cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
                          const DevCtx *ctxs = nullptr, int player = -1);
-// The last n_long items (long frontiers) run with four warps per hand chunk.
+// The last n_long items (long frontiers) run with kCfvSplit warps per hand chunk.
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
                        const DevCtx *ctxs = nullptr, int trav = -1);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,

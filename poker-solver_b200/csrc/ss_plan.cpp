@@ -371,6 +371,7 @@ int build_plan(const Problem &pb, Plan *out) {
     P.sd_pos.assign(static_cast<size_t>(np) * HS, -1);
     P.pos_hand.clear();
     P.sd_seg.clear();
+    P.sd_chunk.clear();
     for (int p = 0; p <= SS_MAX_PLAYERS; ++p) P.sd_seg_off[p] = 0;
     P.strength.assign(static_cast<size_t>(np) * HS, 0u);
     if (need_sd) {
@@ -454,6 +455,14 @@ int build_plan(const Problem &pb, Plan *out) {
             }
         }
         P.sd_seg_off[np] = static_cast<int>(P.sd_seg.size() / 4);
+        P.sd_chunk.assign(static_cast<size_t>(np) * (kSd2Chunks + 1), 0);
+        for (int p = 0; p < np; ++p) {
+            const int a = P.sd_seg_off[p], b = P.sd_seg_off[p + 1], n = b - a;
+            const int K = std::max(1, std::min(kSd2Chunks, n / kSd2SegsPerChunk));
+            int *ch = P.sd_chunk.data() + static_cast<size_t>(p) * (kSd2Chunks + 1);
+            for (int i = 0; i <= kSd2Chunks; ++i)
+                ch[i] = i <= K ? a + static_cast<int>(static_cast<long long>(i) * n / K) : b;
+        }
     }
 
     // per player: the range index of each dense-card pair (both orders), HS
