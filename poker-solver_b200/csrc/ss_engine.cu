@@ -101,6 +101,11 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     CK(cudaSetDevice(device));
     keep_pool_warm(device);
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    for (int k = 0; k < TK_COUNT; ++k) {
+        CK(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    }
     const int np = P.np;
     const size_t HS = static_cast<size_t>(P.HS);
     const size_t E = static_cast<size_t>(P.E), N = static_cast<size_t>(P.N);
