@@ -42,6 +42,14 @@ sys.path[:0] = [ROOT, PKG]
 METRIC = "subgame solves/s and p50/p99 latency at <=0.5% pot exploitability vs plain GPU"
 UNIT = "solves/s"
 WORKLOAD = "turn3"
+# --workload: the benchmark's subgame (turn3 by default) or the 3-player river
+WORKLOADS = {
+    "turn3": ("3-player turn subgame, 1128 combos/player, continuation leaves, 1000 Linear-CFR iterations",
+              "state larger than L2 (regrets, sums, reach, values ~400 MB)"),
+    "river3": ("3-player river subgame, 1081 combos/player with U(0,1) weights, pot 300, stacks 1000, "
+               "bets {0.5, 1.0} + all-in, 2 raises, three-way showdowns, 1000 Linear-CFR iterations",
+               "state a few MB, inside L2"),
+}
 
 
 def parse():
@@ -52,6 +60,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--iterations", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS),
+                    help="subgame of the plain form (the CPU baseline and reference arm cover turn3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="plain,batched,served",
                     help="comma list of plain (the headline), batched, served")
@@ -182,9 +192,13 @@ class ClockSampler:
 # our solver
 # ---------------------------------------------------------------------------
 
-def build_subgame(seed, iterations):
+def build_subgame(seed, iterations, workload=WORKLOAD):
     import workloads as wl
-    cfg = wl.config(WORKLOAD, seed=seed, iterations=iterations)
+    if workload == "river3":
+        cfg = wl.config("river6", seed=seed, num_players=3, iterations=iterations)
+        cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(seed), cfg["board"], 3, None)
+    else:
+        cfg = wl.config(WORKLOAD, seed=seed, iterations=iterations)
     sg = wl.AbiSubgame(cfg, max_hands=1326)
     sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
     return cfg, sg
@@ -207,7 +221,7 @@ def run_ours(args, world, rank, local):
     for f in ("ss_session_run", "ss_session_reset", "ss_session_synchronize"):
         getattr(lib, f).argtypes = [ctypes.c_void_p] + ([ctypes.c_int] if f == "ss_session_run" else [])
 
-    cfg, sg = build_subgame(args.seed + rank, args.iterations)
+    cfg, sg = build_subgame(args.seed + rank, args.iterations, args.workload)
     opts = ssg.SSSolveOptions(local, 10, -1.0, 50, 0)
     sess = ctypes.c_void_p()
     rc = lib.ss_session_create(ctypes.byref(sg.td), ctypes.byref(opts), ctypes.byref(sess))
@@ -553,7 +567,7 @@ def main():
     if rank == 0 and world == 1 and "served" in forms:
         served = run_served(args.rate, args.duration, args.seed, local)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "turn3":
         r = reference_cpu(args.seed, budget_s=20.0)
         if r is not None:
             cpu = {"value": r["solves_per_s"], "unit": UNIT, "cores": r["cores"], "kind": "reference",
@@ -566,10 +580,9 @@ def main():
             "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "3-player turn subgame, 1128 combos/player, continuation leaves, "
-                                   "1000 Linear-CFR iterations",
+            "config": {"workload": WORKLOADS[args.workload][0],
                        "iterations": args.iterations, "tree": res["tree"],
-                       "l2": "state larger than L2 (regrets, sums, reach, values ~400 MB)",
+                       "l2": WORKLOADS[args.workload][1],
                        "parallelism": f"replicas x{world}",
                        "p50_ms": t[len(t) // 2], "p99_ms": t[-1]},
             "roofline": res["roofline"], "cpu_baseline": cpu, "clocks": res["clocks"],
