@@ -334,8 +334,9 @@ def run_ours(args, world, rank, local):
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
-        if dom in tr.get("classes", {}):
-            traffic = tr["classes"][dom].get("dram_bytes_per_launch")
+        tcls = tr.get("workloads", {}).get(args.workload, {}).get("classes", {})
+        if dom in tcls:
+            traffic = tcls[dom].get("dram_bytes_per_launch")
     except Exception:
         pass
 
@@ -495,7 +496,10 @@ def reference_cpu(seed, budget_s=25.0):
     full = wl.config(WORKLOAD, seed=seed)
     sizes, per_iter = [], []
     t_start = time.perf_counter()
-    for H in (6, 8, 10, 12):
+    # the two-opponent terminals enumerate opponent pairs per hand (cost ~H^3
+    # once per-node overhead stops dominating): the fit uses the two largest
+    # sizes that fit the time budget
+    for H in (8, 12, 16, 24):
         cfg = wl.config(WORKLOAD, seed=seed, num_hands=H)
         Hm, Wm, nh = wl.padded(cfg)
         results = [None] * cores
