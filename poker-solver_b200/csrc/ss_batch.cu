@@ -170,9 +170,11 @@ class Batch {
             if (subs[i]) {
                 ctx[i] = subs[i]->c;
                 // launch-time sizes (grids, dynamic shared memory) come from
-                // cmax: the largest row stride and rank table of the batch
+                // cmax: the largest row stride, rank table and sweep run of the batch
                 cmax.HS = std::max(cmax.HS, subs[i]->c.HS);
                 cmax.ncomb = std::max(cmax.ncomb, subs[i]->c.ncomb);
+                for (int lg = 0; lg < kSd2Merge; ++lg)
+                    cmax.sd_span[lg] = std::max(cmax.sd_span[lg], subs[i]->c.sd_span[lg]);
             }
         // merged lists, in launch order
         std::vector<char> blob;

@@ -228,6 +228,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.HS = P.HS;
     c.np = np;
     c.ncomb = P.ncomb;
+    for (int lg = 0; lg < kSd2Merge; ++lg) c.sd_span[lg] = P.sd_span[lg];
     c.deck = P.deck;
     for (int p = 0; p < SS_MAX_PLAYERS; ++p) {
         c.H[p] = p < np ? P.H[p] : 0;

@@ -92,8 +92,16 @@ constexpr int kCfvLongFrontier = 48;
 // A three-way showdown's rank-order sweep is cut into at most this many runs
 // of tie groups, each swept by its own block from a directly computed state.
 constexpr int kSd2Chunks = 16;
-// target number of segments per run
-constexpr int kSd2SegsPerChunk = 24;
+// sweep cost of a segment, in units of one hand added per opponent: a fixed
+// part (its block barriers) plus its hands; a run is cut once it holds about
+// kSd2RunCost units (at least a segment), since each run also pays for two
+// directly computed states
+constexpr int kSd2SegCost = 6;
+constexpr int kSd2RunCost = 96;
+// A launch may give each block 2^lg consecutive runs (lg < kSd2Merge): many
+// terminals in one launch (batches) need fewer, longer sweeps.
+constexpr int kSd2Merge = 5;
+static_assert(kSd2Chunks == 1 << (kSd2Merge - 1), "runs merge in powers of two");
 
 // Terminal kinds per traverser.
 enum TermKind : int {
@@ -191,6 +199,7 @@ struct Plan {
     // blocks: run k = segments [sd_chunk[p*(kSd2Chunks+1)+k], ...[k+1]) (empty
     // runs at the end when the player has few segments)
     std::vector<int> sd_chunk;
+    int sd_span[kSd2Merge] = {};       // most rank positions covered by 2^lg consecutive runs
     std::vector<uint32_t> strength;    // [np][HS], 0 if blocked / padding
     int dup[SS_MAX_PLAYERS] = {};      // range holds some combo more than once
     double enum_work = 0;              // tuple visits per iteration on TK_ENUM

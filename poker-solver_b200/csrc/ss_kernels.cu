@@ -1230,23 +1230,46 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
 // four-card removal for opponent 1).  With Z read after the sweep:
 //   W2 = A, T1 = (B - A) + D(L, E), T2 = (C - B) - D(L, E), lose = Z - C,
 //   value = (pot - bet) W2 + (pot/2 - bet) T1 + (pot/3 - bet) T2 - bet lose.
-// Adding a hand changes one row and column of P and every w entry, so each
-// phase gives threads fixed ownership (P columns or rows, w entries, the
-// scalars, matrix cells) and loops over the phase's hands: no atomics, a
-// fixed summation order.  One block per terminal.
+// Adding a hand changes two rows (or columns) of P, two card sums and every
+// w entry, so each phase gives threads fixed ownership (P cells by column
+// and row residue, one card's u / d / w, the scalars, matrix cells), each
+// accumulating its share of the phase's hands in registers: no atomics, a
+// fixed summation order.  The sweep of a terminal is cut into runs of tie
+// groups of about equal cost, one block each, starting from a directly
+// computed state (the product P as 3x3 FP64 tiles over all 256 threads).
+// C of a group and A of the next are read in one phase (the same state).
 // ---------------------------------------------------------------------------
-constexpr int SD2_S = 49;   // row stride of the sweep's 47-card matrices (odd: conflict-free columns)
+constexpr int SD2_S = 49;   // row stride of the sweep's card matrices (odd: conflict-free columns)
+constexpr int SD2_N = 48;   // cards a matrix covers (dense indices; a river deck has 47)
+constexpr int kSd2BlocksTarget = 2 * 148 * 4;   // sweep blocks per launch before runs merge
+static_assert(kTermThreads == 256, "the sweep's thread roles assume 256 threads");
 
+// the opponents' reach by rank position; after the sweep the same space holds
+// the positive-reach masks, counts and scalars of the exact-zero test
 template <class T>
-constexpr size_t sd2_smem(int HS, int ncomb) {
-    return SD2_S * SD2_S * 8 + 2 * SD2_S * SD2_S * sizeof(T) + 4 * 64 * 8 + 8 * 8 + static_cast<size_t>(HS) * 32 +
-           2 * static_cast<size_t>(ncomb) * sizeof(T) + 53 * sizeof(ulonglong2) + 53 * sizeof(Cr2Cnt) +
-           sizeof(Cr2Scalars) + 16 + 16 * 16;
+__host__ __device__ constexpr size_t sd2_reach_bytes(int ncomb) {
+    return 2 * static_cast<size_t>(ncomb) * sizeof(T) > 53 * sizeof(ulonglong2) + 53 * sizeof(Cr2Cnt) + sizeof(Cr2Scalars)
+               ? 2 * static_cast<size_t>(ncomb) * sizeof(T)
+               : 53 * sizeof(ulonglong2) + 53 * sizeof(Cr2Cnt) + sizeof(Cr2Scalars);
+}
+
+// dynamic shared memory for runs of at most `span` rank positions: P, M1, M2,
+// u1, u2, w, d, scalars, per-position classes of the run, reach (masks), the
+// cards of each position, the traverser's hand at each position of the run,
+// the last positive position; 16 bytes of alignment slack per carve
+template <class T>
+constexpr size_t sd2_smem(int span, int ncomb) {
+    return SD2_S * SD2_S * 8 + 2 * SD2_S * SD2_S * sizeof(T) + 4 * 64 * 8 + 8 * 8 + static_cast<size_t>(span) * 32 +
+           sd2_reach_bytes<T>(ncomb) + static_cast<size_t>(ncomb) * 2 + static_cast<size_t>(span) * 2 + 16 +
+           13 * 16;
 }
 
 struct Sd2State {
     double *P, *u1, *u2, *w, *d, *sc;   // sc: F1, F2, Q, D
 };
+
+__device__ __forceinline__ int sd2_c1(unsigned short e) { return e & 255; }
+__device__ __forceinline__ int sd2_c2(unsigned short e) { return e >> 8; }
 
 // D(., .) of the hand (a, b) on the current sweep state (the two-opponent
 // closed form, see k_term_cr2)
@@ -1255,7 +1278,7 @@ struct Sd2State {
 // are inlined: the class masses below are differences of such evaluations and
 // must come out exactly 0 when the class is empty and the states coincide.
 template <class T>
-__device__ __forceinline__ double sd2_mass(const Sd2State &st, const T *M1, const T *M2, int a, int b) {
+__device__ __forceinline__ double sd2_mass(Sd2State st, const T *M1, const T *M2, int a, int b) {
     const double u1a = st.u1[a], u1b = st.u1[b], u2a = st.u2[a], u2b = st.u2[b];
     const double m1 = static_cast<double>(M1[a * SD2_S + b]), m2 = static_cast<double>(M2[a * SD2_S + b]);
     const double pp = __dadd_rn(st.P[a * SD2_S + b], st.P[b * SD2_S + a]);
@@ -1274,64 +1297,83 @@ __device__ __forceinline__ double sd2_mass(const Sd2State &st, const T *M1, cons
 
 // Add the hands of opponent `who` (0 or 1) at rank positions [lo, hi) to the
 // sweep state.  R: that opponent's reach by rank position; Mo: that
-// opponent's matrix, Mx: the other's; uo / ux: their card sums.
+// opponent's matrix, Mx: the other's (symmetric); uo / ux: their card sums.
 template <class T>
-__device__ __forceinline__ void sd2_add(const Sd2State &st, const SdCombo *__restrict__ cb, const T *R, T *Mo,
-                                        const T *Mx, double *uo, const double *ux, int who, int lo, int hi) {
+__device__ __forceinline__ void sd2_add(Sd2State st, const unsigned short *dd, const T *R, T *Mo, const T *Mx,
+                                        double *uo, const double *ux, int who, int lo, int hi) {
     const int tid = threadIdx.x;
-    if (tid < SD2_S) {
-        // P = M1 M2: opponent 1's hand {x, y} adds to rows x, y (thread = column);
-        // opponent 2's adds to columns x, y (thread = row)
-        const int j = tid;
+    if (tid < 4 * SD2_N) {
+        // P = M1 M2: opponent 1's hand {x, y} adds r Mx[y][.] to row x and
+        // r Mx[x][.] to row y; opponent 2's adds the same to columns x, y.
+        // Thread (part, j) owns column (row) j of the rows (columns) x with
+        // x % 4 == part: the four suits of a rank fall to different threads.
+        const int part = tid / SD2_N, j = tid - part * SD2_N;
         for (int q = lo; q < hi; ++q) {
-            const double r = static_cast<double>(R[q]);
-            if (r == 0.0) continue;
-            const int x = cb[q].d1, y = cb[q].d2;
-            if (who == 0) {
-                st.P[x * SD2_S + j] += r * static_cast<double>(Mx[y * SD2_S + j]);
-                st.P[y * SD2_S + j] += r * static_cast<double>(Mx[x * SD2_S + j]);
-            } else {
-                st.P[j * SD2_S + x] += r * static_cast<double>(Mx[j * SD2_S + y]);
-                st.P[j * SD2_S + y] += r * static_cast<double>(Mx[j * SD2_S + x]);
+            const T rt = R[q];
+            if (rt == T(0)) continue;
+            const double r = static_cast<double>(rt);
+            const unsigned short e = dd[q];
+            const int x = sd2_c1(e), y = sd2_c2(e);
+            if ((x & 3) == part) {
+                double *p = who == 0 ? st.P + x * SD2_S + j : st.P + j * SD2_S + x;
+                *p += r * static_cast<double>(Mx[y * SD2_S + j]);
+            }
+            if ((y & 3) == part) {
+                double *p = who == 0 ? st.P + y * SD2_S + j : st.P + j * SD2_S + y;
+                *p += r * static_cast<double>(Mx[x * SD2_S + j]);
             }
         }
-    } else if (tid >= 64 && tid < 64 + SD2_S) {
-        // w = M2 u1 + M1 u2: the card sums of this opponent change at x, y,
-        // its matrix at (x, y)
-        const int c = tid - 64;
-        double acc = 0.0;
+    } else if (tid < 5 * SD2_N) {
+        // card c: this opponent's card sum u(c), d(c) = sum_b M1[c][b] M2[c][b]
+        // and w(c) = (M2 u1 + M1 u2)(c): the hand changes Mo at (x, y) and uo
+        // at x, y
+        const int c = tid - 4 * SD2_N;
+        double du = 0.0, dd_c = 0.0, dw = 0.0;
         for (int q = lo; q < hi; ++q) {
-            const double r = static_cast<double>(R[q]);
-            if (r == 0.0) continue;
-            const int x = cb[q].d1, y = cb[q].d2;
-            acc += r * (static_cast<double>(Mx[c * SD2_S + x]) + static_cast<double>(Mx[c * SD2_S + y]));
-            if (c == x) acc += r * ux[y];
-            if (c == y) acc += r * ux[x];
+            const T rt = R[q];
+            if (rt == T(0)) continue;
+            const double r = static_cast<double>(rt);
+            const unsigned short e = dd[q];
+            const int x = sd2_c1(e), y = sd2_c2(e);
+            const double mx = static_cast<double>(Mx[c * SD2_S + x]), my = static_cast<double>(Mx[c * SD2_S + y]);
+            dw += r * (mx + my);
+            if (c == x) {
+                du += r;
+                dd_c += r * my;
+                dw += r * ux[y];
+            }
+            if (c == y) {
+                du += r;
+                dd_c += r * mx;
+                dw += r * ux[x];
+            }
         }
-        st.w[c] += acc;
-    } else if (tid == 128) {
+        uo[c] += du;
+        st.d[c] += dd_c;
+        st.w[c] += dw;
+    } else if (tid == 5 * SD2_N) {
+        // F (this opponent's total), Q = sum u1 u2, D = sum d / 2
         double F = st.sc[who], Q = st.sc[2], D = st.sc[3];
         for (int q = lo; q < hi; ++q) {
-            const double r = static_cast<double>(R[q]);
-            if (r == 0.0) continue;
-            const int x = cb[q].d1, y = cb[q].d2;
-            const double m = static_cast<double>(Mx[x * SD2_S + y]);
+            const T rt = R[q];
+            if (rt == T(0)) continue;
+            const double r = static_cast<double>(rt);
+            const unsigned short e = dd[q];
+            const int x = sd2_c1(e), y = sd2_c2(e);
             Q += r * (ux[x] + ux[y]);
-            D += r * m;
-            st.d[x] += r * m;
-            st.d[y] += r * m;
-            uo[x] += r;
-            uo[y] += r;
+            D += r * static_cast<double>(Mx[x * SD2_S + y]);
             F += r;
         }
         st.sc[who] = F;
         st.sc[2] = Q;
         st.sc[3] = D;
-    } else if (tid >= 160) {
-        for (int q = lo + tid - 160; q < hi; q += kTermThreads - 160) {
+    } else {
+        constexpr int kFirst = 5 * SD2_N + 1, kStep = kTermThreads - kFirst;
+        for (int q = lo + tid - kFirst; q < hi; q += kStep) {
             const T r = R[q];
             if (r == T(0)) continue;
-            const int x = cb[q].d1, y = cb[q].d2;
+            const unsigned short e = dd[q];
+            const int x = sd2_c1(e), y = sd2_c2(e);
             Mo[x * SD2_S + y] = r;
             Mo[y * SD2_S + x] = r;
         }
@@ -1340,21 +1382,21 @@ __device__ __forceinline__ void sd2_add(const Sd2State &st, const SdCombo *__res
 
 // The sweep state for the opponents' hands at rank positions [0, qend),
 // computed directly (not by adding them one tie group at a time): the two
-// matrices, P = M1 M2 as FP64 4x4 tiles over the 48-card box, the card sums,
-// d, w and the scalars, each summed in a fixed order.  The caller syncs
-// before and after.
+// matrices, P = M1 M2 as FP64 3x3 tiles over the 48-card box, the card sums,
+// d = diag P, w = column sums + row sums of P, and the scalars, each summed
+// in a fixed order.  The caller syncs before; this syncs after.
 template <class T>
-__device__ void sd2_direct_state(const Sd2State &st, T *M1, T *M2, const T *R1, const T *R2,
-                                 const SdCombo *__restrict__ cb, int qend) {
+__device__ __forceinline__ void sd2_direct_state(Sd2State st, T *M1, T *M2, const T *R1, const T *R2,
+                                                 const unsigned short *dd, int qend) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < SD2_S * SD2_S; i += kTermThreads) {
         M1[i] = T(0);
         M2[i] = T(0);
-        st.P[i] = 0.0;
     }
     __syncthreads();
     for (int q = tid; q < qend; q += kTermThreads) {
-        const int x = cb[q].d1, y = cb[q].d2;
+        const unsigned short e = dd[q];
+        const int x = sd2_c1(e), y = sd2_c2(e);
         const T r1 = R1[q], r2 = R2[q];
         if (r1 != T(0)) {
             M1[x * SD2_S + y] = r1;
@@ -1366,48 +1408,53 @@ __device__ void sd2_direct_state(const Sd2State &st, T *M1, T *M2, const T *R1, 
         }
     }
     __syncthreads();
-    if (tid < 144) {
-        const int i0 = (tid / 12) * 4, j0 = (tid % 12) * 4;
-        double acc[4][4] = {};
-        for (int k = 0; k < 48; ++k) {
-            double xs[4], ys[4];
+    {
+        const int i0 = (tid >> 4) * 3, j0 = (tid & 15) * 3;
+        double acc[3][3] = {};
+        for (int k = 0; k < SD2_N; ++k) {
+            double xs[3], ys[3];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
+            for (int i = 0; i < 3; ++i) {
                 xs[i] = static_cast<double>(M1[(i0 + i) * SD2_S + k]);
                 ys[i] = static_cast<double>(M2[k * SD2_S + j0 + i]);
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] += xs[i] * ys[j];
+                for (int j = 0; j < 3; ++j) acc[i][j] += xs[i] * ys[j];
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) st.P[(i0 + i) * SD2_S + j0 + j] = acc[i][j];
-    } else if (tid >= 160 && tid < 160 + SD2_S) {
-        const int c = tid - 160;
-        double u1 = 0.0, u2 = 0.0, d = 0.0;
-        for (int r = 0; r < SD2_S; ++r) {
-            const double x1 = static_cast<double>(M1[r * SD2_S + c]), x2 = static_cast<double>(M2[r * SD2_S + c]);
-            u1 += x1;
-            u2 += x2;
-            d += x1 * x2;
-        }
-        st.u1[c] = u1;
-        st.u2[c] = u2;
-        st.d[c] = d;
+            for (int j = 0; j < 3; ++j) st.P[(i0 + i) * SD2_S + j0 + j] = acc[i][j];
     }
     __syncthreads();
-    if (tid < SD2_S) {
+    if (tid < SD2_N) {
         const int c = tid;
-        double w = 0.0;
-        for (int b = 0; b < SD2_S; ++b)
-            w += static_cast<double>(M2[c * SD2_S + b]) * st.u1[b] + static_cast<double>(M1[c * SD2_S + b]) * st.u2[b];
+        double u = 0.0;
+        for (int r = 0; r < SD2_N; ++r) u += static_cast<double>(M1[r * SD2_S + c]);
+        st.u1[c] = u;
+        st.d[c] = st.P[c * SD2_S + c];
+    } else if (tid >= 64 && tid < 64 + SD2_N) {
+        const int c = tid - 64;
+        double u = 0.0;
+        for (int r = 0; r < SD2_N; ++r) u += static_cast<double>(M2[r * SD2_S + c]);
+        st.u2[c] = u;
+    } else if (tid >= 128 && tid < 128 + SD2_N) {
+        const int c = tid - 128;
+        double w = 0.0;   // (M2 u1)(c) = sum_r P[r][c]
+        for (int r = 0; r < SD2_N; ++r) w += st.P[r * SD2_S + c];
         st.w[c] = w;
+    }
+    __syncthreads();
+    if (tid < SD2_N) {
+        const int c = tid;
+        double w = 0.0;   // (M1 u2)(c) = sum_r P[c][r]
+        for (int r = 0; r < SD2_N; ++r) w += st.P[c * SD2_S + r];
+        st.w[c] += w;
     } else if (warp == kTermThreads / 32 - 1) {
         double f1 = 0.0, f2 = 0.0, q = 0.0, e = 0.0;
-        for (int c = lane; c < SD2_S; c += 32) {
+        for (int c = lane; c < SD2_N; c += 32) {
             f1 += st.u1[c];
             f2 += st.u2[c];
             q += st.u1[c] * st.u2[c];
@@ -1427,18 +1474,62 @@ __device__ void sd2_direct_state(const Sd2State &st, T *M1, T *M2, const T *R1, 
     __syncthreads();
 }
 
+// A = D(L, L) for the traverser's hands at positions [lo, hi), and D(L, E)
+// summed over opponent 2's hands there (opponent 1 avoiding four cards);
+// classes of position q at cls[4 (q - base)], its hand at pt[q - base]
 template <class T>
-__global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevCtx *__restrict__ ctxs,
-                                                           const TermItem *__restrict__ items, int trav) {
+__device__ __forceinline__ void sd2_phase_a(Sd2State st, const T *M1, const T *M2, const T *R2,
+                                            const unsigned short *dd, const short *pt, double *cls, int base,
+                                            int lo, int hi) {
+    for (int q = lo + threadIdx.x; q < hi; q += kTermThreads) {
+        if (pt[q - base] < 0) continue;
+        const unsigned short e = dd[q];
+        const int a = sd2_c1(e), b = sd2_c2(e);
+        const double A = sd2_mass(st, M1, M2, a, b);
+        const double F1 = st.sc[0], u1a = st.u1[a], u1b = st.u1[b];
+        const double m1ab = static_cast<double>(M1[a * SD2_S + b]);
+        double dle = 0.0;
+        for (int q2 = lo; q2 < hi; ++q2) {
+            const T rt = R2[q2];
+            if (rt == T(0)) continue;
+            const unsigned short e2 = dd[q2];
+            const int x = sd2_c1(e2), y = sd2_c2(e2);
+            if (x == a || x == b || y == a || y == b) continue;
+            const double avoid = F1 - u1a - u1b - st.u1[x] - st.u1[y] + m1ab +
+                                 static_cast<double>(M1[a * SD2_S + x]) + static_cast<double>(M1[a * SD2_S + y]) +
+                                 static_cast<double>(M1[b * SD2_S + x]) + static_cast<double>(M1[b * SD2_S + y]) +
+                                 static_cast<double>(M1[x * SD2_S + y]);
+            dle += static_cast<double>(rt) * avoid;
+        }
+        cls[4 * (q - base)] = A;
+        cls[4 * (q - base) + 1] = dle;
+    }
+}
+
+// mass on the current state for the traverser's hands at [lo, hi), into
+// class slot k
+template <class T>
+__device__ __forceinline__ void sd2_phase_mass(Sd2State st, const T *M1, const T *M2, const unsigned short *dd,
+                                               const short *pt, double *cls, int base, int lo, int hi, int k) {
+    for (int q = lo + threadIdx.x; q < hi; q += kTermThreads)
+        if (pt[q - base] >= 0) cls[4 * (q - base) + k] = sd2_mass(st, M1, M2, sd2_c1(dd[q]), sd2_c2(dd[q]));
+}
+
+// One block per 2^lgm consecutive runs of a terminal's sweep (grid: items x
+// kSd2Chunks / 2^lgm).
+template <class T>
+__global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                              const TermItem *__restrict__ items, int trav, int lgm) {
     extern __shared__ __align__(16) char smem[];
-    const TermItem I = items[blockIdx.x / kSd2Chunks];
-    const int chunk = blockIdx.x % kSd2Chunks;
+    const int per = kSd2Chunks >> lgm;
+    const TermItem I = items[blockIdx.x / per];
+    const int grp = blockIdx.x % per;
     const int o1 = I.opp_player[0], o2 = I.opp_player[1];
     const T *reach;
     T *val;
     const int *pos_hand, *seg, *sd_pos;
     const SdCombo *cb;
-    int HS, nc, Ht, s0, s1;
+    int HS, nc, Ht, s0, s1, span;
     {
         const DevCtx &c = ctxs ? ctxs[I.sg] : c0;   // read once into registers below
         reach = reach_rows<T>(c);
@@ -1449,15 +1540,19 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
         cb = c.sd_combo;
         HS = c.HS;
         nc = c.ncomb;
+        span = c.sd_span[lgm];
         Ht = c.H[trav];
         const int *ch = c.sd_chunk + static_cast<size_t>(trav) * (kSd2Chunks + 1);
-        s0 = ch[chunk];
-        s1 = ch[chunk + 1];
+        s0 = ch[grp << lgm];
+        s1 = ch[(grp + 1) << lgm];
     }
-    // the launch provisioned shared memory for c0's row stride and rank table
+    // the launch provisioned shared memory for c0's rank table and run span
     // (the largest of a batch); a block needing more must not run
-    if (HS > c0.HS || nc > c0.ncomb) return;
+    if (HS > c0.HS || nc > c0.ncomb || span > c0.sd_span[lgm]) return;
     if (s0 >= s1) return;   // an unused run (the player has few tie groups)
+    const int4 *seg4 = reinterpret_cast<const int4 *>(seg);   // {lo, hi, holds a traverser hand, 0}
+    int4 sg = __ldg(seg4 + s0);
+    const int run_lo = sg.x, run_hi = __ldg(seg + 4 * (s1 - 1) + 1);
     const int tid = threadIdx.x, lane = tid & 31;
     Carve cv{smem};
     Sd2State st;
@@ -1469,16 +1564,16 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
     st.w = cv.take<double>(64);
     st.d = cv.take<double>(64);
     st.sc = cv.take<double>(8);
-    double *cls = cv.take<double>(4 * HS);   // per traverser hand: A, D(L, E), B, C
-    T *R1 = cv.take<T>(nc);
-    T *R2 = cv.take<T>(nc);
-    ulonglong2 *Bm = cv.take<ulonglong2>(53);
-    Cr2Cnt *cnt = cv.take<Cr2Cnt>(53);
-    Cr2Scalars *sc2 = cv.take<Cr2Scalars>(1);
+    double *cls = cv.take<double>(4 * span);   // per position of the run: A, D(L, E), B, C
+    char *rbuf = cv.take<char>(static_cast<int>(sd2_reach_bytes<T>(nc)));
+    T *R1 = reinterpret_cast<T *>(rbuf);
+    T *R2 = R1 + nc;
+    unsigned short *dd = cv.take<unsigned short>(nc);
+    short *pt = cv.take<short>(span);   // the traverser's hand at each position of the run, -1 if none
     int *last_pos = cv.take<int>(4);
 
-    // opponents' reach by rank position, and the last position holding
-    // positive reach of either opponent
+    // opponents' reach and the cards by rank position, and the last position
+    // holding positive reach of either opponent
     if (tid == 0) *last_pos = -1;
     if (tid < 64) {
         st.u1[tid] = 0.0;
@@ -1492,74 +1587,55 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
         const T *rb = reach + static_cast<size_t>(I.opp_row[1]) * HS;
         const int *pa = pos_hand + static_cast<size_t>(o1) * nc, *pb = pos_hand + static_cast<size_t>(o2) * nc;
         int lp = -1;
+#pragma unroll 4
         for (int q = tid; q < nc; q += kTermThreads) {
             const int ha = __ldg(pa + q), hb = __ldg(pb + q);
             const T x = ha >= 0 ? ra[ha] : T(0), y = hb >= 0 ? rb[hb] : T(0);
             R1[q] = x;
             R2[q] = y;
+            dd[q] = static_cast<unsigned short>(cb[q].d1 | (cb[q].d2 << 8));
             if (x > T(0) || y > T(0)) lp = q;
         }
         atomicMax(last_pos, lp);
+        const int *ph_t = pos_hand + static_cast<size_t>(trav) * nc + run_lo;
+        for (int k = tid; k < run_hi - run_lo; k += kTermThreads) pt[k] = static_cast<short>(__ldg(ph_t + k));
     }
     __syncthreads();
     // this run starts from the state of every hand ranked below it
-    const int run_lo = __ldg(seg + 4 * s0), run_hi = __ldg(seg + 4 * (s1 - 1) + 1);
-    sd2_direct_state(st, M1, M2, R1, R2, cb, run_lo);
+    sd2_direct_state(st, M1, M2, R1, R2, dd, run_lo);
 
-    const int *ph_t = pos_hand + static_cast<size_t>(trav) * nc;
+    // segment entries come from global memory a step ahead of their use
+    int4 nsg = s0 + 1 < s1 ? __ldg(seg4 + s0 + 1) : make_int4(0, 0, 0, 0);
+    if (sg.z) {
+        sd2_phase_a(st, M1, M2, R2, dd, pt, cls, run_lo, sg.x, sg.y);
+        __syncthreads();
+    }
     for (int si = s0; si < s1; ++si) {
-        const int lo = __ldg(seg + 4 * si), hi = __ldg(seg + 4 * si + 1), has = __ldg(seg + 4 * si + 2);
-        if (has) {
-            // opponents' hands weaker than the group: A, and D(L, E) summed
-            // over opponent 2's group hands (opponent 1 avoiding four cards)
-            for (int q = lo + tid; q < hi; q += kTermThreads) {
-                const int h = __ldg(ph_t + q);
-                if (h < 0) continue;
-                const int a = cb[q].d1, b = cb[q].d2;
-                const double A = sd2_mass(st, M1, M2, a, b);
-                const double F1 = st.sc[0], u1a = st.u1[a], u1b = st.u1[b];
-                const double m1ab = static_cast<double>(M1[a * SD2_S + b]);
-                double dle = 0.0;
-                for (int q2 = lo; q2 < hi; ++q2) {
-                    const double r = static_cast<double>(R2[q2]);
-                    if (r == 0.0) continue;
-                    const int x = cb[q2].d1, y = cb[q2].d2;
-                    if (x == a || x == b || y == a || y == b) continue;
-                    const double avoid = F1 - u1a - u1b - st.u1[x] - st.u1[y] + m1ab +
-                                         static_cast<double>(M1[a * SD2_S + x]) + static_cast<double>(M1[a * SD2_S + y]) +
-                                         static_cast<double>(M1[b * SD2_S + x]) + static_cast<double>(M1[b * SD2_S + y]) +
-                                         static_cast<double>(M1[x * SD2_S + y]);
-                    dle += r * avoid;
-                }
-                cls[4 * h] = A;
-                cls[4 * h + 1] = dle;
-            }
-            __syncthreads();
-        }
-        sd2_add(st, cb, R1, M1, M2, st.u1, st.u2, 0, lo, hi);
+        const int lo = sg.x, hi = sg.y;
+        const bool has = sg.z != 0, nhas = si + 1 < s1 && nsg.z != 0;
+        sd2_add(st, dd, R1, M1, M2, st.u1, st.u2, 0, lo, hi);
         __syncthreads();
         if (has) {
-            for (int q = lo + tid; q < hi; q += kTermThreads) {
-                const int h = __ldg(ph_t + q);
-                if (h >= 0) cls[4 * h + 2] = sd2_mass(st, M1, M2, cb[q].d1, cb[q].d2);
-            }
+            sd2_phase_mass(st, M1, M2, dd, pt, cls, run_lo, lo, hi, 2);
             __syncthreads();
         }
-        sd2_add(st, cb, R2, M2, M1, st.u2, st.u1, 1, lo, hi);
+        sd2_add(st, dd, R2, M2, M1, st.u2, st.u1, 1, lo, hi);
         __syncthreads();
-        if (has) {
-            for (int q = lo + tid; q < hi; q += kTermThreads) {
-                const int h = __ldg(ph_t + q);
-                if (h >= 0) cls[4 * h + 3] = sd2_mass(st, M1, M2, cb[q].d1, cb[q].d2);
-            }
-            __syncthreads();
-        }
+        // C of this group and A of the next group: the same state
+        if (has) sd2_phase_mass(st, M1, M2, dd, pt, cls, run_lo, lo, hi, 3);
+        if (nhas) sd2_phase_a(st, M1, M2, R2, dd, pt, cls, run_lo, nsg.x, nsg.y);
+        if (has || nhas) __syncthreads();
+        sg = nsg;   // the next segment's entry is loaded a full step before its use
+        if (si + 2 < s1) nsg = __ldg(seg4 + si + 2);
     }
 
     // all hands added (directly, unless this run ends the rank order): Z, and
     // the exact positive-pair count for hands whose mass is within the error
-    // bound of zero (masks over the 47-card matrices)
-    if (run_hi < nc) sd2_direct_state(st, M1, M2, R1, R2, cb, nc);
+    // bound of zero (masks over the 47-card matrices, in the reach space)
+    if (run_hi < nc) sd2_direct_state(st, M1, M2, R1, R2, dd, nc);
+    ulonglong2 *Bm = reinterpret_cast<ulonglong2 *>(rbuf);
+    Cr2Cnt *cnt = reinterpret_cast<Cr2Cnt *>(rbuf + 53 * sizeof(ulonglong2));
+    Cr2Scalars *sc2 = reinterpret_cast<Cr2Scalars *>(rbuf + 53 * sizeof(ulonglong2) + 53 * sizeof(Cr2Cnt));
     if (tid < 2 * 64) {
         const int col = tid & 63;
         const T *M = tid < 64 ? M1 : M2;
@@ -1600,27 +1676,31 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd2(DevCtx c0, const DevC
     // - bet, or -bet): a coefficient that is exactly 0 drops its class exactly
     const double cw = static_cast<double>(I.pot - I.bet), c1 = static_cast<double>(I.pot / 2.0f - I.bet);
     const double c2 = static_cast<double>(I.pot / 3.0f - I.bet), cl = -static_cast<double>(I.bet);
-    const int *tp = sd_pos + static_cast<size_t>(trav) * HS;
     T *out = val + static_cast<size_t>(I.node) * HS;
     const int lastp = *last_pos;
-    for (int h = tid; h < HS; h += kTermThreads) {
-        double v = 0.0;
-        const int q = h < Ht ? __ldg(tp + h) : -1;
-        // hands of this run's tie groups; the first run also writes the hands
-        // without a rank position (and the padding)
-        if (q >= 0 ? (q < run_lo || q >= run_hi) : chunk != 0) continue;
-        if (q >= 0) {
-            const int a = cb[q].d1, b = cb[q].d2;
-            const double Z = sd2_mass(st, M1, M2, a, b);
-            const double A = cls[4 * h], dle = cls[4 * h + 1], B = cls[4 * h + 2], C = cls[4 * h + 3];
-            // no positive-reach opponent hand ranked above the group: the loss
-            // class is empty, exactly (Z and C may come from different runs)
-            const double L = cb[q].hi > lastp ? 0.0 : Z - C;
-            const double W2 = A, T1 = (B - A) + dle, T2 = (C - B) - dle;
-            v = cw * W2 + c1 * T1 + c2 * T2 + cl * L;
-            if (fabs(Z) <= zmin && pair_count(Bm, cnt, a, b, S2.IF1, S2.IF2, S2.IQD) <= 0) v = 0.0;
-        }
+    // the traverser's hands at this run's positions
+    for (int q = run_lo + tid; q < run_hi; q += kTermThreads) {
+        const int h = pt[q - run_lo];
+        if (h < 0) continue;
+        const unsigned short e = dd[q];
+        const int a = sd2_c1(e), b = sd2_c2(e);
+        const double Z = sd2_mass(st, M1, M2, a, b);
+        const double *k4 = cls + 4 * (q - run_lo);
+        const double A = k4[0], dle = k4[1], B = k4[2], C = k4[3];
+        // no positive-reach opponent hand ranked above the group: the loss
+        // class is empty, exactly (Z and C may come from different runs)
+        const double L = __ldg(&cb[q].hi) > lastp ? 0.0 : Z - C;
+        const double W2 = A, T1 = (B - A) + dle, T2 = (C - B) - dle;
+        double v = cw * W2 + c1 * T1 + c2 * T2 + cl * L;
+        if (fabs(Z) <= zmin && pair_count(Bm, cnt, a, b, S2.IF1, S2.IF2, S2.IQD) <= 0) v = 0.0;
         out[h] = static_cast<T>(v);
+    }
+    // the first block of the terminal also writes the hands without a rank
+    // position (board-blocked) and the padding
+    if (grp == 0) {
+        const int *tp = sd_pos + static_cast<size_t>(trav) * HS;
+        for (int h = tid; h < HS; h += kTermThreads)
+            if (h >= Ht || __ldg(tp + h) < 0) out[h] = T(0);
     }
 }
 
@@ -1938,10 +2018,13 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             k_term_sd1<T><<<n, kTermThreads, sd1_smem<T>(), s>>>(c, ctxs, items, trav);
             break;
         case TK_SD2: {
-            const size_t sm = sd2_smem<T>(c.HS, c.ncomb);
+            // runs per block: about two waves of four blocks per SM at most
+            int lgm = 0;
+            while (lgm < kSd2Merge - 1 && n * (kSd2Chunks >> lgm) > kSd2BlocksTarget) ++lgm;
+            const size_t sm = sd2_smem<T>(c.sd_span[lgm], c.ncomb);
             e = cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
             if (e != cudaSuccess) return e;
-            k_term_sd2<T><<<n * kSd2Chunks, kTermThreads, sm, s>>>(c, ctxs, items, trav);
+            k_term_sd2<T><<<n * (kSd2Chunks >> lgm), kTermThreads, sm, s>>>(c, ctxs, items, trav, lgm);
             break;
         }
         case TK_ENUM: {

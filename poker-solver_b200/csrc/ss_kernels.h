@@ -33,6 +33,7 @@ struct DevCtx {
     int HS;
     int np;
     int ncomb;
+    int sd_span[kSd2Merge];      // most rank positions of 2^lg merged three-way showdown sweep runs
     int deck;              // number of non-board cards (dense card indices 0 .. deck-1)
     int H[SS_MAX_PLAYERS];
     int dup[SS_MAX_PLAYERS];     // range holds some combo more than once

@@ -229,6 +229,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     c.HS = P.HS;
     c.np = np;
     c.ncomb = P.ncomb;
+    for (int lg = 0; lg < kSd2Merge; ++lg) c.sd_span[lg] = P.sd_span[lg];
     c.deck = P.deck;
     for (int p = 0; p < SS_MAX_PLAYERS; ++p) {
         c.H[p] = p < np ? P.H[p] : 0;

@@ -372,6 +372,7 @@ int build_plan(const Problem &pb, Plan *out) {
     P.pos_hand.clear();
     P.sd_seg.clear();
     P.sd_chunk.clear();
+    for (int lg = 0; lg < kSd2Merge; ++lg) P.sd_span[lg] = 0;
     for (int p = 0; p <= SS_MAX_PLAYERS; ++p) P.sd_seg_off[p] = 0;
     P.strength.assign(static_cast<size_t>(np) * HS, 0u);
     if (need_sd) {
@@ -455,13 +456,37 @@ int build_plan(const Problem &pb, Plan *out) {
             }
         }
         P.sd_seg_off[np] = static_cast<int>(P.sd_seg.size() / 4);
+        // runs of equal sweep cost: K = total cost / kSd2RunCost (1 .. kSd2Chunks),
+        // run k ends at the first segment boundary reaching k / K of the cost
         P.sd_chunk.assign(static_cast<size_t>(np) * (kSd2Chunks + 1), 0);
         for (int p = 0; p < np; ++p) {
-            const int a = P.sd_seg_off[p], b = P.sd_seg_off[p + 1], n = b - a;
-            const int K = std::max(1, std::min(kSd2Chunks, n / kSd2SegsPerChunk));
+            const int a = P.sd_seg_off[p], b = P.sd_seg_off[p + 1];
+            long long total = 0;
+            for (int i = a; i < b; ++i) total += kSd2SegCost + P.sd_seg[4 * i + 1] - P.sd_seg[4 * i];
+            const int K = static_cast<int>(std::max(1LL, std::min<long long>({kSd2Chunks, b - a, total / kSd2RunCost})));
             int *ch = P.sd_chunk.data() + static_cast<size_t>(p) * (kSd2Chunks + 1);
-            for (int i = 0; i <= kSd2Chunks; ++i)
-                ch[i] = i <= K ? a + static_cast<int>(static_cast<long long>(i) * n / K) : b;
+            ch[0] = a;
+            long long acc = 0;
+            int i = a;
+            for (int k = 1; k <= kSd2Chunks; ++k) {
+                if (k < K) {
+                    const long long goal = total * k / K;
+                    // at least one segment per run, and leave one for each later run
+                    do {
+                        acc += kSd2SegCost + P.sd_seg[4 * i + 1] - P.sd_seg[4 * i];
+                        ++i;
+                    } while (i < b - (K - k) && acc < goal);
+                    ch[k] = i;
+                } else {
+                    ch[k] = b;
+                }
+            }
+            for (int lg = 0; lg < kSd2Merge; ++lg)
+                for (int r = 0; r < kSd2Chunks; r += 1 << lg) {
+                    const int s0 = ch[r], s1 = ch[r + (1 << lg)];
+                    if (s1 > s0)
+                        P.sd_span[lg] = std::max(P.sd_span[lg], P.sd_seg[4 * (s1 - 1) + 1] - P.sd_seg[4 * s0]);
+                }
         }
     }
 

@@ -139,3 +139,96 @@ def test_sweep_matches_enumeration(seed, nh, board):
     scale = max(1.0, max(abs(v) for v in want.values()))
     for h in trav:
         assert abs(got[h] - want[h]) <= 1e-9 * scale, (h, got[h], want[h])
+
+
+def _direct(order, dense, opp1, opp2, qend):
+    """The state of the hands at rank positions [0, qend) computed directly,
+    as the kernel does at the start of each run: d = diag(P) and
+    w = M2 u1 + M1 u2 = column sums + row sums of P (M1, M2 symmetric)."""
+    st = Sweep()
+    for c in order[:qend]:
+        x, y = dense[c[0]], dense[c[1]]
+        for k, opp in enumerate((opp1, opp2)):
+            r = opp.get(c, 0.0)
+            if r > 0:
+                st.M[k][x, y] = st.M[k][y, x] = r
+    st.P = st.M[0] @ st.M[1]
+    st.u = [st.M[0].sum(0), st.M[1].sum(0)]
+    st.d = np.diag(st.P).copy()
+    st.w = st.P.sum(0) + st.P.sum(1)
+    st.F = [0.5 * st.u[0].sum(), 0.5 * st.u[1].sum()]
+    st.Q = float(st.u[0] @ st.u[1])
+    st.Dd = 0.5 * st.d.sum()
+    return st
+
+
+def _sweep_runs(strength, order, dense, trav, opp1, opp2, nruns):
+    """The sweep cut into runs of tie groups, each starting from a directly
+    computed state; the loss class from a direct state of all hands."""
+    groups, q = [], 0
+    while q < len(order):
+        hi = q
+        while hi < len(order) and strength[order[hi]] == strength[order[q]]:
+            hi += 1
+        groups.append((q, hi))
+        q = hi
+    cuts = [len(groups) * k // nruns for k in range(nruns + 1)]
+    cls = {}
+    for k in range(nruns):
+        g0, g1 = cuts[k], cuts[k + 1]
+        if g0 == g1:
+            continue
+        st = _direct(order, dense, opp1, opp2, groups[g0][0])
+        for lo, hi in groups[g0:g1]:
+            group = order[lo:hi]
+            hs = [h for h in group if h in trav]
+            h1 = [((dense[c[0]], dense[c[1]]), opp1[c]) for c in group if opp1.get(c, 0.0) > 0]
+            h2 = [((dense[c[0]], dense[c[1]]), opp2[c]) for c in group if opp2.get(c, 0.0) > 0]
+            for h in hs:
+                a, b = dense[h[0]], dense[h[1]]
+                M1, u1 = st.M[0], st.u[0]
+                dle = sum(r * (st.F[0] - u1[a] - u1[b] - u1[x] - u1[y] + M1[a, b] + M1[a, x] + M1[a, y]
+                               + M1[b, x] + M1[b, y] + M1[x, y])
+                          for (x, y), r in h2 if len({a, b, x, y}) == 4)
+                cls[h] = [st.mass(a, b), dle]
+            st.add(0, h1)
+            for h in hs:
+                cls[h].append(st.mass(dense[h[0]], dense[h[1]]))
+            st.add(1, h2)
+            for h in hs:
+                cls[h].append(st.mass(dense[h[0]], dense[h[1]]))
+    full = _direct(order, dense, opp1, opp2, len(order))
+    out = {}
+    for h in trav:
+        A, dle, B, C = cls[h]
+        Z = full.mass(dense[h[0]], dense[h[1]])
+        W2, T1, T2 = A, (B - A) + dle, (C - B) - dle
+        out[h] = (POT - BET) * W2 + (POT / 2 - BET) * T1 + (POT / 3 - BET) * T2 - BET * (Z - C)
+    return out
+
+
+@pytest.mark.parametrize("seed,nh,board,nruns", [
+    (5, 12, None, 3), (6, 14, None, 7), (7, 10, None, 16),
+    (8, 12, ["Ks", "Kd", "Kh", "Kc", "2s"], 4),
+    (9, 10, ["As", "Ks", "Qs", "Js", "Ts"], 2),
+])
+def test_runs_from_direct_states_match_enumeration(seed, nh, board, nruns):
+    b = None if board is None else [card_to_int(c) for c in board]
+    strength, order, dense, trav, opp1, opp2 = _setup(seed, nh, b)
+    want = _brute(strength, trav, opp1, opp2)
+    got = _sweep_runs(strength, order, dense, trav, opp1, opp2, nruns)
+    scale = max(1.0, max(abs(v) for v in want.values()))
+    for h in trav:
+        assert abs(got[h] - want[h]) <= 1e-9 * scale, (h, got[h], want[h])
+
+
+def test_direct_state_equals_incremental():
+    strength, order, dense, trav, opp1, opp2 = _setup(10, 40, None)
+    inc = Sweep()
+    inc.add(0, [((dense[c[0]], dense[c[1]]), opp1[c]) for c in order if opp1.get(c, 0.0) > 0])
+    inc.add(1, [((dense[c[0]], dense[c[1]]), opp2[c]) for c in order if opp2.get(c, 0.0) > 0])
+    dr = _direct(order, dense, opp1, opp2, len(order))
+    for a, b in [(inc.P, dr.P), (inc.w, dr.w), (inc.d, dr.d), (inc.u[0], dr.u[0]), (inc.u[1], dr.u[1])]:
+        assert np.allclose(a, b, rtol=1e-12, atol=1e-12)
+    assert abs(inc.Q - dr.Q) < 1e-9 and abs(inc.Dd - dr.Dd) < 1e-9
+    assert abs(inc.F[0] - dr.F[0]) < 1e-9 and abs(inc.F[1] - dr.F[1]) < 1e-9
