@@ -98,6 +98,9 @@ constexpr int kSd2Chunks = 16;
 // directly computed states
 constexpr int kSd2SegCost = 6;
 constexpr int kSd2RunCost = 96;
+// sweep blocks resident at once (148 SMs, 4 blocks each): a traverser's runs
+// are capped so that its terminals' blocks fit one wave
+constexpr int kSd2Slots = 148 * 4;
 // A launch may give each block 2^lg consecutive runs (lg < kSd2Merge): many
 // terminals in one launch (batches) need fewer, longer sweeps.
 constexpr int kSd2Merge = 5;

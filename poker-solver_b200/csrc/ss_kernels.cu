@@ -1224,12 +1224,14 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
 // only X's and Y's hands.  The kernel sweeps the combos in rank order and
 // keeps that form's aggregates (P = M1 M2, u_i, w, d, F_i, Q, D; FP64) for
 // the opponents' hands added so far; per tie group of the traverser's hands
-// it reads A = D(L, L) before the group, B = D(L+E, L) after adding
-// opponent 1's group hands and C = D(L+E, L+E) after opponent 2's, and sums
-// D(L, E) directly over opponent 2's group hands (each term an exact
-// four-card removal for opponent 1).  With Z read after the sweep:
-//   W2 = A, T1 = (B - A) + D(L, E), T2 = (C - B) - D(L, E), lose = Z - C,
-//   value = (pot - bet) W2 + (pot/2 - bet) T1 + (pot/3 - bet) T2 - bet lose.
+// it reads A = D(L, L) before the group and C = D(L+E, L+E) after adding
+// both opponents' group hands, and sums D(L, E) over opponent 2's group
+// hands and D(E, L) over opponent 1's directly (each term an exact four-card
+// removal for the other opponent).  With Z read after the sweep:
+//   W2 = A, T1 = D(E, L) + D(L, E), T2 = C - A - T1, lose = Z - C,
+//   value = (pot - bet) W2 + (pot/2 - bet) T1 + (pot/3 - bet) T2 - bet lose,
+// and T2 = 0 exactly when opponent 2 holds nothing in the group (C is then
+// B = D(L+E, L), and C - B the empty class).
 // Adding a hand changes two rows (or columns) of P, two card sums and every
 // w entry, so each phase gives threads fixed ownership (P cells by column
 // and row residue, one card's u / d / w, the scalars, matrix cells), each
@@ -1237,7 +1239,8 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
 // fixed summation order.  The sweep of a terminal is cut into runs of tie
 // groups of about equal cost, one block each, starting from a directly
 // computed state (the product P as 3x3 FP64 tiles over all 256 threads).
-// C of a group and A of the next are read in one phase (the same state).
+// C of a group and A of the next are read in one phase (the same state); the
+// tie sums of a traverser hand are split over eight lanes.
 // ---------------------------------------------------------------------------
 constexpr int SD2_S = 49;   // row stride of the sweep's card matrices (odd: conflict-free columns)
 constexpr int SD2_N = 48;   // cards a matrix covers (dense indices; a river deck has 47)
@@ -1474,35 +1477,62 @@ __device__ __forceinline__ void sd2_direct_state(Sd2State st, T *M1, T *M2, cons
     __syncthreads();
 }
 
-// A = D(L, L) for the traverser's hands at positions [lo, hi), and D(L, E)
-// summed over opponent 2's hands there (opponent 1 avoiding four cards);
-// classes of position q at cls[4 (q - base)], its hand at pt[q - base]
+// For the traverser's hands at positions [lo, hi) (a tie group), on the state
+// before the group: A = D(L, L); T1 = D(L, E) + D(E, L), summing over
+// opponent 2's group hands (opponent 1's weaker hands avoiding four cards)
+// and over opponent 1's (opponent 2's avoiding four cards); whether opponent 2
+// holds any group hand.  Eight lanes per hand, each taking every eighth group
+// position, combined in a fixed order.  Classes of position q at
+// cls[4 (q - base)]: A, T1, opponent 2 present, (C).
 template <class T>
-__device__ __forceinline__ void sd2_phase_a(Sd2State st, const T *M1, const T *M2, const T *R2,
+__device__ __forceinline__ void sd2_phase_a(Sd2State st, const T *M1, const T *M2, const T *R1, const T *R2,
                                             const unsigned short *dd, const short *pt, double *cls, int base,
                                             int lo, int hi) {
-    for (int q = lo + threadIdx.x; q < hi; q += kTermThreads) {
-        if (pt[q - base] < 0) continue;
-        const unsigned short e = dd[q];
-        const int a = sd2_c1(e), b = sd2_c2(e);
-        const double A = sd2_mass(st, M1, M2, a, b);
-        const double F1 = st.sc[0], u1a = st.u1[a], u1b = st.u1[b];
-        const double m1ab = static_cast<double>(M1[a * SD2_S + b]);
-        double dle = 0.0;
-        for (int q2 = lo; q2 < hi; ++q2) {
-            const T rt = R2[q2];
-            if (rt == T(0)) continue;
-            const unsigned short e2 = dd[q2];
-            const int x = sd2_c1(e2), y = sd2_c2(e2);
-            if (x == a || x == b || y == a || y == b) continue;
-            const double avoid = F1 - u1a - u1b - st.u1[x] - st.u1[y] + m1ab +
-                                 static_cast<double>(M1[a * SD2_S + x]) + static_cast<double>(M1[a * SD2_S + y]) +
-                                 static_cast<double>(M1[b * SD2_S + x]) + static_cast<double>(M1[b * SD2_S + y]) +
-                                 static_cast<double>(M1[x * SD2_S + y]);
-            dle += static_cast<double>(rt) * avoid;
+    const int l8 = threadIdx.x & 7, team = threadIdx.x >> 3;
+    const int tbit = threadIdx.x & 24;   // the team's first lane in its warp
+    for (int q0 = lo; q0 < hi; q0 += kTermThreads / 8) {
+        const int q = q0 + team;
+        const bool mine = q < hi && pt[q - base] >= 0;   // the same for all lanes of a team
+        double t1 = 0.0;
+        bool any2 = false;
+        int a = 0, b = 0;
+        if (mine) {
+            const unsigned short e = dd[q];
+            a = sd2_c1(e);
+            b = sd2_c2(e);
+            const double F1 = st.sc[0], F2 = st.sc[1];
+            const double u1a = st.u1[a], u1b = st.u1[b], u2a = st.u2[a], u2b = st.u2[b];
+            const double m1ab = static_cast<double>(M1[a * SD2_S + b]), m2ab = static_cast<double>(M2[a * SD2_S + b]);
+            double dle = 0.0, del = 0.0;
+            for (int q2 = lo + l8; q2 < hi; q2 += 8) {
+                const T r1 = R1[q2], r2 = R2[q2];
+                any2 = any2 || r2 != T(0);
+                if (r1 == T(0) && r2 == T(0)) continue;
+                const unsigned short e2 = dd[q2];
+                const int x = sd2_c1(e2), y = sd2_c2(e2);
+                if (x == a || x == b || y == a || y == b) continue;
+                if (r2 != T(0))
+                    dle += static_cast<double>(r2) *
+                           (F1 - u1a - u1b - st.u1[x] - st.u1[y] + m1ab + static_cast<double>(M1[a * SD2_S + x]) +
+                            static_cast<double>(M1[a * SD2_S + y]) + static_cast<double>(M1[b * SD2_S + x]) +
+                            static_cast<double>(M1[b * SD2_S + y]) + static_cast<double>(M1[x * SD2_S + y]));
+                if (r1 != T(0))
+                    del += static_cast<double>(r1) *
+                           (F2 - u2a - u2b - st.u2[x] - st.u2[y] + m2ab + static_cast<double>(M2[a * SD2_S + x]) +
+                            static_cast<double>(M2[a * SD2_S + y]) + static_cast<double>(M2[b * SD2_S + x]) +
+                            static_cast<double>(M2[b * SD2_S + y]) + static_cast<double>(M2[x * SD2_S + y]));
+            }
+            t1 = dle + del;
         }
-        cls[4 * (q - base)] = A;
-        cls[4 * (q - base) + 1] = dle;
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) t1 += __shfl_xor_sync(0xffffffffu, t1, o);
+        const unsigned bal = __ballot_sync(0xffffffffu, any2);
+        if (mine && l8 == 0) {
+            double *k4 = cls + 4 * (q - base);
+            k4[0] = sd2_mass(st, M1, M2, a, b);
+            k4[1] = t1;
+            k4[2] = ((bal >> tbit) & 0xffu) ? 1.0 : 0.0;
+        }
     }
 }
 
@@ -1564,7 +1594,7 @@ __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const D
     st.w = cv.take<double>(64);
     st.d = cv.take<double>(64);
     st.sc = cv.take<double>(8);
-    double *cls = cv.take<double>(4 * span);   // per position of the run: A, D(L, E), B, C
+    double *cls = cv.take<double>(4 * span);   // per position of the run: A, T1, opponent 2 present, C
     char *rbuf = cv.take<char>(static_cast<int>(sd2_reach_bytes<T>(nc)));
     T *R1 = reinterpret_cast<T *>(rbuf);
     T *R2 = R1 + nc;
@@ -1607,7 +1637,7 @@ __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const D
     // segment entries come from global memory a step ahead of their use
     int4 nsg = s0 + 1 < s1 ? __ldg(seg4 + s0 + 1) : make_int4(0, 0, 0, 0);
     if (sg.z) {
-        sd2_phase_a(st, M1, M2, R2, dd, pt, cls, run_lo, sg.x, sg.y);
+        sd2_phase_a(st, M1, M2, R1, R2, dd, pt, cls, run_lo, sg.x, sg.y);
         __syncthreads();
     }
     for (int si = s0; si < s1; ++si) {
@@ -1615,15 +1645,11 @@ __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const D
         const bool has = sg.z != 0, nhas = si + 1 < s1 && nsg.z != 0;
         sd2_add(st, dd, R1, M1, M2, st.u1, st.u2, 0, lo, hi);
         __syncthreads();
-        if (has) {
-            sd2_phase_mass(st, M1, M2, dd, pt, cls, run_lo, lo, hi, 2);
-            __syncthreads();
-        }
         sd2_add(st, dd, R2, M2, M1, st.u2, st.u1, 1, lo, hi);
         __syncthreads();
         // C of this group and A of the next group: the same state
         if (has) sd2_phase_mass(st, M1, M2, dd, pt, cls, run_lo, lo, hi, 3);
-        if (nhas) sd2_phase_a(st, M1, M2, R2, dd, pt, cls, run_lo, nsg.x, nsg.y);
+        if (nhas) sd2_phase_a(st, M1, M2, R1, R2, dd, pt, cls, run_lo, nsg.x, nsg.y);
         if (has || nhas) __syncthreads();
         sg = nsg;   // the next segment's entry is loaded a full step before its use
         if (si + 2 < s1) nsg = __ldg(seg4 + si + 2);
@@ -1686,12 +1712,12 @@ __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const D
         const int a = sd2_c1(e), b = sd2_c2(e);
         const double Z = sd2_mass(st, M1, M2, a, b);
         const double *k4 = cls + 4 * (q - run_lo);
-        const double A = k4[0], dle = k4[1], B = k4[2], C = k4[3];
+        const double A = k4[0], T1 = k4[1], C = k4[3];
         // no positive-reach opponent hand ranked above the group: the loss
         // class is empty, exactly (Z and C may come from different runs)
         const double L = __ldg(&cb[q].hi) > lastp ? 0.0 : Z - C;
-        const double W2 = A, T1 = (B - A) + dle, T2 = (C - B) - dle;
-        double v = cw * W2 + c1 * T1 + c2 * T2 + cl * L;
+        const double T2 = k4[2] != 0.0 ? (C - A) - T1 : 0.0;
+        double v = cw * A + c1 * T1 + c2 * T2 + cl * L;
         if (fabs(Z) <= zmin && pair_count(Bm, cnt, a, b, S2.IF1, S2.IF2, S2.IQD) <= 0) v = 0.0;
         out[h] = static_cast<T>(v);
     }

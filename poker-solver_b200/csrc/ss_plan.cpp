@@ -456,14 +456,18 @@ int build_plan(const Problem &pb, Plan *out) {
             }
         }
         P.sd_seg_off[np] = static_cast<int>(P.sd_seg.size() / 4);
-        // runs of equal sweep cost: K = total cost / kSd2RunCost (1 .. kSd2Chunks),
-        // run k ends at the first segment boundary reaching k / K of the cost
+        // runs of equal sweep cost: K = total cost / kSd2RunCost (1 .. kSd2Chunks,
+        // and at most one wave of blocks over the traverser's three-way
+        // showdowns), run k ends at the first segment boundary reaching k / K
+        // of the cost
         P.sd_chunk.assign(static_cast<size_t>(np) * (kSd2Chunks + 1), 0);
         for (int p = 0; p < np; ++p) {
             const int a = P.sd_seg_off[p], b = P.sd_seg_off[p + 1];
             long long total = 0;
             for (int i = a; i < b; ++i) total += kSd2SegCost + P.sd_seg[4 * i + 1] - P.sd_seg[4 * i];
-            const int K = static_cast<int>(std::max(1LL, std::min<long long>({kSd2Chunks, b - a, total / kSd2RunCost})));
+            const long long nt = static_cast<long long>(P.term[p][TK_SD2].size());
+            const int K = static_cast<int>(std::max(
+                1LL, std::min<long long>({kSd2Chunks, b - a, total / kSd2RunCost, nt ? kSd2Slots / nt : kSd2Chunks})));
             int *ch = P.sd_chunk.data() + static_cast<size_t>(p) * (kSd2Chunks + 1);
             ch[0] = a;
             long long acc = 0;

@@ -164,7 +164,10 @@ def _direct(order, dense, opp1, opp2, qend):
 
 def _sweep_runs(strength, order, dense, trav, opp1, opp2, nruns):
     """The sweep cut into runs of tie groups, each starting from a directly
-    computed state; the loss class from a direct state of all hands."""
+    computed state, in the kernel's class form: A before the group, both tie
+    sums D(L, E) + D(E, L) directly, C after the group, T2 = C - A - T1 (0
+    when opponent 2 holds nothing in the group); the loss class from a direct
+    state of all hands."""
     groups, q = [], 0
     while q < len(order):
         hi = q
@@ -184,26 +187,27 @@ def _sweep_runs(strength, order, dense, trav, opp1, opp2, nruns):
             hs = [h for h in group if h in trav]
             h1 = [((dense[c[0]], dense[c[1]]), opp1[c]) for c in group if opp1.get(c, 0.0) > 0]
             h2 = [((dense[c[0]], dense[c[1]]), opp2[c]) for c in group if opp2.get(c, 0.0) > 0]
-            for h in hs:
+            for h in hs:                 # A, and both tie sums directly (four-card removals)
                 a, b = dense[h[0]], dense[h[1]]
-                M1, u1 = st.M[0], st.u[0]
+                M1, u1, M2, u2 = st.M[0], st.u[0], st.M[1], st.u[1]
                 dle = sum(r * (st.F[0] - u1[a] - u1[b] - u1[x] - u1[y] + M1[a, b] + M1[a, x] + M1[a, y]
                                + M1[b, x] + M1[b, y] + M1[x, y])
                           for (x, y), r in h2 if len({a, b, x, y}) == 4)
-                cls[h] = [st.mass(a, b), dle]
+                del_ = sum(r * (st.F[1] - u2[a] - u2[b] - u2[x] - u2[y] + M2[a, b] + M2[a, x] + M2[a, y]
+                                + M2[b, x] + M2[b, y] + M2[x, y])
+                           for (x, y), r in h1 if len({a, b, x, y}) == 4)
+                cls[h] = [st.mass(a, b), dle + del_, len(h2) > 0]
             st.add(0, h1)
-            for h in hs:
-                cls[h].append(st.mass(dense[h[0]], dense[h[1]]))
             st.add(1, h2)
             for h in hs:
                 cls[h].append(st.mass(dense[h[0]], dense[h[1]]))
     full = _direct(order, dense, opp1, opp2, len(order))
     out = {}
     for h in trav:
-        A, dle, B, C = cls[h]
+        A, T1, opp2_present, C = cls[h]
         Z = full.mass(dense[h[0]], dense[h[1]])
-        W2, T1, T2 = A, (B - A) + dle, (C - B) - dle
-        out[h] = (POT - BET) * W2 + (POT / 2 - BET) * T1 + (POT / 3 - BET) * T2 - BET * (Z - C)
+        T2 = (C - A) - T1 if opp2_present else 0.0
+        out[h] = (POT - BET) * A + (POT / 2 - BET) * T1 + (POT / 3 - BET) * T2 - BET * (Z - C)
     return out
 
 
