@@ -393,6 +393,9 @@ def run_batched(n, seed, device):
             raise RuntimeError(f"plain solve failed ({rc})")
         plain.append(r["stats"])
     t_plain = time.perf_counter() - t0
+    # warm the batched path (its kernels load on first use) as the plain
+    # leg was warmed above: one short batch over the first requests
+    rc, _ = wl.batch_solve(subs[:16], CHECK, target=TARGET, check_every=CHECK, device=device)
     t0 = time.perf_counter()
     rc, res = wl.batch_solve(subs, MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
     t_batch = time.perf_counter() - t0

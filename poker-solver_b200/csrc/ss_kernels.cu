@@ -214,7 +214,17 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
 #pragma unroll
                     for (int i = 0; i < 8; ++i) add2(e, x[i]);
                 }
-                for (; k < k1; k += S) add2(e, ld2(val + static_cast<size_t>(__ldg(fr + k)) * HS));
+                if (k < k1) {
+                    // the last (< 8) rows of this warp, loaded together; the
+                    // missing ones add +0, so the sum is the row-order sum
+                    float2 x[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        x[i] = k + i * S < k1 ? ld2(val + static_cast<size_t>(__ldg(fr + k + i * S)) * HS)
+                                              : make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) add2(e, x[i]);
+                }
                 ev[a] = e;
             }
         }
