@@ -204,6 +204,42 @@ def build_subgame(seed, iterations, workload=WORKLOAD):
     return cfg, sg
 
 
+def flow_bytes_per_iteration(td, H):
+    """FP32 bytes one CFR iteration of the reference's data flow moves on this
+    tree with H hands per player (street_solve.cu:1471-1550), summed over the
+    traversers t; for each decision node with A actions: regret matching
+    (regrets read, strategy written) 8 A H; reach of every player rp != t
+    (parent row read, A child rows written, plus the strategy read at rp's
+    own nodes) 4 H + 4 A H (+ 4 A H); values (A child rows read, one row
+    written, plus strategy read and regret / strategy-sum read-modify-write
+    at t's nodes) 4 A H + 4 H (+ 20 A H); each terminal: the counted
+    opponents' reach rows and the value row 4 H (k + 1), plus k + 1 rank rows
+    at showdowns and the leaf-value row at leaves."""
+    np_ = td.num_players_field
+    typ, ply, nch, act = [], [], [], []
+    for i in range(td.num_nodes):
+        n = td.nodes[i]
+        typ.append(n.type)
+        ply.append(n.player)
+        nch.append(n.num_children)
+        act.append([n.active_players[o] for o in range(np_)])
+    total = 0
+    for t in range(np_):
+        for ty, p, A, ac in zip(typ, ply, nch, act):
+            if ty == 0:
+                total += 8 * A * H
+                total += (np_ - 1) * (4 * H + 4 * A * H) + (4 * A * H if p != t else 0)
+                total += 4 * A * H + 4 * H + (20 * A * H if p == t else 0)
+            else:
+                k = np_ - 1 if ty == 1 else sum(1 for o in range(np_) if o != t and ac[o])
+                total += 4 * H * (k + 1)
+                if ty == 2:
+                    total += 4 * H * (k + 1)
+                elif ty == 4:
+                    total += 4 * H
+    return total
+
+
 def run_ours(args, world, rank, local):
     import torch
     import street_solver_gpu as ssg
@@ -341,6 +377,15 @@ def run_ours(args, world, rank, local):
         pass
 
     tree_info = {"nodes": nnodes, "decision": ndec, "leaves": sg.num_leaves, "hands": nh}
+    # whole iterations against the bytes the reference's own data flow moves
+    # per iteration on this tree (formula in flow_bytes_per_iteration)
+    flow = flow_bytes_per_iteration(sg.td, mh)
+    t_iter = (total_ms_max / args.steps) / args.iterations / 1e3   # seconds, uninstrumented
+    flow_gbs = flow / t_iter / 1e9
+    roof_iter = {"bytes_per_iteration": flow, "iteration_ms": t_iter * 1e3, "achieved": flow_gbs, "peak": peak,
+                 "peak_source": peak_src, "unit": "GB/s", "frac": flow_gbs / peak,
+                 "basis": "reference data flow per iteration: regret matching of every decision node, "
+                          "reach of every non-traverser player, values, terminals (per traverser)"}
     lib.ss_session_destroy(sess)
     sg.free()
     return {
@@ -360,6 +405,7 @@ def run_ours(args, world, rank, local):
         "iteration_ms": prof.iteration_ms,
         "exploitability_pct": exploit,
         "tree": tree_info,
+        "roofline_iteration": roof_iter,
     }
 
 
@@ -592,7 +638,8 @@ def main():
                        "l2": WORKLOADS[args.workload][1],
                        "parallelism": f"replicas x{world}",
                        "p50_ms": t[len(t) // 2], "p99_ms": t[-1]},
-            "roofline": res["roofline"], "cpu_baseline": cpu, "clocks": res["clocks"],
+            "roofline": res["roofline"], "roofline_iteration": res["roofline_iteration"],
+            "cpu_baseline": cpu, "clocks": res["clocks"],
             "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
