@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="plain,batched,served",
                     help="comma list of plain (the headline), batched, served")
-    ap.add_argument("--batch-size", type=int, default=64)
+    ap.add_argument("--batch-size", type=int, default=512, help="batched form: mixed requests in one batch")
     ap.add_argument("--rate", type=float, default=100.0, help="served form: requests per second")
     ap.add_argument("--duration", type=float, default=3.0, help="served form: seconds of arrivals")
     return ap.parse_args()
