@@ -61,12 +61,14 @@ def test_batch_equals_alone():
 
 
 @pytest.mark.gpu
-def test_batch_merged_sweep_runs_agree_with_alone():
-    # three full-range 3-player rivers: 120 three-way showdown terminals per
-    # launch, so the batch merges the sweep's runs pairwise (a solo solve
-    # does not)
+@pytest.mark.parametrize("count", [3, 15])
+def test_batch_merged_sweep_runs_agree_with_alone(count):
+    # full-range 3-player rivers, 40 three-way showdowns per traverser each:
+    # 3 of them (120 per launch) make the batch merge the sweep's runs
+    # pairwise, 15 (600 per launch) give each block all 16 runs, a whole
+    # sweep without directly computed states (a solo solve merges nothing)
     subs = []
-    for seed in (71, 72, 73):
+    for seed in range(71, 71 + count):
         cfg = wl.config("river6", seed=seed, num_players=3)
         cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(seed), cfg["board"], 3, None)
         subs.append(wl.AbiSubgame(cfg, max_hands=1326))
