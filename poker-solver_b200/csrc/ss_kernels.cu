@@ -1402,6 +1402,24 @@ template <class T>
 __device__ __forceinline__ void sd2_direct_state(Sd2State st, T *M1, T *M2, const T *R1, const T *R2,
                                                  const unsigned short *dd, int qend) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (qend == 0) {
+        // no hands: every aggregate is zero (the same for every thread of the
+        // block, so the early return passes no barrier unevenly)
+        for (int i = tid; i < SD2_S * SD2_S; i += kTermThreads) {
+            M1[i] = T(0);
+            M2[i] = T(0);
+            st.P[i] = 0.0;
+        }
+        if (tid < 64) {
+            st.u1[tid] = 0.0;
+            st.u2[tid] = 0.0;
+            st.w[tid] = 0.0;
+            st.d[tid] = 0.0;
+        }
+        if (tid < 8) st.sc[tid] = 0.0;
+        __syncthreads();
+        return;
+    }
     for (int i = tid; i < SD2_S * SD2_S; i += kTermThreads) {
         M1[i] = T(0);
         M2[i] = T(0);
