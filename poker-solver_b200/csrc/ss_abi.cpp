@@ -153,7 +153,7 @@ void ss_free_output(SSOutput *out) {
     if (!out) return;
     std::free(out->root_strategy);
     std::free(out->root_ev);
-    std::free(out->avg_strategies);
+    if (!ssb::host_block_give(out->avg_strategies)) std::free(out->avg_strategies);
     std::free(out->avg_strategy_node_ids);
     std::memset(out, 0, sizeof(SSOutput));
 }

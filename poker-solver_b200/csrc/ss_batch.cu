@@ -351,7 +351,7 @@ int batch_solve(const std::vector<Problem> &pbs, int max_iterations, const Solve
             for (size_t j = 0; j < i; ++j) {
                 std::free(outs[j].root_strategy);
                 std::free(outs[j].root_ev);
-                std::free(outs[j].avg_strategies);
+                if (!host_block_give(outs[j].avg_strategies)) std::free(outs[j].avg_strategies);
                 std::free(outs[j].avg_strategy_node_ids);
                 std::memset(&outs[j], 0, sizeof(SSOutput));
             }
@@ -443,7 +443,7 @@ class Server {
             SSOutput &o = kv.second->out;
             std::free(o.root_strategy);
             std::free(o.root_ev);
-            std::free(o.avg_strategies);
+            if (!host_block_give(o.avg_strategies)) std::free(o.avg_strategies);
             std::free(o.avg_strategy_node_ids);
         }
     }
@@ -514,7 +514,7 @@ class Server {
         } else {
             std::free(r->out.root_strategy);
             std::free(r->out.root_ev);
-            std::free(r->out.avg_strategies);
+            if (!host_block_give(r->out.avg_strategies)) std::free(r->out.avg_strategies);
             std::free(r->out.avg_strategy_node_ids);
         }
         std::memset(&r->out, 0, sizeof(SSOutput));

@@ -68,6 +68,85 @@ const char *kClassName[SS_PROFILE_CLASSES] = {"reach", "cfv", "term_fill", "term
 void set_error(const std::string &msg) { g_err = msg; }
 const char *last_error() { return g_err.c_str(); }
 
+// Average strategies are the one large output (200 MB for a full-range
+// 3-player turn).  Written into a freshly allocated buffer, the copy first
+// faults in every page and stages through pageable memory; instead the
+// buffer comes from a pool of page-locked blocks that ss_free_output hands
+// back, so a later solve of similar size copies straight into mapped,
+// locked pages.  The pool is never destroyed (it would outlive the CUDA
+// runtime at exit); at most kPoolIdleBytes wait idle.
+namespace {
+constexpr size_t kPoolIdleBytes = size_t(2) << 30;
+constexpr size_t kPoolGrain = size_t(2) << 20;
+
+struct HostPool {
+    struct Block {
+        size_t bytes;
+        bool locked;
+    };
+    std::mutex mu;
+    std::vector<std::pair<void *, Block>> out, idle;
+    size_t idle_bytes = 0;
+
+    static void release(void *p, const Block &b) {
+        if (b.locked) cudaHostUnregister(p);
+        std::free(p);
+    }
+};
+HostPool &host_pool() {
+    static HostPool *pool = new HostPool;
+    return *pool;
+}
+}  // namespace
+
+void *host_block_take(size_t bytes) {
+    HostPool &hp = host_pool();
+    const size_t cap = (std::max<size_t>(bytes, 1) + kPoolGrain - 1) / kPoolGrain * kPoolGrain;
+    {
+        std::lock_guard<std::mutex> lk(hp.mu);
+        // the smallest idle block that fits and wastes at most half of itself
+        size_t best = hp.idle.size();
+        for (size_t i = 0; i < hp.idle.size(); ++i) {
+            const size_t b = hp.idle[i].second.bytes;
+            if (b >= cap && b <= 2 * cap && (best == hp.idle.size() || b < hp.idle[best].second.bytes)) best = i;
+        }
+        if (best < hp.idle.size()) {
+            auto blk = hp.idle[best];
+            hp.idle.erase(hp.idle.begin() + static_cast<std::ptrdiff_t>(best));
+            hp.idle_bytes -= blk.second.bytes;
+            hp.out.push_back(blk);
+            return blk.first;
+        }
+    }
+    void *p = std::aligned_alloc(4096, cap);
+    if (!p) return nullptr;
+    const bool locked = cudaHostRegister(p, cap, cudaHostRegisterPortable) == cudaSuccess;
+    if (!locked) cudaGetLastError();   // stays pageable; clear the error
+    std::lock_guard<std::mutex> lk(hp.mu);
+    hp.out.push_back({p, HostPool::Block{cap, locked}});
+    return p;
+}
+
+bool host_block_give(void *p) {
+    if (!p) return false;
+    HostPool &hp = host_pool();
+    std::pair<void *, HostPool::Block> blk{nullptr, {0, false}};
+    {
+        std::lock_guard<std::mutex> lk(hp.mu);
+        auto it = std::find_if(hp.out.begin(), hp.out.end(), [p](const auto &e) { return e.first == p; });
+        if (it == hp.out.end()) return false;
+        blk = *it;
+        hp.out.erase(it);
+        if (hp.idle_bytes + blk.second.bytes <= kPoolIdleBytes) {
+            hp.idle.push_back(blk);
+            hp.idle_bytes += blk.second.bytes;
+            return true;
+        }
+    }
+    HostPool::release(blk.first, blk.second);
+    return true;
+}
+
 #define CK(call)                                                                      \
     do {                                                                              \
         cudaError_t e_ = (call);                                                      \
@@ -293,12 +372,12 @@ int Session::output(SSOutput *out) {
         e = launch_avg_strategy(c, dec_fe, dec_na, dec_pl, P.num_dec, P.max_h, davg, stream);
     float *h_rs = static_cast<float *>(std::calloc(std::max<size_t>(n_rs, 1), sizeof(float)));
     float *h_rev = static_cast<float *>(std::calloc(static_cast<size_t>(np) * P.max_h, sizeof(float)));
-    float *h_avg = static_cast<float *>(std::malloc(std::max<size_t>(n_avg, 1) * sizeof(float)));
+    float *h_avg = static_cast<float *>(host_block_take(std::max<size_t>(n_avg, 1) * sizeof(float)));
     int *h_ids = static_cast<int *>(std::malloc(std::max<size_t>(P.num_dec, 1) * sizeof(int)));
     if (!h_rs || !h_rev || !h_avg || !h_ids) {
         std::free(h_rs);
         std::free(h_rev);
-        std::free(h_avg);
+        host_block_give(h_avg);
         std::free(h_ids);
         cudaFreeAsync(davg, stream);
         set_error("host allocation of the outputs failed");
@@ -316,7 +395,7 @@ int Session::output(SSOutput *out) {
     if (e != cudaSuccess) {
         std::free(h_rs);
         std::free(h_rev);
-        std::free(h_avg);
+        host_block_give(h_avg);
         std::free(h_ids);
         set_error(std::string("CUDA: ") + cudaGetErrorString(e));
         return SS_ERR_CUDA;

@@ -22,6 +22,17 @@ void set_error(const std::string &msg);
 const char *last_error();
 
 // ---------------------------------------------------------------------------
+// host blocks for the largest output array (ss_engine.cu)
+// ---------------------------------------------------------------------------
+// host_block_take: a block of at least `bytes`, page-locked where the host
+// allows it, reused from earlier outputs when one is idle; nullptr when host
+// memory is exhausted.  host_block_give: returns a block from host_block_take
+// to the pool (or releases it past the pool's cap) and reports true; false
+// for any other pointer, which the caller then frees itself.
+void *host_block_take(size_t bytes);
+bool host_block_give(void *p);
+
+// ---------------------------------------------------------------------------
 // tree builder (ss_tree.cpp)
 // ---------------------------------------------------------------------------
 struct BuiltTree {
