@@ -238,3 +238,57 @@ def test_wrapper_trims_ranges_to_the_build_width():
                             pot_bb=5, stack_bb=20, bet_sizes=[1.0], max_hands=1326)
     assert len(w.player_hands[0]) > 200
     w.free()
+
+
+def test_wrapper_strategy_readout_on_a_given_output():
+    # the reader of the reference module (street_solver_gpu.py:375-548) over
+    # a synthetic output block: root strategy, the walk along action labels,
+    # the per-hand average strategy map and the 0.001 cut
+    s = ssg.StreetSolverGPU(board=["Qs", "As", "2d", "7h", "4c"], oop_range="AhKh,QhQc,JhTh",
+                            ip_range="AcKc,8c8d", pot_bb=10.0, stack_bb=50.0, bet_sizes=[0.75])
+    t = s._tree
+    nd = t.num_decision_nodes
+    ids = np.array([t.decision_node_indices[i] for i in range(nd)], np.int32)
+    mh = s._max_hands
+    avg = np.zeros((nd, 8, mh), np.float32)
+    for di, nidx in enumerate(ids):
+        na = t.nodes[int(nidx)].num_children
+        for a in range(na):
+            avg[di, a, :] = (a + 1) / (na * (na + 1) / 2)
+    avg[0, 0, 1] = 0.0005                       # below the reader's cut
+    nh0 = len(s.player_hands[0])
+    na0 = t.nodes[0].num_children
+    rs = np.full((na0, nh0), 1.0 / na0, np.float32)
+    rev = np.zeros(mh, np.float32)
+    keep = (avg, ids, rs, rev)
+    o = ssg.SSOutput()
+    o.root_strategy = rs.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    o.root_num_actions = na0
+    o.root_player = 0
+    o.root_ev = rev.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    o.avg_strategies = avg.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    o.avg_strategy_node_ids = ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    o.num_avg_nodes = nd
+    o.num_players_out = 2
+    o.max_hands = mh
+    s._output, s._solved = o, True
+    try:
+        labels0 = ssg._build_labels_at_node(t, 0)
+        root = s.get_strategy(0, hand_idx=0)
+        assert set(root) == set(labels0) and abs(sum(root.values()) - 1.0) < 1e-6
+        # player 1 after "Check": the row of the child node
+        child = t.children[t.nodes[0].first_child + labels0.index("Check")]
+        di = int(np.nonzero(ids == child)[0][0])
+        got = s.get_strategy(1, hand_idx=1, frozen_actions=["check"])
+        labels1 = ssg._build_labels_at_node(t, child)
+        assert got == {labels1[a]: float(avg[di, a, 1]) for a in range(len(labels1))}
+        # player 0's first decision row, hand 1: the action under the cut is left out
+        amap = s.get_avg_strategy(0)
+        c0, c1, _ = s.player_hands[0][1]
+        row = amap[(min(c0, c1), max(c0, c1))]
+        assert labels0[0] not in row and set(row) == set(labels0[1:])
+        assert s.get_avg_strategy_probs(0, labels0[0])[(min(c0, c1), max(c0, c1))] == 0.0
+    finally:
+        s._output, s._solved = ssg.SSOutput(), False   # synthetic buffers are not the library's
+        del keep
+        s.free()
