@@ -1,10 +1,14 @@
-"""Host-side check of the planner's three-way showdown sweep tables
-(ss_plan.cpp): the per-player segments tile the rank axis, a segment holding
-the player's hands is one tie group, the runs cover the segments in order
-with about equal cost and at most one wave of blocks per traverser, and the
-planned spans bound every run (and every merged group of runs) that a
-kernel block carves class storage for.  The planner and tree builder are
-compiled with g++ into a small driver (tests/native/plan_runs.cpp)."""
+"""Host-side checks of the planner (ss_plan.cpp), compiled with g++ with the
+tree builder into small drivers (tests/native/):
+* plan_runs: the three-way showdown sweep tables -- the per-player segments
+  tile the rank axis, a segment holding the player's hands is one tie group,
+  the runs cover the segments in order with about equal cost and at most one
+  wave of blocks per traverser, and the planned spans bound every run (and
+  every merged group of runs) that a kernel block carves class storage for;
+* plan_kinds: the terminal routing -- each terminal goes to the closed form
+  for its number of counted opponents (folds count every other player,
+  showdowns and leaves the live ones), the scatter form for ranges that
+  repeat a combo, and exact enumeration for the rest."""
 import json
 import os
 import shutil
@@ -18,15 +22,24 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "poker-solver_b200", "csrc")
 
 
-@pytest.fixture(scope="module")
-def driver(tmp_path_factory):
+def _compile(tmp_path_factory, name):
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    out = str(tmp_path_factory.mktemp("plan") / "plan_runs")
+    out = str(tmp_path_factory.mktemp("plan") / name)
     subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-                    os.path.join(ROOT, "tests", "native", "plan_runs.cpp"), os.path.join(CSRC, "ss_plan.cpp"),
+                    os.path.join(ROOT, "tests", "native", name + ".cpp"), os.path.join(CSRC, "ss_plan.cpp"),
                     os.path.join(CSRC, "ss_tree.cpp"), "-o", out], check=True)
     return out
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    return _compile(tmp_path_factory, "plan_runs")
+
+
+@pytest.fixture(scope="module")
+def kinds_driver(tmp_path_factory):
+    return _compile(tmp_path_factory, "plan_kinds")
 
 
 def plan(driver, seed, hands, board):
@@ -92,3 +105,49 @@ def test_one_wave_cap(driver):
         assert p["sd2_terminals"] == 40
         used = sum(1 for k in range(d["chunks"]) if p["chunk"][k + 1] > p["chunk"][k])
         assert used == 14
+
+
+# TermKind values (ss_engine.h)
+ZERO, LEAF0, CR1, CR2, SD1, ENUM, SD2, CR1D = range(8)
+FOLD, SHOWDOWN, LEAF = 1, 2, 4
+
+
+def expected_kinds(d, np_, river, leaves):
+    """The routing rule restated: folds count every other player, showdowns
+    (river, traverser live) and leaves (with leaf values) the live others;
+    0 / 1 / 2 counted opponents take the closed forms, one opponent whose
+    range repeats a combo the scatter form, three-way showdowns with such a
+    range and anything with 3+ counted opponents exact enumeration."""
+    want = [[0] * 8 for _ in range(np_)]
+    dup = d["dup"]
+    for typ, leaf_idx, active in d["terminals"]:
+        for t in range(np_):
+            opp = [o for o in range(np_) if o != t and (typ == FOLD or active[o])]
+            k = len(opp)
+            kind = ZERO
+            if typ == FOLD or (typ == LEAF and leaves and leaf_idx >= 0):
+                kind = (LEAF0 if k == 0 else (CR1D if dup[opp[0]] else CR1) if k == 1
+                        else CR2 if k == 2 else ENUM)
+            elif typ == SHOWDOWN and river and active[t]:
+                kind = (SD1 if k == 1 else SD2 if k == 2 and not (dup[t] or dup[opp[0]] or dup[opp[1]])
+                        else ENUM)
+            want[t][kind] += 1
+    return want
+
+
+@pytest.mark.parametrize("np_,nb,nh,dup,leaves,raises", [
+    (2, 5, 30, -1, 0, 2),     # heads-up river
+    (2, 5, 30, 1, 0, 2),      # heads-up, opponent 1 repeats a combo: its folds take the scatter form
+    (3, 5, 20, -1, 0, 2),     # three-way showdowns, two-opponent folds
+    (3, 5, 20, 1, 0, 1),      # a repeated combo: scatter form, enumerated three-way showdowns
+    (4, 5, 8, -1, 0, 1),      # three counted opponents at folds: enumeration
+    (3, 4, 12, -1, 1, 1),     # turn with continuation leaves
+    (3, 4, 12, -1, 0, 1),     # the same without leaf values: leaves are zero
+])
+def test_terminal_routing(kinds_driver, np_, nb, nh, dup, leaves, raises):
+    r = subprocess.run([kinds_driver, str(np_), str(nb), str(nh), str(dup), str(leaves), str(raises)],
+                       check=True, capture_output=True, text=True)
+    d = json.loads(r.stdout)
+    assert d["rc"] == 0
+    assert d["dup"] == [1 if p == dup else 0 for p in range(np_)]
+    assert d["kinds"] == expected_kinds(d, np_, nb == 5, leaves)
