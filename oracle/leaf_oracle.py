@@ -1,0 +1,147 @@
+"""Test infrastructure: a restatement of the reference's turn leaf-value
+producer (python/leaf_values.py), the input a depth-limited turn subgame
+takes for its continuation leaves.  Only tests/ use it, as the checker of a
+future device producer; tests/golden/make_leaf_golden.py pins it against the
+reference module itself (leaf_values_*.npz).
+
+Per turn leaf (one per betting-tree leaf, before the continuation
+expansion) and each of the 4^N continuation bias profiles:
+  value(p, h) = first-order bias adjustment of hand h's river equity at the
+                leaf's pot,
+where the equity is averaged over river cards (all of them, or 12 drawn with
+numpy's RandomState(42) when some range holds more than 50 hands) of the
+unweighted share of opponent hand tuples the hand beats (ties split), with
+the tuples enumerated when there are at most 2000 of them and otherwise 2000
+drawn with Python's random.Random(42), as the reference does.  Hand
+strengths come from the oracle's evaluator (pinned to src/hand_eval.h); the
+golden script checks that it orders hands as the reference module's own
+evaluator does."""
+import itertools
+import random
+
+import numpy as np
+
+from oracle.oracle import Oracle
+
+# per bias profile (0 unmodified, 1 fold, 2 call, 3 raise):
+# leaf_values.py:86, :89
+FOLD_PROB = (0.0, 0.35, 0.0, 0.0)
+POT_FACTOR = (1.0, 0.7, 1.0, 1.4)
+RIVER_SAMPLES = 12        # leaf_values.py:762
+RANGE_SAMPLE_ABOVE = 50   # :763
+TUPLE_LIMIT = 2000        # :617
+
+
+def biased_value(equity, pot, s_self, s_opp):
+    """leaf_values.py:91-121: with the opponent's fold probability the hand
+    collects half the pot; otherwise (equity - 1/2) of the pot scaled by both
+    profiles' pot factors."""
+    fold = FOLD_PROB[s_opp]
+    showdown = pot * (POT_FACTOR[s_self] * POT_FACTOR[s_opp])
+    return fold * (0.5 * pot) + (1.0 - fold) * ((equity - 0.5) * showdown)
+
+
+def leaf_infos(td, num_players):
+    """leaf_values.py:189-262: (leaf index before the expansion, pot, bets)
+    of every continuation chain -- N nested levels of 4-way decisions, the
+    first owned by player 0, ending in leaves."""
+    nodes, children = td.nodes, td.children
+
+    def chain(x, depth):
+        n = nodes[x]
+        if n.type != 0 or n.num_children != 4:
+            return False
+        kids = [children[n.first_child + c] for c in range(4)]
+        if depth == num_players - 1:
+            return all(nodes[k].type == 4 for k in kids)
+        return all(chain(k, depth + 1) for k in kids)
+
+    per = 4 ** num_players
+    out = []
+    for x in range(td.num_nodes):
+        n = nodes[x]
+        if n.type != 0 or n.player != 0 or n.num_children != 4 or not chain(x, 0):
+            continue
+        y = x
+        for _ in range(num_players):
+            y = children[nodes[y].first_child]
+        out.append((nodes[y].leaf_idx // per, n.pot, tuple(n.bets[p] for p in range(num_players))))
+    return sorted(out, key=lambda t: t[0])
+
+
+def _equity_one_runout(hero, hands, strength, raw, cnt):
+    """leaf_values.py:573-691 for one river card: hero's share of the
+    opponent tuples it beats, over tuples with no shared card."""
+    mine = strength[hero]
+    if not mine:
+        return
+    opps = [q for q in range(len(hands)) if q != hero]
+    lists = [list(strength[q].keys()) for q in opps]
+    total = 1
+    for lst in lists:
+        total *= len(lst)
+    if total == 0:
+        return
+    if total <= TUPLE_LIMIT:
+        tuples = list(itertools.product(*lists))
+    else:
+        rng = random.Random(42)
+        tuples = [tuple(rng.choice(lst) for lst in lists) for _ in range(TUPLE_LIMIT)]
+    for h, s in mine.items():
+        c0, c1 = hands[hero][h][0], hands[hero][h][1]
+        won, n = 0.0, 0
+        for tup in tuples:
+            cards = [c for q, o in zip(opps, tup) for c in hands[q][o][:2]]
+            if c0 in cards or c1 in cards or len(set(cards)) < len(cards):
+                continue
+            best = max(strength[q][o] for q, o in zip(opps, tup))
+            n += 1
+            if s > best:
+                won += 1.0
+            elif s == best:
+                won += 1.0 / (1 + sum(1 for q, o in zip(opps, tup) if strength[q][o] == s))
+        if n > 0:
+            raw[hero, h] += won / n
+            cnt[hero, h] += 1.0
+
+
+def turn_leaf_values(board4, infos, max_hands, player_hands, oracle=None):
+    """leaf_values.py:694-816: float32 [len(infos) * 4^N, N, max_hands];
+    player_hands[p] = [(card, card, weight), ...]."""
+    orc = oracle or Oracle()
+    N = len(player_hands)
+    per = 4 ** N
+    total = len(infos) * per
+    out = np.zeros((total, N, max_hands), dtype=np.float32)
+    on_board = set(board4)
+    rivers = [c for c in range(52) if c not in on_board]
+    nh = [len(h) for h in player_hands]
+    if len(rivers) > RIVER_SAMPLES and any(n > RANGE_SAMPLE_ABOVE for n in nh):
+        rivers = sorted(np.random.RandomState(42).choice(rivers, RIVER_SAMPLES, replace=False))
+    raw = np.zeros((N, max_hands), dtype=np.float64)
+    cnt = np.zeros((N, max_hands), dtype=np.float64)
+    for r in rivers:
+        b5 = list(board4) + [int(r)]
+        dead = set(b5)
+        strength = []
+        for p in range(N):
+            strength.append({h: orc.eval7(b5 + [c0, c1]) for h, (c0, c1, _w) in enumerate(player_hands[p])
+                             if c0 not in dead and c1 not in dead})
+        for p in range(N):
+            _equity_one_runout(p, player_hands, strength, raw, cnt)
+    ok = cnt > 0
+    raw[ok] /= cnt[ok]
+    for leaf, pot, _bets in infos:
+        for combo in range(per):
+            flat = leaf * per + combo
+            if flat >= total:
+                continue
+            prof = [(combo // 4 ** i) % 4 for i in range(N)]
+            for p in range(N):
+                if N > 2:
+                    s_opp = max(0, min(3, int(round(sum(prof[q] for q in range(N) if q != p) / (N - 1)))))
+                else:
+                    s_opp = prof[1 - p]
+                for h in range(min(nh[p], max_hands)):
+                    out[flat, p, h] = biased_value(raw[p, h], pot, prof[p], s_opp)
+    return out
