@@ -1,6 +1,6 @@
-"""Test infrastructure: a restatement of the reference's turn leaf-value
-producer (python/leaf_values.py), the input a depth-limited turn subgame
-takes for its continuation leaves.  Only tests/ use it, as the checker of a
+"""Test infrastructure: a restatement of the reference's turn and flop
+leaf-value producers (python/leaf_values.py), the input a depth-limited turn
+or flop subgame takes for its continuation leaves.  Only tests/ use it, as the checker of a
 future device producer; tests/golden/make_leaf_golden.py pins it against the
 reference module itself (leaf_values_*.npz).
 
@@ -8,8 +8,9 @@ Per turn leaf (one per betting-tree leaf, before the continuation
 expansion) and each of the 4^N continuation bias profiles:
   value(p, h) = first-order bias adjustment of hand h's river equity at the
                 leaf's pot,
-where the equity is averaged over river cards (all of them, or 12 drawn with
-numpy's RandomState(42) when some range holds more than 50 hands) of the
+where the equity is averaged over the runouts -- river cards of a turn (all
+of them, or 12 drawn with numpy's RandomState(42) when some range holds
+more than 50 hands), turn and river cards of a flop (likewise sampled) -- of the
 unweighted share of opponent hand tuples the hand beats (ties split), with
 the tuples enumerated when there are at most 2000 of them and otherwise 2000
 drawn with Python's random.Random(42), as the reference does.  Hand
@@ -105,23 +106,55 @@ def _equity_one_runout(hero, hands, strength, raw, cnt):
             cnt[hero, h] += 1.0
 
 
+def turn_runouts(board4, player_hands):
+    """River cards of a turn (leaf_values.py:754-770)."""
+    on_board = set(board4)
+    rivers = [c for c in range(52) if c not in on_board]
+    if len(rivers) > RIVER_SAMPLES and any(len(h) > RANGE_SAMPLE_ABOVE for h in player_hands):
+        rivers = sorted(np.random.RandomState(42).choice(rivers, RIVER_SAMPLES, replace=False))
+    return [[int(r)] for r in rivers]
+
+
+def flop_runouts(board3, player_hands):
+    """Turn and river cards of a flop (leaf_values.py:479-499): 12 turn cards
+    drawn with RandomState(42) and, per turn card tc, 12 river cards drawn
+    with RandomState(43 + tc), when some range holds more than 50 hands."""
+    on_board = set(board3)
+    large = any(len(h) > RANGE_SAMPLE_ABOVE for h in player_hands)
+    turns = [c for c in range(52) if c not in on_board]
+    if len(turns) > RIVER_SAMPLES and large:
+        turns = sorted(np.random.RandomState(42).choice(turns, RIVER_SAMPLES, replace=False))
+    out = []
+    for tc in turns:
+        rivers = [c for c in range(52) if c not in on_board and c != tc]
+        if len(rivers) > RIVER_SAMPLES and large:
+            rivers = sorted(np.random.RandomState(43 + int(tc)).choice(rivers, RIVER_SAMPLES, replace=False))
+        out.extend([int(tc), int(rc)] for rc in rivers)
+    return out
+
+
 def turn_leaf_values(board4, infos, max_hands, player_hands, oracle=None):
     """leaf_values.py:694-816: float32 [len(infos) * 4^N, N, max_hands];
     player_hands[p] = [(card, card, weight), ...]."""
+    return _leaf_values(board4, turn_runouts(board4, player_hands), infos, max_hands, player_hands, oracle)
+
+
+def flop_leaf_values(board3, infos, max_hands, player_hands, oracle=None):
+    """leaf_values.py:408-571: the same over turn and river cards."""
+    return _leaf_values(board3, flop_runouts(board3, player_hands), infos, max_hands, player_hands, oracle)
+
+
+def _leaf_values(board, runouts, infos, max_hands, player_hands, oracle):
     orc = oracle or Oracle()
     N = len(player_hands)
     per = 4 ** N
     total = len(infos) * per
     out = np.zeros((total, N, max_hands), dtype=np.float32)
-    on_board = set(board4)
-    rivers = [c for c in range(52) if c not in on_board]
     nh = [len(h) for h in player_hands]
-    if len(rivers) > RIVER_SAMPLES and any(n > RANGE_SAMPLE_ABOVE for n in nh):
-        rivers = sorted(np.random.RandomState(42).choice(rivers, RIVER_SAMPLES, replace=False))
     raw = np.zeros((N, max_hands), dtype=np.float64)
     cnt = np.zeros((N, max_hands), dtype=np.float64)
-    for r in rivers:
-        b5 = list(board4) + [int(r)]
+    for extra in runouts:
+        b5 = list(board) + extra
         dead = set(b5)
         strength = []
         for p in range(N):

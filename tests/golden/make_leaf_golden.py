@@ -1,8 +1,9 @@
 """Generate the leaf-value golden fixtures (tests/golden/leaf_values_*.npz)
-from the reference's own producer, python/leaf_values.py
-(compute_turn_leaf_values and extract_leaf_info_from_tree), imported from
-the reference sources, on seeded turn subgames whose trees come from this
-library's ss_build_tree.  Each fixture stores the subgame (board, pot,
+from the reference's own producers, python/leaf_values.py
+(compute_turn_leaf_values, compute_flop_leaf_equity and
+extract_leaf_info_from_tree), imported from the reference sources, on
+seeded turn and flop subgames whose trees come from this library's
+ss_build_tree.  Each fixture stores the subgame (board, pot,
 stack, bet sizes, raise cap, ranges), the reference's leaf descriptors and
 its leaf values.  The script also checks that the reference module's own
 7-card evaluator orders hands as the oracle's evaluator (pinned to
@@ -26,12 +27,14 @@ from oracle.oracle import Oracle  # noqa: E402
 
 REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT", "/root/reference")
 
-# name, seed, players, hands per player, bet sizes, raise cap
+# name, seed, board cards, players, hands per player, bet sizes, raise cap
 CASES = [
-    ("hu_small", 201, 2, 30, [1.0], 1),        # every river card, every opponent hand
-    ("hu_sampled", 202, 2, 60, [0.75], 1),     # 12 sampled river cards
-    ("three_small", 203, 3, 10, [1.0], 1),     # opponent pairs enumerated
-    ("three_sampled", 204, 3, 52, [1.0], 1),   # 2000 sampled opponent pairs, 12 rivers
+    ("hu_small", 201, 4, 2, 30, [1.0], 1),        # every river card, every opponent hand
+    ("hu_sampled", 202, 4, 2, 60, [0.75], 1),     # 12 sampled river cards
+    ("three_small", 203, 4, 3, 10, [1.0], 1),     # opponent pairs enumerated
+    ("three_sampled", 204, 4, 3, 52, [1.0], 1),   # 2000 sampled opponent pairs, 12 rivers
+    ("flop_hu_small", 205, 3, 2, 16, [1.0], 1),   # every turn and river card
+    ("flop_hu_sampled", 206, 3, 2, 56, [1.0], 1), # 12 x 12 sampled runouts
 ]
 
 
@@ -57,9 +60,9 @@ def main():
     ref = load_reference()
     orc = Oracle()
     check_evaluators(ref, orc, np.random.default_rng(7))
-    for name, seed, np_, nh, sizes, raises in CASES:
+    for name, seed, nb, np_, nh, sizes, raises in CASES:
         rng = np.random.default_rng(seed)
-        board = [int(x) for x in rng.permutation(52)[:4]]
+        board = [int(x) for x in rng.permutation(52)[:nb]]
         hands, ws = wl.make_ranges(rng, board, np_, nh)
         cfg = dict(board=board, pot=120, stack=480, bet_sizes=sizes, max_raises=raises, num_players=np_,
                    hands=hands, weights=ws)
@@ -67,7 +70,8 @@ def main():
         infos = ref.extract_leaf_info_from_tree(sg.td, np_)
         ph = [[(int(h[0]), int(h[1]), float(w)) for h, w in zip(hands[p], ws[p])] for p in range(np_)]
         mh = max(len(h) for h in hands)
-        lv = ref.compute_turn_leaf_values(board, infos, mh, 120, player_hands=ph)
+        produce = ref.compute_turn_leaf_values if nb == 4 else ref.compute_flop_leaf_equity
+        lv = produce(board, infos, mh, 120, player_hands=ph)
         np.savez_compressed(
             os.path.join(HERE, f"leaf_values_{name}.npz"),
             board=np.array(board, np.int32), pot=120, stack=480, bet_sizes=np.array(sizes, np.float32),

@@ -1,9 +1,10 @@
-"""The oracle's restatement of the reference's turn leaf-value producer
-(oracle/leaf_oracle.py) against golden vectors made by the reference module
-itself (tests/golden/make_leaf_golden.py): leaf descriptors read from this
-library's trees and the leaf values, bit for bit, on heads-up and 3-player
-turns with every river card and every opponent tuple, and with the
-reference's sampled river cards and sampled opponent pairs."""
+"""The oracle's restatement of the reference's turn and flop leaf-value
+producers (oracle/leaf_oracle.py) against golden vectors made by the
+reference module itself (tests/golden/make_leaf_golden.py): leaf descriptors
+read from this library's trees and the leaf values, bit for bit, on
+heads-up and 3-player turns and heads-up flops, with every runout and every
+opponent tuple, and with the reference's sampled runouts and sampled
+opponent pairs."""
 import glob
 import os
 
@@ -33,10 +34,11 @@ def test_leaf_values_match_reference(path):
     assert [i[1] for i in infos] == g["leaf_pot"].tolist()
     assert [list(i[2]) for i in infos] == g["leaf_bets"].tolist()
     ph = [[(int(h[0]), int(h[1]), float(w)) for h, w in zip(hands[p], ws[p])] for p in range(np_)]
-    got = leaf_oracle.turn_leaf_values(board, infos, int(g["max_hands"]), ph)
+    produce = leaf_oracle.turn_leaf_values if len(board) == 4 else leaf_oracle.flop_leaf_values
+    got = produce(board, infos, int(g["max_hands"]), ph)
     assert got.shape == g["leaf_values"].shape
     assert np.array_equal(got, g["leaf_values"])
 
 
 def test_fixtures_present():
-    assert len(FIXTURES) >= 4
+    assert len(FIXTURES) >= 6
