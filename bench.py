@@ -64,8 +64,9 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS),
                     help="subgame of the plain form (the CPU baseline and reference arm cover turn3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="plain,batched,served",
-                    help="comma list of plain (the headline), batched, served")
+    ap.add_argument("--forms", default="plain,batched,served,leaf",
+                    help="comma list of plain (the headline), batched, served, leaf (the turn subgame's "
+                         "continuation values produced on the GPU)")
     ap.add_argument("--batch-size", type=int, default=512, help="batched form: mixed requests in one batch")
     ap.add_argument("--rate", type=float, default=100.0, help="served form: requests per second")
     ap.add_argument("--duration", type=float, default=3.0, help="served form: seconds of arrivals")
@@ -533,6 +534,62 @@ class _Quiet:
         os.close(self.null)
 
 
+def run_leaf_producer(seed, calls=3):
+    """Continuation values of the 3-player turn subgame (the input its
+    15,616 continuation leaves read) produced through the host module
+    leaf_values.compute_turn_leaf_values -> ss_leaf_values_gpu: host plan,
+    upload, kernels and the 126 MB of values copied back, wall clock per
+    call.  Beside it the oracle's loop form of the reference's Python
+    producer (python/leaf_values.py:694-816) on a bounded sample: 100 hero
+    hands of one (river card, player) pair and 100,000 bias-adjusted values,
+    scaled to 12 river cards x 3 players x 1128 hands and every value."""
+    import leaf_values as lv
+    import workloads as wl
+    from oracle import leaf_oracle
+    from oracle.oracle import Oracle
+    cfg = wl.config("turn3", seed=seed)
+    sg = wl.AbiSubgame(cfg)
+    try:
+        infos = lv.extract_leaf_info_from_tree(sg.td, cfg["num_players"])
+    finally:
+        sg.free()
+    N = cfg["num_players"]
+    ph = [[(int(h[0]), int(h[1]), float(w)) for h, w in zip(cfg["hands"][p], cfg["weights"][p])] for p in range(N)]
+    mh = max(len(h) for h in ph)
+    lv.compute_turn_leaf_values(cfg["board"], infos, mh, cfg["pot"], player_hands=ph)   # warm-up
+    times = []
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        out = lv.compute_turn_leaf_values(cfg["board"], infos, mh, cfg["pot"], player_hands=ph)
+        times.append((time.perf_counter() - t0) * 1e3)
+    runouts = lv.turn_runouts(cfg["board"], [len(h) for h in ph])
+    orc = Oracle()
+    b5 = list(cfg["board"]) + runouts[0]
+    strength = [{h: orc.eval7(b5 + [c0, c1]) for h, (c0, c1, _w) in enumerate(ph[p])
+                 if c0 not in b5 and c1 not in b5} for p in range(N)]
+    sample_hands = 100
+    strength[0] = dict(list(strength[0].items())[:sample_hands])
+    raw = np.zeros((N, mh))
+    cnt = np.zeros((N, mh))
+    t0 = time.perf_counter()
+    leaf_oracle._equity_one_runout(0, ph, strength, raw, cnt)
+    eq_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for k in range(100000):
+        leaf_oracle.biased_value(0.25, 300, k & 3, (k >> 2) & 3)
+    bias_s = time.perf_counter() - t0
+    cpu_ms = 1e3 * (eq_s * len(runouts) * N * mh / sample_hands + bias_s * out.size / 100000)
+    t = sorted(times)
+    return {"workload": f"3-player turn subgame leaf values: {len(infos)} leaf descriptors x 64 profiles x "
+                        f"{N} players x {mh} hands ({out.nbytes / 1e6:.0f} MB FP32), {len(runouts)} river cards, "
+                        f"2000 sampled opponent pairs per (river, player)",
+            "ms_per_call_e2e": t[len(t) // 2], "calls": calls, "d2h_bytes_per_call": int(out.nbytes),
+            "cpu_baseline": {"ms_per_call": cpu_ms, "cores": 1, "kind": "port",
+                             "sample": f"oracle loop form of python/leaf_values.py: {sample_hands} hero hands of "
+                                       f"one (river, player) pair ({eq_s:.2f} s) and 100,000 bias values "
+                                       f"({bias_s:.2f} s), scaled"}}
+
+
 def reference_cpu(seed, budget_s=25.0):
     """Seconds per CFR iteration of the reference kernels (host build) on the
     full turn3 tree, measured at small range sizes with every core running
@@ -626,6 +683,12 @@ def main():
         batched = run_batched(args.batch_size, args.seed, local)
     if rank == 0 and world == 1 and "served" in forms:
         served = run_served(args.rate, args.duration, args.seed, local)
+    leaf = None
+    if rank == 0 and world == 1 and "leaf" in forms and args.workload == "turn3":
+        try:
+            leaf = run_leaf_producer(args.seed)
+        except Exception as e:  # the solver's line is printed whatever happens here
+            leaf = {"error": f"{type(e).__name__}: {e}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "turn3":
         r = reference_cpu(args.seed, budget_s=20.0)
@@ -650,7 +713,7 @@ def main():
             "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
-            "batched": batched, "served": served,
+            "batched": batched, "served": served, "leaf_producer": leaf,
         }
         print(json.dumps(line))
     try:

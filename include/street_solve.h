@@ -340,6 +340,53 @@ int ss_server_wait(SSServer *server, long long request_id, SSOutput *output, SSS
 /* EXTENSION: stop the worker and release the server (unfetched results too). */
 void ss_server_destroy(SSServer *server);
 
+/* ── Continuation values of a depth-limited subgame on the GPU ───────────
+ *
+ * Replaces the reference's Python producers compute_turn_leaf_values
+ * (python/leaf_values.py:694-816) and compute_flop_leaf_equity
+ * (python/leaf_values.py:408-571), which hud_solver.py calls before
+ * ss_solve_gpu to fill SSTreeData.leaf_values.  Same result, bit for bit:
+ * per runout, each hand's share of the opponent hand tuples it beats (ties
+ * split 1/k), over tuples with no shared card, enumerated when there are at
+ * most SS_LEAF_TUPLE_LIMIT of them and otherwise SS_LEAF_TUPLE_LIMIT drawn
+ * with Python's random.Random(42) (python/leaf_values.py:573-691); averaged
+ * over the runouts in the order given; then the first-order bias adjustment
+ * at each leaf's pot for every one of the 4^N continuation profiles
+ * (python/leaf_values.py:91-121), in FP64, stored as FP32. */
+
+#define SS_LEAF_TUPLE_LIMIT 2000   /* python/leaf_values.py:615 */
+
+typedef struct {
+    int num_players;          /* 2 .. SS_MAX_PLAYERS */
+    int max_hands;            /* row length of the output; >= every num_hands[p], <= 1326 */
+    const int *num_hands;     /* [num_players] range sizes */
+    const int *hand_cards;    /* [num_players][max_hands][2] cards 0..51 (rank * 4 + suit) */
+    const int *board;         /* num_board cards: 3 (flop subgame) or 4 (turn subgame) */
+    int num_board;
+    const int *runout_cards;  /* [num_runouts][5 - num_board] cards completing the board, in averaging order */
+    int num_runouts;
+    const int *leaf_idx;      /* [num_leaves] LeafInfo.leaf_idx (index before the continuation expansion), >= 0 */
+    const double *leaf_pot;   /* [num_leaves] LeafInfo.pot */
+    int num_leaves;
+} SSLeafValueInput;
+
+/* EXTENSION (GPU form of python/leaf_values.py:694-816 and :408-571):
+ * leaf_values [num_leaves * 4^num_players][num_players][max_hands] FP32,
+ * laid out as the reference returns it and as SSTreeData.leaf_values reads
+ * it; row leaf_idx * 4^N + profile of every leaf descriptor is written (a
+ * later descriptor with the same leaf_idx wins, as in the reference loop),
+ * every other entry is 0.  Returns SS_OK or a negative SS_ERR_* code. */
+int ss_leaf_values_gpu(const SSLeafValueInput *input, float *leaf_values);
+
+/* EXTENSION (host only, no GPU): the reference's opponent-tuple rule
+ * (python/leaf_values.py:615-629) for opponents whose live-hand lists hold
+ * list_sizes[0..num_opponents-1] hands: every tuple in itertools.product
+ * order when their product is at most SS_LEAF_TUPLE_LIMIT, otherwise
+ * SS_LEAF_TUPLE_LIMIT tuples drawn by random.Random(42).choice per opponent.
+ * Writes positions into the lists, tuples[t * num_opponents + k], for at most
+ * max_tuples tuples; returns the tuple count or a negative SS_ERR_* code. */
+int ss_leaf_opponent_tuples(int num_opponents, const int *list_sizes, int *tuples, int max_tuples);
+
 /* EXTENSION: message for the last failure on the calling thread ("" if none). */
 const char *ss_last_error(void);
 

@@ -147,9 +147,6 @@ def flop_leaf_values(board3, infos, max_hands, player_hands, oracle=None):
 def _leaf_values(board, runouts, infos, max_hands, player_hands, oracle):
     orc = oracle or Oracle()
     N = len(player_hands)
-    per = 4 ** N
-    total = len(infos) * per
-    out = np.zeros((total, N, max_hands), dtype=np.float32)
     nh = [len(h) for h in player_hands]
     raw = np.zeros((N, max_hands), dtype=np.float64)
     cnt = np.zeros((N, max_hands), dtype=np.float64)
@@ -164,6 +161,15 @@ def _leaf_values(board, runouts, infos, max_hands, player_hands, oracle):
             _equity_one_runout(p, player_hands, strength, raw, cnt)
     ok = cnt > 0
     raw[ok] /= cnt[ok]
+    return _bias_rows(raw, infos, max_hands, nh)
+
+
+def _bias_rows(raw, infos, max_hands, nh):
+    """leaf_values.py:795-814: the rows of every leaf descriptor and profile."""
+    N = len(nh)
+    per = 4 ** N
+    total = len(infos) * per
+    out = np.zeros((total, N, max_hands), dtype=np.float32)
     for leaf, pot, _bets in infos:
         for combo in range(per):
             flat = leaf * per + combo
@@ -175,6 +181,75 @@ def _leaf_values(board, runouts, infos, max_hands, player_hands, oracle):
                     s_opp = max(0, min(3, int(round(sum(prof[q] for q in range(N) if q != p) / (N - 1)))))
                 else:
                     s_opp = prof[1 - p]
-                for h in range(min(nh[p], max_hands)):
-                    out[flat, p, h] = biased_value(raw[p, h], pot, prof[p], s_opp)
+                m = min(nh[p], max_hands)
+                # biased_value over the row: the same IEEE operations, element by element
+                out[flat, p, :m] = biased_value(raw[p, :m], pot, prof[p], s_opp)
     return out
+
+
+def _reference_tuples(lists):
+    """leaf_values.py:603-629: the opponent tuples scored on one runout."""
+    total = 1
+    for lst in lists:
+        total *= len(lst)
+    if total == 0:
+        return []
+    if total <= TUPLE_LIMIT:
+        return list(itertools.product(*lists))
+    rng = random.Random(42)
+    return [tuple(rng.choice(lst) for lst in lists) for _ in range(TUPLE_LIMIT)]
+
+
+def leaf_values_vectorised(board, runouts, infos, max_hands, player_hands, oracle=None):
+    """The same values as _leaf_values with numpy over (hero hand, tuple):
+    per runout and hero player, the tuples' card masks, best strengths and
+    tie counts, each hand's per-tuple credit (1, 1/k or 0), and the credits
+    summed with a running sum in tuple order (np.cumsum adds left to right,
+    like the reference's loop) -- fast enough for full-size ranges."""
+    orc = oracle or Oracle()
+    N = len(player_hands)
+    nh = [len(h) for h in player_hands]
+    raw = np.zeros((N, max_hands), dtype=np.float64)
+    cnt = np.zeros((N, max_hands), dtype=np.float64)
+    cards = [np.array([(int(h[0]), int(h[1])) for h in ph], dtype=np.int64).reshape(-1, 2) for ph in player_hands]
+    one = np.uint64(1)
+    bits = [(one << c[:, 0].astype(np.uint64)) | (one << c[:, 1].astype(np.uint64)) for c in cards]
+    for extra in runouts:
+        b5 = list(board) + list(extra)
+        dead = set(b5)
+        live = [np.array([h for h in range(nh[p]) if cards[p][h, 0] not in dead and cards[p][h, 1] not in dead],
+                         dtype=np.int64) for p in range(N)]
+        st = [np.zeros(nh[p], dtype=np.int64) for p in range(N)]
+        for p in range(N):
+            for h in live[p]:
+                st[p][h] = orc.eval7(b5 + [int(cards[p][h, 0]), int(cards[p][h, 1])])
+        for p in range(N):
+            if not len(live[p]):
+                continue
+            opps = [q for q in range(N) if q != p]
+            tup = _reference_tuples([live[q].tolist() for q in opps])
+            if not tup:
+                continue
+            tup = np.array(tup, dtype=np.int64)
+            mask = np.zeros(len(tup), dtype=np.uint64)
+            clash = np.zeros(len(tup), dtype=bool)
+            best = np.zeros(len(tup), dtype=np.int64)
+            for k, q in enumerate(opps):
+                b = bits[q][tup[:, k]]
+                clash |= (mask & b) != 0
+                mask |= b
+                best = np.maximum(best, st[q][tup[:, k]])
+            nbest = sum((st[q][tup[:, k]] == best).astype(np.int64) for k, q in enumerate(opps))
+            hero = live[p]
+            blocked = ((bits[p][hero][:, None] & mask[None, :]) != 0) | clash[None, :]
+            hs = st[p][hero][:, None]
+            credit = np.where(hs > best[None, :], 1.0, np.where(hs == best[None, :], 1.0 / (1.0 + nbest[None, :]), 0.0))
+            credit[blocked] = 0.0
+            valid = (~blocked).sum(axis=1)
+            wins = np.cumsum(credit, axis=1)[:, -1]
+            ok = valid > 0
+            raw[p, hero[ok]] += wins[ok] / valid[ok]
+            cnt[p, hero[ok]] += 1.0
+    ok = cnt > 0
+    raw[ok] /= cnt[ok]
+    return _bias_rows(raw, infos, max_hands, nh)

@@ -6,10 +6,13 @@
 #include "street_solve.h"
 
 #include "ss_engine.h"
+#include "ss_leaf.h"
 
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <string>
+#include <vector>
 
 namespace {
 
@@ -408,6 +411,42 @@ void ss_server_destroy(SSServer *s) {
     if (!s) return;
     ssb::server_destroy(s->impl);
     delete s;
+}
+
+int ss_leaf_values_gpu(const SSLeafValueInput *input, float *leaf_values) {
+    try {
+        return ssb::leaf::leaf_values_gpu(input, leaf_values);
+    } catch (const std::bad_alloc &) {
+        ssb::set_error("ss_leaf_values_gpu: host allocation failed");
+        return SS_ERR_NOMEM;
+    }
+}
+
+int ss_leaf_opponent_tuples(int num_opponents, const int *list_sizes, int *tuples, int max_tuples) {
+    if (num_opponents < 1 || num_opponents > SS_MAX_PLAYERS - 1 || !list_sizes || max_tuples < 0 ||
+        (max_tuples > 0 && !tuples)) {
+        ssb::set_error("ss_leaf_opponent_tuples: bad arguments");
+        return SS_ERR_INVALID;
+    }
+    for (int k = 0; k < num_opponents; ++k)
+        if (list_sizes[k] < 0 || list_sizes[k] > ssb::leaf::kMaxHands) {
+            ssb::set_error("ss_leaf_opponent_tuples: list sizes must be 0..1326");
+            return SS_ERR_INVALID;
+        }
+    try {
+        std::vector<int> pos;
+        const int n = ssb::leaf::opponent_tuples(num_opponents, list_sizes, &pos);
+        if (n > max_tuples) {
+            ssb::set_error("ss_leaf_opponent_tuples: " + std::to_string(n) + " tuples, room for " +
+                           std::to_string(max_tuples));
+            return SS_ERR_INVALID;
+        }
+        if (!pos.empty()) std::memcpy(tuples, pos.data(), pos.size() * sizeof(int));
+        return n;
+    } catch (const std::bad_alloc &) {
+        ssb::set_error("ss_leaf_opponent_tuples: host allocation failed");
+        return SS_ERR_NOMEM;
+    }
 }
 
 const char *ss_last_error(void) { return ssb::last_error(); }

@@ -30,7 +30,15 @@ def _have_gpu():
 HAVE_GPU = _have_gpu()
 
 
+# Files run after all others, in this order: the continuation-value
+# producer's GPU tests after the solver's (so that under -x a failure there
+# cannot keep the solver's tests from running), the no-allocation entry
+# point last.  The sort is stable: everything else keeps file order.
+_RUN_LATE = {"test_leaf_values_gpu.py": 1, "test_zz_no_alloc.py": 2}
+
+
 def pytest_collection_modifyitems(config, items):
+    items.sort(key=lambda it: _RUN_LATE.get(os.path.basename(str(it.fspath)), 0))
     if HAVE_GPU:
         return
     skip = pytest.mark.skip(reason="no CUDA device")

@@ -42,3 +42,17 @@ def test_leaf_values_match_reference(path):
 
 def test_fixtures_present():
     assert len(FIXTURES) >= 6
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[12:-4] for p in FIXTURES])
+def test_vectorised_form_matches_reference(path):
+    """The numpy form of the oracle (used at full size by the GPU tests)
+    against the same reference-generated fixtures, bit for bit."""
+    g = np.load(path)
+    np_ = int(g["num_players"])
+    board = [int(c) for c in g["board"]]
+    ph = [[(int(h[0]), int(h[1]), float(w)) for h, w in zip(g["hands"][p], g["weights"][p])] for p in range(np_)]
+    infos = [(int(i), int(pot), ()) for i, pot in zip(g["leaf_idx"], g["leaf_pot"])]
+    runouts = (leaf_oracle.turn_runouts if len(board) == 4 else leaf_oracle.flop_runouts)(board, ph)
+    got = leaf_oracle.leaf_values_vectorised(board, runouts, infos, int(g["max_hands"]), ph)
+    assert np.array_equal(got, g["leaf_values"])
