@@ -408,6 +408,8 @@ def run_ours(args, world, rank, local):
         "exploitability_pct": exploit,
         "tree": tree_info,
         "roofline_iteration": roof_iter,
+        # node-hand updates: nodes x sum of the players' hand counts, per iteration
+        "nhu_per_solve": float(nnodes) * sum(nh) * args.iterations,
     }
 
 
@@ -452,11 +454,16 @@ def run_batched(n, seed, device):
     its = [r["stats"]["iterations_run"] for r in res]
     expl = [r["stats"]["exploitability_pct"] for r in res]
     nodes = [sg.td.num_nodes for sg in subs]
+    per_it = [float(sg.td.num_nodes) * float(sum(sg.nh)) for sg in subs]   # node-hand updates per iteration
+    nhu_batch = sum(n * k for n, k in zip(per_it, its))
+    nhu_plain = sum(n * p["iterations_run"] for n, p in zip(per_it, plain))
     for sg in subs:
         sg.free()
     return {"subgames": n, "target_pct": TARGET, "check_every": CHECK,
             "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch,
             "speedup_vs_plain": t_plain / t_batch,
+            "plain_node_hand_updates_per_s": nhu_plain / t_plain,
+            "batched_node_hand_updates_per_s": nhu_batch / t_batch,
             "iterations_p50": pct(its, 50), "iterations_max": max(its),
             "exploitability_max_pct": max(expl),
             "plain_iterations_p50": pct([p["iterations_run"] for p in plain], 50),
@@ -491,13 +498,14 @@ def run_served(rate, duration, seed, device):
 
     th = threading.Thread(target=feeder)
     th.start()
-    lat, its = [], []
+    lat, its, nhu = [], [], []
     for i, sg in enumerate(subs):
         while ids[i] is None:
             time.sleep(0.0005)
         r = srv.wait(ids[i], sg.nh)
         lat.append(r["latency_ms"])
         its.append(r["stats"]["iterations_run"])
+        nhu.append(float(sg.td.num_nodes) * float(sum(sg.nh)) * r["stats"]["iterations_run"])
     th.join()
     wall = time.perf_counter() - t_start
     srv.close()
@@ -509,6 +517,7 @@ def run_served(rate, duration, seed, device):
     for sg in subs:
         sg.free()
     return {"rate_per_s": rate, "requests": n, "solves_per_s": n / wall,
+            "node_hand_updates_per_s": sum(nhu) / wall,
             "latency_p50_ms": pct(lat, 50), "latency_p99_ms": pct(lat, 99),
             "iterations_p50": pct(its, 50),
             "plain_service_p50_ms": pct(service, 50), "plain_service_p99_ms": pct(service, 99),
@@ -711,6 +720,7 @@ def main():
             "roofline": res["roofline"], "roofline_iteration": res["roofline_iteration"],
             "cpu_baseline": cpu, "clocks": res["clocks"],
             "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
+            "node_hand_updates_per_s": res["value"] * res["nhu_per_solve"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
             "batched": batched, "served": served, "leaf_producer": leaf,

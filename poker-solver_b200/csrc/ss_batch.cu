@@ -588,6 +588,7 @@ class Server {
                 batch.retire(static_cast<int>(i));
                 SSOutput o{};
                 if (rc == SS_OK) rc = batch.subs[i]->output(&o);
+                const double nhu = batch.subs[i]->P.node_hands * batch.iters_run[i];
                 batch.release(static_cast<int>(i));
                 std::lock_guard<std::mutex> lk(mu);
                 used -= r->bytes;
@@ -598,6 +599,7 @@ class Server {
                     r->stats.iterations_run = batch.iters_run[i];
                     r->stats.exploitability_pct = pct;
                     r->stats.nashconv = nash;
+                    r->stats.node_hand_updates = nhu;
                     r->t_done = std::chrono::steady_clock::now();
                     r->state = 2;
                 }
