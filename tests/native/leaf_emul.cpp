@@ -4,19 +4,24 @@
 // (ss_leaf_plan.cpp), for tests/test_leaf_producer.py.  This checks the
 // element arithmetic and indexing without a GPU; the GPU tests run the
 // kernels themselves.
-//   leaf_emul <input.txt> <output.f32>
+//   leaf_emul <input.txt> <output.f32> [rows per chunk]
+// With a chunk size the value phase runs chunk by chunk into a chunk-sized
+// buffer copied into place, as the device driver does with its 256 MiB
+// chunks.
 // input: np mh num_board nr num_leaves / nh[np] / hand cards [np*mh*2] /
 //        board[num_board] / runout cards [nr*(5-num_board)] / leaf_idx[num_leaves] / leaf_pot[num_leaves]
 // output: the float32 values [num_leaves*4^np][np][mh], raw bytes.
 #include "ss_leaf.cuh"
 #include "ss_leaf.h"
 
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
 int main(int argc, char **argv) {
-    if (argc != 3) return 2;
+    if (argc != 3 && argc != 4) return 2;
     FILE *f = std::fopen(argv[1], "r");
     if (!f) return 2;
     int np, mh, nb, nr, nl;
@@ -81,12 +86,19 @@ int main(int argc, char **argv) {
     c.digest = digest.data();
     c.ratio = ratio.data();
     c.equity = equity.data();
-    c.values = values.data();
     for (long i = 0; i < nsh; ++i) strength_at(i, c);
     for (long t = 0; t < static_cast<long>(P.num_tuples()); ++t) digest_at(t, c);
     for (long i = 0; i < nsh; ++i) ratio_at(i, c);
     for (long i = 0; i < per_row; ++i) equity_at(i, c);
-    for (long i = 0; i < static_cast<long>(values.size()); ++i) value_at(i, 0, c);
+    const long rows = static_cast<long>(P.num_rows());
+    const long chunk = argc == 4 ? std::max(1L, std::atol(argv[3])) : std::max(1L, rows);
+    std::vector<float> buf(static_cast<size_t>(chunk * per_row));
+    c.values = buf.data();
+    for (long row0 = 0; row0 < rows; row0 += chunk) {
+        const long n = std::min(chunk, rows - row0) * per_row;
+        for (long i = 0; i < n; ++i) value_at(i, row0, c);
+        std::copy(buf.begin(), buf.begin() + n, values.begin() + row0 * per_row);
+    }
 
     FILE *o = std::fopen(argv[2], "wb");
     if (!o) return 2;

@@ -102,7 +102,7 @@ def emul(tmp_path_factory):
     return out
 
 
-def emulate(driver, tmp_path, board, runouts, infos, max_hands, ph):
+def emulate(driver, tmp_path, board, runouts, infos, max_hands, ph, chunk_rows=None):
     N = len(ph)
     cards = np.zeros((N, max_hands, 2), np.int64)
     for p, hs in enumerate(ph):
@@ -115,7 +115,7 @@ def emulate(driver, tmp_path, board, runouts, infos, max_hands, ph):
              " ".join(str(int(i[0])) for i in infos), " ".join(repr(float(i[1])) for i in infos)]
     inp, outp = tmp_path / "in.txt", tmp_path / "out.f32"
     inp.write_text("\n".join(lines) + "\n")
-    subprocess.run([driver, str(inp), str(outp)], check=True)
+    subprocess.run([driver, str(inp), str(outp)] + ([str(chunk_rows)] if chunk_rows else []), check=True)
     return np.fromfile(outp, np.float32).reshape(len(infos) * 4 ** N, N, max_hands)
 
 
@@ -125,6 +125,9 @@ def test_element_functions_reproduce_reference_values(emul, tmp_path, path):
     got = emulate(emul, tmp_path, board, runouts_for(board, ph), infos, int(g["max_hands"]), ph)
     assert got.shape == g["leaf_values"].shape
     assert np.array_equal(got, g["leaf_values"])
+    # the value phase in chunks of 7 rows (a tail chunk, rows starting mid-leaf)
+    chunked = emulate(emul, tmp_path, board, runouts_for(board, ph), infos, int(g["max_hands"]), ph, chunk_rows=7)
+    assert np.array_equal(chunked, g["leaf_values"])
 
 
 def edge_cases():
