@@ -64,9 +64,10 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS),
                     help="subgame of the plain form (the CPU baseline and reference arm cover turn3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="plain,batched,served,leaf",
-                    help="comma list of plain (the headline), batched, served, leaf (the turn subgame's "
-                         "continuation values produced on the GPU)")
+    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf",
+                    help="comma list of plain (the headline), batched, served, hu_river (the heads-up river "
+                         "beside the reference's CPU solver), leaf (the turn subgame's continuation values "
+                         "produced on the GPU)")
     ap.add_argument("--batch-size", type=int, default=512, help="batched form: mixed requests in one batch")
     ap.add_argument("--rate", type=float, default=100.0, help="served form: requests per second")
     ap.add_argument("--duration", type=float, default=3.0, help="served form: seconds of arrivals")
@@ -599,6 +600,80 @@ def run_leaf_producer(seed, calls=3):
                                        f"({bias_s:.2f} s), scaled"}}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def run_hu_river(seed, device, solves=5, cpu_iterations=20):
+    """The heads-up river configuration, the reference's CPU-runnable case:
+    5-card board, both ranges all 1081 combos with U(0,1) weights, pot 100,
+    stacks 400, bets {0.5, 1.0 pot} + all-in, 2 raises, 1000 Linear-CFR
+    iterations.  GPU: ss_solve_gpu_ex from host buffers to host outputs, wall
+    clock per solve after one warm-up solve.  CPU: the reference's own CPU
+    solver src/solver.c (-O2 -fopenmp, single-threaded per solve), one solve
+    per host core at once (one OS thread each), timed on cpu_iterations
+    iterations and scaled to 1000; its rules differ from street_solve.cu's
+    (a timing baseline, not a parity target)."""
+    import workloads as wl
+    cfg = wl.config("hu_river", seed=seed)
+    iters = cfg["iterations"]
+    sg = wl.AbiSubgame(cfg)
+    try:
+        rc, _ = sg.solve(iters, device=device)
+        if rc != 0:
+            raise RuntimeError(f"ss_solve_gpu failed ({rc})")
+        times = []
+        for _ in range(solves):
+            t0 = time.perf_counter()
+            rc, _ = sg.solve(iters, device=device)
+            times.append(time.perf_counter() - t0)
+            if rc != 0:
+                raise RuntimeError(f"ss_solve_gpu failed ({rc})")
+        nodes = sg.td.num_nodes
+    finally:
+        sg.free()
+    t = sorted(times)
+    out = {"workload": "heads-up river, 1081 combos per player, 2 raises, 1000 iterations",
+           "tree_nodes": nodes, "gpu_ms_per_solve_e2e": 1e3 * t[len(t) // 2],
+           "gpu_solves_per_s": len(times) / sum(times), "cpu_baseline": None}
+    try:
+        from oracle.oracle import RefSolverC, ref_solver_available
+    except ImportError:
+        return out
+    if not ref_solver_available():
+        return out
+    ref = RefSolverC()
+    cores = os.cpu_count() or 1
+    secs = [None] * cores
+
+    def one(i):
+        secs[i] = ref.solve(cfg["board"], cfg["hands"], cfg["weights"], cfg["pot"], cfg["stack"],
+                            cfg["bet_sizes"], cpu_iterations)
+
+    with _Quiet():
+        th = [threading.Thread(target=one, args=(i,)) for i in range(cores)]
+        t0 = time.perf_counter()
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        wall = time.perf_counter() - t0
+    scale = iters / cpu_iterations
+    per_solve = statistics.median(secs) * scale
+    out["cpu_baseline"] = {"solves_per_s": cores / (wall * scale), "s_per_solve": per_solve, "cores": cores,
+                           "cpu_model": cpu_model(), "kind": "reference",
+                           "sample": f"src/solver.c, {cores} concurrent solves of {cpu_iterations} iterations "
+                                     f"({wall:.1f} s wall), scaled to {iters}"}
+    return out
+
+
 def reference_cpu(seed, budget_s=25.0):
     """Seconds per CFR iteration of the reference kernels (host build) on the
     full turn3 tree, measured at small range sizes with every core running
@@ -692,6 +767,12 @@ def main():
         batched = run_batched(args.batch_size, args.seed, local)
     if rank == 0 and world == 1 and "served" in forms:
         served = run_served(args.rate, args.duration, args.seed, local)
+    hu = None
+    if rank == 0 and world == 1 and "hu_river" in forms:
+        try:
+            hu = run_hu_river(args.seed, local)
+        except Exception as e:  # the solver's line is printed whatever happens here
+            hu = {"error": f"{type(e).__name__}: {e}"}
     leaf = None
     if rank == 0 and world == 1 and "leaf" in forms and args.workload == "turn3":
         try:
@@ -723,7 +804,7 @@ def main():
             "node_hand_updates_per_s": res["value"] * res["nhu_per_solve"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
-            "batched": batched, "served": served, "leaf_producer": leaf,
+            "batched": batched, "served": served, "hu_river": hu, "leaf_producer": leaf,
         }
         print(json.dumps(line))
     try:

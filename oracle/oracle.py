@@ -426,3 +426,53 @@ class RefHandEval:
 def ref_available(max_hands=200, max_raises=3):
     return os.path.exists(os.path.join(REF_DIR, f"ref_h{max_hands}_r{max_raises}",
                                        "libref_street_solve_cpu.so"))
+
+
+class RefSolverC:
+    """src/solver.c, the reference's 2-player CPU Linear-CFR solver (built
+    -O2 -fopenmp into oracle/_ref/libref_solver.so), through its own API
+    (src/solver.h:140-187).  Its Solver struct holds fixed-size ranges
+    (MAX_HANDS = 1326, about 32 KB); it is passed as an opaque zeroed block
+    of SOLVER_BYTES.  Used as a CPU timing baseline only: its payoff, tie,
+    averaging and discount rules differ from street_solve.cu's."""
+
+    SOLVER_BYTES = 1 << 16
+
+    def __init__(self):
+        path = os.path.join(REF_DIR, "libref_solver.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        ip, fp, vp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), ctypes.c_void_p
+        self.lib.solver_init.restype = ctypes.c_int
+        self.lib.solver_init.argtypes = [vp, ip, ctypes.c_int, ip, fp, ctypes.c_int, ip, fp, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, fp, ctypes.c_int]
+        self.lib.solver_solve.restype = ctypes.c_float
+        self.lib.solver_solve.argtypes = [vp, ctypes.c_int, ctypes.c_float]
+        self.lib.solver_free.restype = None
+        self.lib.solver_free.argtypes = [vp]
+
+    def solve(self, board, hands, weights, starting_pot, effective_stack, bet_sizes, iterations):
+        """One solve (solver_init, solver_solve, solver_free); returns the
+        seconds spent in solver_solve."""
+        import time
+        b = np.ascontiguousarray(board, dtype=np.int32)
+        h = [np.ascontiguousarray(x, dtype=np.int32).reshape(-1, 2) for x in hands]
+        w = [np.ascontiguousarray(x, dtype=np.float32) for x in weights]
+        sz = np.ascontiguousarray(bet_sizes, dtype=np.float32)
+        blk = ctypes.create_string_buffer(self.SOLVER_BYTES)
+        rc = self.lib.solver_init(blk, _i32p(b), len(b), _i32p(h[0]), _f32p(w[0]), len(w[0]),
+                                  _i32p(h[1]), _f32p(w[1]), len(w[1]), int(starting_pot), int(effective_stack),
+                                  _f32p(sz), len(sz))
+        if rc != 0:
+            raise RuntimeError(f"solver_init failed ({rc})")
+        try:
+            t0 = time.perf_counter()
+            self.lib.solver_solve(blk, int(iterations), ctypes.c_float(0.0))
+            return time.perf_counter() - t0
+        finally:
+            self.lib.solver_free(blk)
+
+
+def ref_solver_available():
+    return os.path.exists(os.path.join(REF_DIR, "libref_solver.so"))

@@ -2,7 +2,9 @@
 the kernel roofline (roofline_iteration), on the three benchmark trees:
 heads-up river (51 nodes, 1081 hands), 3-player turn with continuation
 leaves (21,436 nodes, 1128 hands), 6-player river (19,579 nodes, 1081
-hands).  Trees come from the library's host-side builder; no GPU."""
+hands).  Trees come from the library's host-side builder; no GPU.  Also
+the binding of the reference's CPU solver src/solver.c that the heads-up
+river leg times as its baseline."""
 import pytest
 
 import workloads as wl
@@ -31,3 +33,16 @@ def test_flow_bytes(bench, name, over, H, nodes, want):
     assert sg.td.num_nodes == nodes
     assert bench.flow_bytes_per_iteration(sg.td, H) == want
     sg.free()
+
+
+def test_reference_cpu_solver_binding():
+    """The heads-up river CPU baseline drives the reference's own src/solver.c
+    (oracle/_ref/libref_solver.so) through its API: a small seeded solve."""
+    from oracle.oracle import RefSolverC, ref_solver_available
+    if not ref_solver_available():
+        pytest.skip("reference solver build missing")
+    import workloads as wl
+    cfg = wl.config("hu_river", seed=3, num_hands=40)
+    secs = RefSolverC().solve(cfg["board"], cfg["hands"], cfg["weights"], cfg["pot"], cfg["stack"],
+                              cfg["bet_sizes"], 5)
+    assert 0.0 < secs < 60.0
