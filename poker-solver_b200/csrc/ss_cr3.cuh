@@ -1,0 +1,265 @@
+// ss_cr3.cuh -- card-removal mass of three counted opponents (folds and
+// leaves of 4+ player subgames), the block phases of k_term_cr3.
+//
+// The reference sums, per traverser hand h, the reach products of every
+// tuple of opponent hands (o1, o2, o3) that are pairwise disjoint and
+// disjoint from h (street_solve.cu:771-823 folds, :1079-1127 leaves): O(H^3)
+// per hand.  Conditioning on the third opponent's hand gives it in O(H):
+//   M3(h) = sum_{o3 disjoint from h} r3(o3) * D2(h + o3),
+// where D2(S), the two-opponent mass avoiding a card set S, takes O(|S|^2)
+// lookups of aggregates of the first two opponents' combo matrices A, B
+// (symmetric, zero diagonal, over the dense deck):
+//   D2(S) = F_A(S) F_B(S) - Q(S) + E(S)
+//   F_A(S) = F_A - sum_{c in S} u_A(c) + sum_{pairs in S} A
+//   Q(S)   = Q - sum_{e in S} w(e) + sum_{e, f in S} P[e][f] - sum_{c in S} u~_A(c) u~_B(c),
+//            u~_A(c) = u_A(c) - sum_{e in S} A[c][e]
+//   E(S)   = E - sum_{c in S} d(c) + sum_{pairs in S} A B
+// with u = A 1, F = sum u / 2, P = A B, w = A u_B + B u_A, Q = u_A . u_B,
+// d = diag P, E = sum d / 2.  The same formula on the 0/1 matrices of
+// positive reach counts the tuples exactly (integers), which gives the
+// reference's exact zero: a hand with no tuple of positive products gets 0.
+//
+// A board card of the traverser's hand maps to the dummy index `deck`,
+// whose rows, columns and vectors are zero, so it drops out of every sum
+// (opponent hands never hold board cards).
+//
+// Each phase is a function of (thread index, thread count) whose work items
+// are independent within the phase; the kernel separates phases with block
+// barriers, and a host build runs them one after another (the check in
+// tests/native/cr3_emul.cpp).
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define SSB_CR3_HD __host__ __device__ __forceinline__
+#else
+#define SSB_CR3_HD inline
+#endif
+
+namespace ssb {
+namespace cr3 {
+
+constexpr int kS = 52;   // table stride (cards 0 .. deck, deck <= 49 plus the dummy)
+
+SSB_CR3_HD int popc64(unsigned long long x) {
+#if defined(__CUDA_ARCH__)
+    return __popcll(x);
+#else
+    return __builtin_popcountll(x);
+#endif
+}
+
+// the block's shared tables
+struct Tables {
+    double *A, *B, *P, *PT;           // [kS][kS]; PT[x][a] = P[a][x]
+    double *uA, *uB, *w, *d;          // [kS]
+    int *iuA, *iuB, *iw, *id;         // [kS]: the same on the 0/1 matrices
+    unsigned long long *mA, *mB;      // [kS]: positive cells of each row
+    double *r3;                       // [HS]: the third opponent's positive reach, compacted
+    unsigned short *xy;               // [HS]: its dense cards x | y << 8
+    double *sc;                       // [5]: F_A, F_B, Q, E, F3 (sum of the compacted r3)
+    long long *isc;                   // [5]: the same on the 0/1 matrices, then the number of o3 entries
+};
+
+// the inputs of one terminal: reach rows of the three counted opponents and
+// their pair tables ([52][52] dense-card pair -> range index, HS if none)
+template <class T>
+struct Opp3 {
+    const T *r1, *r2, *r3;
+    const int *pair1, *pair2;
+    const int *code3;                 // hand codes of the third opponent ([HS])
+    int H3, HS, deck;
+};
+
+// phase 1: the combo matrices A, B (zero outside 0..deck-1) and PT cleared
+template <class T>
+SSB_CR3_HD void phase_gather(int tid, int nt, const Opp3<T> &in, const Tables &t) {
+    for (int i = tid; i < kS * kS; i += nt) {
+        const int c = i / kS, e = i - c * kS;
+        double a = 0.0, b = 0.0;
+        if (c < in.deck && e < in.deck) {
+            const int j1 = in.pair1[c * 52 + e], j2 = in.pair2[c * 52 + e];
+            if (j1 < in.HS) a = static_cast<double>(in.r1[j1]);
+            if (j2 < in.HS) b = static_cast<double>(in.r2[j2]);
+        }
+        t.A[i] = a;
+        t.B[i] = b;
+    }
+}
+
+// phase 2: per card c (one item each): u, the positive-cell masks and counts
+SSB_CR3_HD void phase_rows(int tid, int nt, const Tables &t) {
+    for (int c = tid; c < kS; c += nt) {
+        double sa = 0.0, sb = 0.0;
+        unsigned long long ma = 0ull, mb = 0ull;
+        for (int e = 0; e < kS; ++e) {
+            const double a = t.A[c * kS + e], b = t.B[c * kS + e];
+            sa += a;
+            sb += b;
+            if (a > 0.0) ma |= 1ull << e;
+            if (b > 0.0) mb |= 1ull << e;
+        }
+        t.uA[c] = sa;
+        t.uB[c] = sb;
+        t.mA[c] = ma;
+        t.mB[c] = mb;
+        t.iuA[c] = popc64(ma);
+        t.iuB[c] = popc64(mb);
+    }
+}
+
+// phase 3: P = A B and its transpose, one cell per item (fixed order over c)
+SSB_CR3_HD void phase_product(int tid, int nt, const Tables &t) {
+    for (int i = tid; i < kS * kS; i += nt) {
+        const int e = i / kS, f = i - e * kS;
+        double s = 0.0;
+        for (int c = 0; c < kS; ++c) s += t.A[e * kS + c] * t.B[c * kS + f];
+        t.P[i] = s;
+        t.PT[f * kS + e] = s;
+    }
+}
+
+// phase 4: per card w and d, and on item kS the third opponent's compacted
+// list (in hand order) -- done by one item, so its order is fixed
+template <class T>
+SSB_CR3_HD void phase_vectors(int tid, int nt, const Opp3<T> &in, const Tables &t) {
+    for (int c = tid; c <= kS; c += nt) {
+        if (c == kS) {
+            long long n = 0;
+            double f3 = 0.0;
+            for (int h = 0; h < in.H3; ++h) {
+                const int code = in.code3[h];
+                if (code & 0x10000) continue;   // touches the board
+                const T r = in.r3[h];
+                if (!(r > T(0))) continue;
+                t.r3[n] = static_cast<double>(r);
+                f3 += t.r3[n];
+                t.xy[n] = static_cast<unsigned short>(((code >> 20) & 63) | (((code >> 26) & 63) << 8));
+                ++n;
+            }
+            t.isc[4] = n;
+            t.sc[4] = f3;
+            continue;
+        }
+        double w = 0.0;
+        int iw = 0;
+        for (int f = 0; f < kS; ++f) {
+            w += t.A[c * kS + f] * t.uB[f] + t.B[c * kS + f] * t.uA[f];
+            iw += ((t.mA[c] >> f) & 1ull ? t.iuB[f] : 0) + ((t.mB[c] >> f) & 1ull ? t.iuA[f] : 0);
+        }
+        t.w[c] = w;
+        t.iw[c] = iw;
+        t.d[c] = t.P[c * kS + c];
+        t.id[c] = popc64(t.mA[c] & t.mB[c]);
+    }
+}
+
+// phase 5 (one item): the scalars
+SSB_CR3_HD void phase_scalars(int tid, const Tables &t) {
+    if (tid != 0) return;
+    double fa = 0.0, fb = 0.0, q = 0.0, e = 0.0;
+    long long ifa = 0, ifb = 0, iq = 0, ie = 0;
+    for (int c = 0; c < kS; ++c) {
+        fa += t.uA[c];
+        fb += t.uB[c];
+        q += t.uA[c] * t.uB[c];
+        e += t.d[c];
+        ifa += t.iuA[c];
+        ifb += t.iuB[c];
+        iq += static_cast<long long>(t.iuA[c]) * t.iuB[c];
+        ie += t.id[c];
+    }
+    t.sc[0] = 0.5 * fa;
+    t.sc[1] = 0.5 * fb;
+    t.sc[2] = q;
+    t.sc[3] = 0.5 * e;
+    t.isc[0] = ifa / 2;
+    t.isc[1] = ifb / 2;
+    t.isc[2] = iq;
+    t.isc[3] = ie / 2;
+}
+
+// the mass of one traverser hand with dense cards (a, b), a board card
+// given as the dummy index (the deck size)
+SSB_CR3_HD double hand_mass(int a, int b, const Tables &t) {
+    const double *A = t.A, *B = t.B, *P = t.P, *PT = t.PT;
+    const double Aab = A[a * kS + b], Bab = B[a * kS + b];
+    const double fa_h = t.sc[0] - t.uA[a] - t.uA[b] + Aab, fb_h = t.sc[1] - t.uB[a] - t.uB[b] + Bab;
+    const double Phh = P[a * kS + a] + P[a * kS + b] + P[b * kS + a] + P[b * kS + b];
+    const double wdh = t.w[a] + t.w[b], ddh = t.d[a] + t.d[b];
+    const double Q = t.sc[2], E = t.sc[3];
+    double mass = 0.0;
+    const long long n3 = t.isc[4];
+    for (long long k = 0; k < n3; ++k) {
+        const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
+        if (x == a || x == b || y == a || y == b) continue;   // shares a card with the traverser
+        // cross terms between {a, b} and {x, y}: rows x and y of the
+        // symmetric A, B and of P and P^T
+        const double Aax = A[x * kS + a], Aay = A[y * kS + a], Abx = A[x * kS + b], Aby = A[y * kS + b];
+        const double Bax = B[x * kS + a], Bay = B[y * kS + a], Bbx = B[x * kS + b], Bby = B[y * kS + b];
+        const double Axy = A[x * kS + y], Bxy = B[x * kS + y];
+        const double Px = P[x * kS + a] + P[x * kS + b] + PT[x * kS + a] + PT[x * kS + b];
+        const double Py = P[y * kS + a] + P[y * kS + b] + PT[y * kS + a] + PT[y * kS + b];
+        const double Poo = P[x * kS + x] + P[x * kS + y] + P[y * kS + x] + P[y * kS + y];
+        const double FAS = fa_h - t.uA[x] - t.uA[y] + Axy + (Aax + Aay + Abx + Aby);
+        const double FBS = fb_h - t.uB[x] - t.uB[y] + Bxy + (Bax + Bay + Bbx + Bby);
+        const double ua = t.uA[a] - Aab - Aax - Aay, ub = t.uA[b] - Aab - Abx - Aby;
+        const double ux = t.uA[x] - Axy - Aax - Abx, uy = t.uA[y] - Axy - Aay - Aby;
+        const double va = t.uB[a] - Bab - Bax - Bay, vb = t.uB[b] - Bab - Bbx - Bby;
+        const double vx = t.uB[x] - Bxy - Bax - Bbx, vy = t.uB[y] - Bxy - Bay - Bby;
+        const double QS = Q - (wdh + t.w[x] + t.w[y]) + (Phh + Poo + Px + Py) - (ua * va + ub * vb + ux * vx + uy * vy);
+        const double ES = E - (ddh + t.d[x] + t.d[y]) + Aab * Bab + Axy * Bxy + Aax * Bax + Aay * Bay + Abx * Bbx +
+                          Aby * Bby;
+        mass += t.r3[k] * (FAS * FBS - QS + ES);
+    }
+    return mass;
+}
+
+// the number of disjoint tuples with positive reach products: the same
+// formula on the 0/1 matrices, exact in integers
+SSB_CR3_HD long long hand_count(int a, int b, const Tables &t) {
+    const unsigned long long mAa = t.mA[a], mAb = t.mA[b], mBa = t.mB[a], mBb = t.mB[b];
+    const int iAab = static_cast<int>((mAa >> b) & 1ull), iBab = static_cast<int>((mBa >> b) & 1ull);
+    const long long fa_h = t.isc[0] - t.iuA[a] - t.iuA[b] + iAab, fb_h = t.isc[1] - t.iuB[a] - t.iuB[b] + iBab;
+    const int Phh = popc64(mAa & mBa) + popc64(mAa & mBb) + popc64(mAb & mBa) + popc64(mAb & mBb);
+    const int wdh = t.iw[a] + t.iw[b], ddh = t.id[a] + t.id[b];
+    const long long Q = t.isc[2], E = t.isc[3];
+    long long count = 0;
+    const long long n3 = t.isc[4];
+    for (long long k = 0; k < n3; ++k) {
+        const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
+        if (x == a || x == b || y == a || y == b) continue;
+        const unsigned long long mAx = t.mA[x], mAy = t.mA[y], mBx = t.mB[x], mBy = t.mB[y];
+        const int Aax = static_cast<int>((mAx >> a) & 1ull), Aay = static_cast<int>((mAy >> a) & 1ull);
+        const int Abx = static_cast<int>((mAx >> b) & 1ull), Aby = static_cast<int>((mAy >> b) & 1ull);
+        const int Bax = static_cast<int>((mBx >> a) & 1ull), Bay = static_cast<int>((mBy >> a) & 1ull);
+        const int Bbx = static_cast<int>((mBx >> b) & 1ull), Bby = static_cast<int>((mBy >> b) & 1ull);
+        const int Axy = static_cast<int>((mAx >> y) & 1ull), Bxy = static_cast<int>((mBx >> y) & 1ull);
+        const int Px = popc64(mAx & mBa) + popc64(mAx & mBb) + popc64(mAa & mBx) + popc64(mAb & mBx);
+        const int Py = popc64(mAy & mBa) + popc64(mAy & mBb) + popc64(mAa & mBy) + popc64(mAb & mBy);
+        const int Poo = popc64(mAx & mBx) + popc64(mAx & mBy) + popc64(mAy & mBx) + popc64(mAy & mBy);
+        const long long FAS = fa_h - t.iuA[x] - t.iuA[y] + Axy + (Aax + Aay + Abx + Aby);
+        const long long FBS = fb_h - t.iuB[x] - t.iuB[y] + Bxy + (Bax + Bay + Bbx + Bby);
+        const long long ua = t.iuA[a] - iAab - Aax - Aay, ub = t.iuA[b] - iAab - Abx - Aby;
+        const long long ux = t.iuA[x] - Axy - Aax - Abx, uy = t.iuA[y] - Axy - Aay - Aby;
+        const long long va = t.iuB[a] - iBab - Bax - Bay, vb = t.iuB[b] - iBab - Bbx - Bby;
+        const long long vx = t.iuB[x] - Bxy - Bax - Bbx, vy = t.iuB[y] - Bxy - Bay - Bby;
+        const long long QS = Q - (wdh + t.iw[x] + t.iw[y]) + (Phh + Poo + Px + Py) - (ua * va + ub * vb + ux * vx + uy * vy);
+        const long long ES = E - (ddh + t.id[x] + t.id[y]) + iAab * iBab + Axy * Bxy + Aax * Bax + Aay * Bay +
+                             Abx * Bbx + Aby * Bby;
+        count += FAS * FBS - QS + ES;
+    }
+    return count;
+}
+
+// The largest FP64 rounding of hand_mass on a tuple set that is empty: each
+// of its ~H3 terms is a few F_A F_B in size times r3 <= F3, so 1e-9 of
+// F_A F_B F3 bounds it with a wide margin; a hand whose mass is at or below
+// this bound takes the exact count to decide whether it is 0.
+SSB_CR3_HD double zero_bound(const Tables &t) {
+    return 1e-9 * (t.sc[0] + 1.0) * (t.sc[1] + 1.0) * (t.sc[4] + 1.0);
+}
+
+}  // namespace cr3
+}  // namespace ssb

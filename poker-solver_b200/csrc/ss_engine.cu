@@ -472,10 +472,13 @@ int Session::exploitability(const float *host_avg, double *pct, double *nash, do
         deal.opp_row[o - 1] = P.E + o;
         deal.opp_player[o - 1] = o;
     }
+    const bool deal_cr3 = np == 4 && !P.dup[1] && !P.dup[2] && P.H[1] >= kCr3MinHands &&
+                          P.H[2] >= kCr3MinHands && P.H[3] >= kCr3MinHands;
     const int deal_kind = np == 1   ? TK_LEAF0
                           : np == 2 ? (P.dup[1] ? TK_CR1D : TK_CR1)
                           : np == 3 ? TK_CR2
-                                    : TK_ENUM;
+                          : deal_cr3 ? TK_CR3
+                                     : TK_ENUM;
     if (deal_kind == TK_ENUM) {
         double w = P.H[0];
         for (int o = 1; o < np; ++o) w *= std::max(1, P.H[o]);

@@ -117,6 +117,11 @@ constexpr int kSd2Slots = 148 * 4;
 constexpr int kSd2Merge = 5;
 static_assert(kSd2Chunks == 1 << (kSd2Merge - 1), "runs merge in powers of two");
 
+// Folds and leaves with three counted opponents use the conditioning closed
+// form (TK_CR3) once every counted range holds at least this many hands and
+// the first two hold no combo twice; smaller ranges enumerate (TK_ENUM).
+constexpr int kCr3MinHands = 16;
+
 // Terminal kinds per traverser.
 enum TermKind : int {
     TK_ZERO = 0,     // value 0 (folded traverser at showdown, leaves without leaf values)
@@ -127,7 +132,8 @@ enum TermKind : int {
     TK_ENUM = 5,     // anything else: exact tuple enumeration (small ranges only)
     TK_SD2 = 6,      // three-way showdown (two live opponents), ranges without repeated combos
     TK_CR1D = 7,     // TK_CR1 against a range that holds some combo more than once
-    TK_COUNT = 8
+    TK_CR3 = 8,      // fold / leaf with three counted opponents (large ranges; small ones enumerate)
+    TK_COUNT = 9
 };
 
 // One terminal for one traverser.  factor: payoff for folds; leaf_off >= 0

@@ -13,6 +13,7 @@
 // opponents).  The reference enumerates opponent tuples per traverser hand
 // instead (street_solve.cu:704-1130), which is O(H^k).
 #include "ss_kernels.h"
+#include "ss_cr3.cuh"
 
 namespace ssb {
 
@@ -1847,6 +1848,92 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c0, const DevCtx *__re
     out[h] = sd ? total : static_cast<T>(term_factor(c, I, h)) * total;
 }
 
+// Folds and leaves with three counted opponents (4+ player subgames): the
+// card-removal mass by conditioning on the third opponent (ss_cr3.cuh), in
+// FP64, one block per (terminal, chunk of kTermThreads traverser hands), one
+// thread per hand; the first two opponents' aggregates are rebuilt by every
+// chunk's block (O(deck^3), small beside the O(H3) walk of each hand).  A
+// hand whose mass is within rounding of 0 takes the exact tuple count, and 0
+// when there is none (the reference adds only positive products).
+constexpr size_t cr3_smem(int HS) {
+    return (4 * cr3::kS * cr3::kS + 4 * cr3::kS + 8) * sizeof(double) + 4 * cr3::kS * sizeof(int) +
+           2 * cr3::kS * sizeof(unsigned long long) + 8 * sizeof(long long) +
+           static_cast<size_t>(HS) * (sizeof(double) + sizeof(unsigned short)) + 16 * 16;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                             const TermItem *__restrict__ items, int nchunk,
+                                                             int trav) {
+    extern __shared__ __align__(16) char smem[];
+    const int it = blockIdx.x / nchunk;
+    const int ch = blockIdx.x - it * nchunk;
+    const TermItem I = items[it];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    const int HS = c.HS;
+    // shared memory was provisioned for c0's row stride (the largest of a batch)
+    if (HS > c0.HS || c.deck > cr3::kS - 1) return;
+    const int h0 = ch * kTermThreads;
+    if (h0 >= HS) return;
+    Carve cv{smem};
+    cr3::Tables t;
+    t.A = cv.take<double>(cr3::kS * cr3::kS);
+    t.B = cv.take<double>(cr3::kS * cr3::kS);
+    t.P = cv.take<double>(cr3::kS * cr3::kS);
+    t.PT = cv.take<double>(cr3::kS * cr3::kS);
+    t.uA = cv.take<double>(cr3::kS);
+    t.uB = cv.take<double>(cr3::kS);
+    t.w = cv.take<double>(cr3::kS);
+    t.d = cv.take<double>(cr3::kS);
+    t.sc = cv.take<double>(8);
+    t.iuA = cv.take<int>(cr3::kS);
+    t.iuB = cv.take<int>(cr3::kS);
+    t.iw = cv.take<int>(cr3::kS);
+    t.id = cv.take<int>(cr3::kS);
+    t.mA = cv.take<unsigned long long>(cr3::kS);
+    t.mB = cv.take<unsigned long long>(cr3::kS);
+    t.isc = cv.take<long long>(8);
+    t.r3 = cv.take<double>(HS);
+    t.xy = cv.take<unsigned short>(HS);
+    const T *reach = reach_rows<T>(c);
+    const size_t hs = static_cast<size_t>(HS);
+    cr3::Opp3<T> in;
+    in.r1 = reach + static_cast<size_t>(I.opp_row[0]) * hs;
+    in.r2 = reach + static_cast<size_t>(I.opp_row[1]) * hs;
+    in.r3 = reach + static_cast<size_t>(I.opp_row[2]) * hs;
+    in.pair1 = c.pair_idx + static_cast<size_t>(I.opp_player[0]) * 52 * 52;
+    in.pair2 = c.pair_idx + static_cast<size_t>(I.opp_player[1]) * 52 * 52;
+    in.code3 = c.hand_code + static_cast<size_t>(I.opp_player[2]) * hs;
+    in.H3 = c.H[I.opp_player[2]];
+    in.HS = HS;
+    in.deck = c.deck;
+    const int tid = threadIdx.x;
+    cr3::phase_gather(tid, kTermThreads, in, t);
+    __syncthreads();
+    cr3::phase_rows(tid, kTermThreads, t);
+    __syncthreads();
+    cr3::phase_product(tid, kTermThreads, t);
+    __syncthreads();
+    cr3::phase_vectors(tid, kTermThreads, in, t);
+    __syncthreads();
+    cr3::phase_scalars(tid, t);
+    __syncthreads();
+    const int h = h0 + tid;
+    if (h >= HS) return;
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * hs;
+    if (h >= c.H[trav]) {
+        out[h] = T(0);
+        return;
+    }
+    const int hc = c.hand_code[static_cast<size_t>(trav) * hs + h];
+    int a = (hc >> 20) & 63, b = (hc >> 26) & 63;
+    if (a >= c.deck) a = c.deck;   // a board card: the zero dummy row
+    if (b >= c.deck) b = c.deck;
+    double m = cr3::hand_mass(a, b, t);
+    if (fabs(m) <= cr3::zero_bound(t) && cr3::hand_count(a, b, t) == 0) m = 0.0;
+    out[h] = static_cast<T>(static_cast<double>(term_factor(c, I, h)) * m);
+}
+
 // --------------------------------------------------------------------------
 // best response (FP64): exploitability of an average-strategy profile
 // avg[(di * 8 + a) * max_h + h] (the SSOutput layout)
@@ -2084,6 +2171,15 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
         case TK_ENUM: {
             const int nc = (c.HS + 127) / 128;
             k_term_enum<T><<<n * nc, 128, 0, s>>>(c, ctxs, items, nc, trav);
+            break;
+        }
+        case TK_CR3: {
+            if (c.HS > kMaxHS) return cudaErrorInvalidValue;
+            const int nc = (c.HS + kTermThreads - 1) / kTermThreads;
+            e = cudaFuncSetAttribute(k_term_cr3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(cr3_smem(kMaxHS)));
+            if (e != cudaSuccess) return e;
+            k_term_cr3<T><<<n * nc, kTermThreads, cr3_smem(c.HS), s>>>(c, ctxs, items, nc, trav);
             break;
         }
         default:

@@ -303,20 +303,28 @@ int build_plan(const Problem &pb, Plan *out) {
                 it.opp_player[k] = o;
                 ++k;
             };
+            // three counted opponents: closed form for large ranges without
+            // repeated combos in the two that form its matrices
+            auto multi = [&]() {
+                if (k != 3 || P.dup[it.opp_player[0]] || P.dup[it.opp_player[1]]) return static_cast<int>(TK_ENUM);
+                for (int i = 0; i < 3; ++i)
+                    if (P.H[it.opp_player[i]] < kCr3MinHands) return static_cast<int>(TK_ENUM);
+                return static_cast<int>(TK_CR3);
+            };
             if (n.type == SS_NODE_FOLD) {
                 for (int o = 0; o < np; ++o)
                     if (o != t) add_opp(o);
                 it.payoff = (n.player == t) ? static_cast<float>(n.pot - n.bets[t])
                                             : -static_cast<float>(n.bets[t]);
                 it.kind_detail = 0;
-                kind = k == 0 ? TK_LEAF0 : k == 1 ? (P.dup[it.opp_player[0]] ? TK_CR1D : TK_CR1) : k == 2 ? TK_CR2 : TK_ENUM;
+                kind = k == 0 ? TK_LEAF0 : k == 1 ? (P.dup[it.opp_player[0]] ? TK_CR1D : TK_CR1) : k == 2 ? TK_CR2 : multi();
             } else if (n.type == SS_NODE_LEAF) {
                 if (pb.leaf_values && n.leaf_idx >= 0) {
                     for (int o = 0; o < np; ++o)
                         if (o != t && n.active_players[o]) add_opp(o);
                     it.leaf_off = (n.leaf_idx * np + t) * P.max_h;
                     it.kind_detail = 1;
-                    kind = k == 0 ? TK_LEAF0 : k == 1 ? (P.dup[it.opp_player[0]] ? TK_CR1D : TK_CR1) : k == 2 ? TK_CR2 : TK_ENUM;
+                    kind = k == 0 ? TK_LEAF0 : k == 1 ? (P.dup[it.opp_player[0]] ? TK_CR1D : TK_CR1) : k == 2 ? TK_CR2 : multi();
                 }
             } else {  // showdown
                 if (pb.is_river && n.active_players[t]) {

@@ -76,6 +76,8 @@ int main(int argc, char **argv) {
     const int rc = ssb::build_plan(pb, &P);
     std::printf("{\"rc\": %d, \"dup\": [", rc);
     for (int p = 0; p < np; ++p) std::printf("%s%d", p ? ", " : "", rc == SS_OK ? P.dup[p] : -1);
+    std::printf("], \"hands\": [");
+    for (int p = 0; p < np; ++p) std::printf("%s%d", p ? ", " : "", rc == SS_OK ? P.H[p] : -1);
     std::printf("], \"terminals\": [");
     bool first = true;
     for (size_t x = 0; x < bt.nodes.size(); ++x) {

@@ -108,8 +108,9 @@ def test_one_wave_cap(driver):
 
 
 # TermKind values (ss_engine.h)
-ZERO, LEAF0, CR1, CR2, SD1, ENUM, SD2, CR1D = range(8)
+ZERO, LEAF0, CR1, CR2, SD1, ENUM, SD2, CR1D, CR3 = range(9)
 FOLD, SHOWDOWN, LEAF = 1, 2, 4
+CR3_MIN_HANDS = 16   # kCr3MinHands
 
 
 def expected_kinds(d, np_, river, leaves):
@@ -117,17 +118,23 @@ def expected_kinds(d, np_, river, leaves):
     (river, traverser live) and leaves (with leaf values) the live others;
     0 / 1 / 2 counted opponents take the closed forms, one opponent whose
     range repeats a combo the scatter form, three-way showdowns with such a
-    range and anything with 3+ counted opponents exact enumeration."""
-    want = [[0] * 8 for _ in range(np_)]
+    range and anything else with 3+ counted opponents exact enumeration --
+    except folds and leaves with exactly three, which take the conditioning
+    closed form when every counted range holds at least 16 hands and the
+    first two repeat no combo."""
+    want = [[0] * 9 for _ in range(np_)]
     dup = d["dup"]
+    nh = d["hands"]
     for typ, leaf_idx, active in d["terminals"]:
         for t in range(np_):
             opp = [o for o in range(np_) if o != t and (typ == FOLD or active[o])]
             k = len(opp)
             kind = ZERO
             if typ == FOLD or (typ == LEAF and leaves and leaf_idx >= 0):
+                cr3 = (k == 3 and not dup[opp[0]] and not dup[opp[1]]
+                       and all(nh[o] >= CR3_MIN_HANDS for o in opp))
                 kind = (LEAF0 if k == 0 else (CR1D if dup[opp[0]] else CR1) if k == 1
-                        else CR2 if k == 2 else ENUM)
+                        else CR2 if k == 2 else CR3 if cr3 else ENUM)
             elif typ == SHOWDOWN and river and active[t]:
                 kind = (SD1 if k == 1 else SD2 if k == 2 and not (dup[t] or dup[opp[0]] or dup[opp[1]])
                         else ENUM)
@@ -140,7 +147,11 @@ def expected_kinds(d, np_, river, leaves):
     (2, 5, 30, 1, 0, 2),      # heads-up, opponent 1 repeats a combo: its folds take the scatter form
     (3, 5, 20, -1, 0, 2),     # three-way showdowns, two-opponent folds
     (3, 5, 20, 1, 0, 1),      # a repeated combo: scatter form, enumerated three-way showdowns
-    (4, 5, 8, -1, 0, 1),      # three counted opponents at folds: enumeration
+    (4, 5, 8, -1, 0, 1),      # three counted opponents at folds, small ranges: enumeration
+    (4, 5, 20, -1, 0, 1),     # ... larger ranges: the three-opponent closed form
+    (4, 5, 20, 1, 0, 1),      # ... unless a matrix opponent repeats a combo
+    (4, 4, 16, -1, 1, 1),     # 4-player turn: folds and leaves with three counted opponents
+    (5, 5, 20, -1, 0, 1),     # four counted opponents: enumeration
     (3, 4, 12, -1, 1, 1),     # turn with continuation leaves
     (3, 4, 12, -1, 0, 1),     # the same without leaf values: leaves are zero
 ])
