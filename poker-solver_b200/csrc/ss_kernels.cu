@@ -1850,11 +1850,14 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c0, const DevCtx *__re
 
 // Folds and leaves with three counted opponents (4+ player subgames): the
 // card-removal mass by conditioning on the third opponent (ss_cr3.cuh), in
-// FP64, one block per (terminal, chunk of kTermThreads traverser hands), one
-// thread per hand; the first two opponents' aggregates are rebuilt by every
-// chunk's block (O(deck^3), small beside the O(H3) walk of each hand).  A
-// hand whose mass is within rounding of 0 takes the exact tuple count, and 0
-// when there is none (the reference adds only positive products).
+// FP64, one block per (group of terminals, chunk of kTermThreads traverser
+// hands), one thread per hand; the first two opponents' aggregates are
+// rebuilt by every chunk's block (O(deck^3), small beside the O(H3) walk of
+// each hand).  A hand whose mass is within rounding of 0 takes the exact
+// tuple count, and 0 when there is none (the reference adds only positive
+// products).  Terminals on the same opponent reach rows (the traverser's own
+// continuation choices) form a group: its first item's blocks write every
+// member's row, each with its own factor.
 constexpr size_t cr3_smem(int HS) {
     return (4 * cr3::kS * cr3::kS + 4 * cr3::kS + 8) * sizeof(double) + 4 * cr3::kS * sizeof(int) +
            2 * cr3::kS * sizeof(unsigned long long) + 8 * sizeof(long long) +
@@ -1868,7 +1871,10 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     extern __shared__ __align__(16) char smem[];
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
-    const TermItem I = items[it];
+    const TermItem *I0 = items + it;
+    if (I0->follow) return;   // written by the blocks of its group's first item
+    const int ng = I0->gextra + 1;
+    const TermItem I = *I0;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int HS = c.HS;
     // shared memory was provisioned for c0's row stride (the largest of a batch)
@@ -1920,9 +1926,9 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     __syncthreads();
     const int h = h0 + tid;
     if (h >= HS) return;
-    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * hs;
+    T *val = val_rows<T>(c);
     if (h >= c.H[trav]) {
-        out[h] = T(0);
+        for (int g = 0; g < ng; ++g) val[static_cast<size_t>(I0[g].node) * hs + h] = T(0);
         return;
     }
     const int hc = c.hand_code[static_cast<size_t>(trav) * hs + h];
@@ -1931,7 +1937,10 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     if (b >= c.deck) b = c.deck;
     double m = cr3::hand_mass(a, b, t);
     if (fabs(m) <= cr3::zero_bound(t) && cr3::hand_count(a, b, t) == 0) m = 0.0;
-    out[h] = static_cast<T>(static_cast<double>(term_factor(c, I, h)) * m);
+    for (int g = 0; g < ng; ++g) {
+        const TermItem &Ig = I0[g];
+        val[static_cast<size_t>(Ig.node) * hs + h] = static_cast<T>(static_cast<double>(term_factor(c, Ig, h)) * m);
+    }
 }
 
 // --------------------------------------------------------------------------

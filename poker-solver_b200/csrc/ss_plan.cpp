@@ -350,20 +350,25 @@ int build_plan(const Problem &pb, Plan *out) {
         }
     }
 
-    // one- and two-opponent terminals sharing their opponents' reach rows
-    // share their card-removal mass: order them by the rows and mark groups
+    // one-, two- and three-opponent terminals sharing their opponents' reach
+    // rows share their card-removal mass: order them by the rows and mark
+    // groups (rows and players past the counted ones are 0)
     for (int t = 0; t < np; ++t)
-        for (int kind : {TK_CR1, TK_CR2}) {
+        for (int kind : {TK_CR1, TK_CR2, TK_CR3}) {
             std::vector<TermItem> &v = P.term[t][kind];
             std::stable_sort(v.begin(), v.end(), [](const TermItem &u, const TermItem &w) {
                 if (u.opp_row[0] != w.opp_row[0]) return u.opp_row[0] < w.opp_row[0];
-                return u.opp_row[1] < w.opp_row[1];
+                if (u.opp_row[1] != w.opp_row[1]) return u.opp_row[1] < w.opp_row[1];
+                return u.opp_row[2] < w.opp_row[2];
             });
+            auto same = [](const TermItem &u, const TermItem &w) {
+                for (int i = 0; i < 3; ++i)
+                    if (u.opp_row[i] != w.opp_row[i] || u.opp_player[i] != w.opp_player[i]) return false;
+                return true;
+            };
             for (size_t i = 0; i < v.size();) {
                 size_t j = i + 1;
-                while (j < v.size() && j - i < static_cast<size_t>(kTermGroupMax) &&
-                       v[j].opp_row[0] == v[i].opp_row[0] && v[j].opp_row[1] == v[i].opp_row[1] &&
-                       v[j].opp_player[0] == v[i].opp_player[0] && v[j].opp_player[1] == v[i].opp_player[1])
+                while (j < v.size() && j - i < static_cast<size_t>(kTermGroupMax) && same(v[j], v[i]))
                     ++j;
                 v[i].gextra = static_cast<int>(j - i - 1);
                 for (size_t m = i + 1; m < j; ++m) v[m].follow = 1;

@@ -95,6 +95,25 @@ int main(int argc, char **argv) {
             std::printf("%s%zu", k ? ", " : "", rc == SS_OK ? P.term[t][k].size() : static_cast<size_t>(0));
         std::printf("]");
     }
+    // closed-form groups: per traverser and kind (CR1, CR2, CR3), every item
+    // as [gextra, follow, rows 0..2, players 0..2]
+    std::printf("], \"groups\": [");
+    for (int t = 0; t < np; ++t) {
+        std::printf("%s[", t ? ", " : "");
+        int kk = 0;
+        for (int kind : {ssb::TK_CR1, ssb::TK_CR2, ssb::TK_CR3}) {
+            std::printf("%s[", kk++ ? ", " : "");
+            if (rc == SS_OK)
+                for (size_t i = 0; i < P.term[t][kind].size(); ++i) {
+                    const ssb::TermItem &it = P.term[t][kind][i];
+                    std::printf("%s[%d, %d, %d, %d, %d, %d, %d, %d]", i ? ", " : "", it.gextra, it.follow,
+                                it.opp_row[0], it.opp_row[1], it.opp_row[2], it.opp_player[0], it.opp_player[1],
+                                it.opp_player[2]);
+                }
+            std::printf("]");
+        }
+        std::printf("]");
+    }
     std::printf("]}\n");
     return 0;
 }

@@ -162,3 +162,25 @@ def test_terminal_routing(kinds_driver, np_, nb, nh, dup, leaves, raises):
     assert d["rc"] == 0
     assert d["dup"] == [1 if p == dup else 0 for p in range(np_)]
     assert d["kinds"] == expected_kinds(d, np_, nb == 5, leaves)
+    check_groups(d)
+
+
+def check_groups(d):
+    """Closed-form terminals sharing their opponents' reach rows form
+    groups: a leader with gextra followers right after it, all on the same
+    rows and players, at most 16 items; nothing else shares rows with a
+    neighbour outside its group."""
+    for per_kind in d["groups"]:
+        for items in per_kind:
+            i = 0
+            while i < len(items):
+                lead = items[i]
+                assert lead[1] == 0, "a group starts with its leader"
+                n = lead[0] + 1
+                assert n <= 16
+                for m in items[i + 1:i + n]:
+                    assert m[1] == 1 and m[2:] == lead[2:]
+                nxt = items[i + n] if i + n < len(items) else None
+                if nxt is not None and n < 16:
+                    assert nxt[2:] != lead[2:], "a full group ends where its rows end"
+                i += n
