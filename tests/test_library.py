@@ -174,8 +174,10 @@ def test_rejects_empty_ranges_and_bad_iterations():
 
 
 def test_large_multiway_enumeration_is_refused():
-    """Terminals with three or more counted opponents at full range size are
-    refused with SS_ERR_UNSUPPORTED instead of running for hours."""
+    """Terminals that still need enumeration at full range size -- the
+    6-player river's folds with five counted opponents and its 4+-way
+    showdowns -- are refused with SS_ERR_UNSUPPORTED instead of running for
+    hours."""
     cfg = wl.config("river6", seed=0)
     sg = wl.AbiSubgame(cfg, max_hands=1326)
     rc, msg = _solve_rc(sg)
