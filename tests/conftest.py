@@ -30,12 +30,12 @@ def _have_gpu():
 HAVE_GPU = _have_gpu()
 
 
-# Files run after all others, in this order: the three-opponent closed form's
-# and the continuation-value producer's GPU tests after the rest of the
-# solver's (so that under -x a failure there cannot keep the solver's tests
-# from running), the no-allocation entry point last.  The sort is stable:
-# everything else keeps file order.
-_RUN_LATE = {"test_cr3_gpu.py": 1, "test_leaf_values_gpu.py": 2, "test_zz_no_alloc.py": 3}
+# Files run after all others, in this order: the continuation-value
+# producer's and the three-opponent closed form's GPU tests after the rest
+# of the solver's (so that under -x a failure there cannot keep the solver's
+# tests from running), the no-allocation entry point last.  The sort is
+# stable: everything else keeps file order.
+_RUN_LATE = {"test_leaf_values_gpu.py": 1, "test_cr3_gpu.py": 2, "test_zz_no_alloc.py": 3}
 
 
 def pytest_collection_modifyitems(config, items):
