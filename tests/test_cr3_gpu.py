@@ -7,7 +7,10 @@ ones enumerate), on the GPU against the oracle:
 * a 4-player turn with continuation leaves (5,681 nodes, 16 hands): folds
   and leaves with three counted opponents, against the FP32 oracle;
 * the FP64 best response, whose 4-player deal mass also takes the closed
-  form, against the oracle's FP64 CPU best response to 1e-9 relative.
+  form, against the oracle's FP64 CPU best response to 1e-9 relative;
+* what remains on exact enumeration: the 6-player river benchmark tree
+  (19,579 nodes; folds with five counted opponents, 2- to 6-way showdowns)
+  at 5 hands per player, against the FP32 oracle.
 The closed form itself is checked against enumeration on the host
 (tests/test_cr3_host.py).  Collected after the solver's other GPU tests
 (tests/conftest.py)."""
@@ -69,3 +72,10 @@ def test_four_player_best_response(oracle):
         scale = max(abs(ref["br_value"][p]), abs(ref["cur_value"][p]), 1e-300)
         assert abs(g["br"][p] - ref["br_value"][p]) / scale <= 1e-9
         assert abs(g["cur"][p] - ref["cur_value"][p]) / scale <= 1e-9
+
+
+def test_six_player_river_tree_small_ranges(oracle):
+    cfg = wl.config("river6", seed=31, num_hands=5)
+    cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(31), cfg["board"], 6, 5)
+    ours, lv = solve(cfg, 3)
+    strict(ours, oracle_f32(oracle, cfg, 3, lv))
