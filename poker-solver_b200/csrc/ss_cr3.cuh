@@ -123,9 +123,10 @@ SSB_CR3_HD void phase_product(int tid, int nt, const Tables &t) {
 // phase 4: per card w and d, and on item kS the third opponent's compacted
 // list (in hand order) -- done by one item, so its order is fixed
 template <class T>
-SSB_CR3_HD void phase_vectors(int tid, int nt, const Opp3<T> &in, const Tables &t) {
+SSB_CR3_HD void phase_vectors(int tid, int nt, const Opp3<T> &in, const Tables &t, bool compact = true) {
     for (int c = tid; c <= kS; c += nt) {
         if (c == kS) {
+            if (!compact) continue;
             long long n = 0;
             double f3 = 0.0;
             for (int h = 0; h < in.H3; ++h) {
@@ -180,38 +181,103 @@ SSB_CR3_HD void phase_scalars(int tid, const Tables &t) {
     t.isc[3] = ie / 2;
 }
 
+// The traverser's part of every sum in D2(S), S = {a, b} + {x, y}: computed
+// once per hand, reused for every third-opponent hand (x, y).
+struct HandPart {
+    double Aab, Bab, fa, fb, Phh, wd, dd;
+};
+
+SSB_CR3_HD HandPart hand_part(int a, int b, const Tables &t) {
+    const double *A = t.A, *B = t.B, *P = t.P;
+    HandPart hp;
+    hp.Aab = A[a * kS + b];
+    hp.Bab = B[a * kS + b];
+    hp.fa = t.sc[0] - t.uA[a] - t.uA[b] + hp.Aab;
+    hp.fb = t.sc[1] - t.uB[a] - t.uB[b] + hp.Bab;
+    hp.Phh = P[a * kS + a] + P[a * kS + b] + P[b * kS + a] + P[b * kS + b];
+    hp.wd = t.w[a] + t.w[b];
+    hp.dd = t.d[a] + t.d[b];
+    return hp;
+}
+
+// D2({a, b, x, y}) of the tables' two matrices; (x, y) disjoint from (a, b).
+// The cross terms between {a, b} and {x, y} read rows x and y of the
+// symmetric A, B and of P and P^T.
+SSB_CR3_HD double d2_at(const HandPart &hp, int a, int b, int x, int y, const Tables &t) {
+    const double *A = t.A, *B = t.B, *P = t.P, *PT = t.PT;
+    const double Aax = A[x * kS + a], Aay = A[y * kS + a], Abx = A[x * kS + b], Aby = A[y * kS + b];
+    const double Bax = B[x * kS + a], Bay = B[y * kS + a], Bbx = B[x * kS + b], Bby = B[y * kS + b];
+    const double Axy = A[x * kS + y], Bxy = B[x * kS + y];
+    const double Px = P[x * kS + a] + P[x * kS + b] + PT[x * kS + a] + PT[x * kS + b];
+    const double Py = P[y * kS + a] + P[y * kS + b] + PT[y * kS + a] + PT[y * kS + b];
+    const double Poo = P[x * kS + x] + P[x * kS + y] + P[y * kS + x] + P[y * kS + y];
+    const double FAS = hp.fa - t.uA[x] - t.uA[y] + Axy + (Aax + Aay + Abx + Aby);
+    const double FBS = hp.fb - t.uB[x] - t.uB[y] + Bxy + (Bax + Bay + Bbx + Bby);
+    const double ua = t.uA[a] - hp.Aab - Aax - Aay, ub = t.uA[b] - hp.Aab - Abx - Aby;
+    const double ux = t.uA[x] - Axy - Aax - Abx, uy = t.uA[y] - Axy - Aay - Aby;
+    const double va = t.uB[a] - hp.Bab - Bax - Bay, vb = t.uB[b] - hp.Bab - Bbx - Bby;
+    const double vx = t.uB[x] - Bxy - Bax - Bbx, vy = t.uB[y] - Bxy - Bay - Bby;
+    const double QS = t.sc[2] - (hp.wd + t.w[x] + t.w[y]) + (hp.Phh + Poo + Px + Py) -
+                      (ua * va + ub * vb + ux * vx + uy * vy);
+    const double ES = t.sc[3] - (hp.dd + t.d[x] + t.d[y]) + hp.Aab * hp.Bab + Axy * Bxy + Aax * Bax + Aay * Bay +
+                      Abx * Bbx + Aby * Bby;
+    return FAS * FBS - QS + ES;
+}
+
+// the same on the 0/1 matrices: the number of disjoint (o1, o2) pairs of
+// positive reach avoiding {a, b, x, y}
+struct HandCount {
+    long long fa, fb;
+    int iAab, iBab, Phh, wd, dd;
+};
+
+SSB_CR3_HD HandCount hand_count_part(int a, int b, const Tables &t) {
+    const unsigned long long mAa = t.mA[a], mAb = t.mA[b], mBa = t.mB[a], mBb = t.mB[b];
+    HandCount hc;
+    hc.iAab = static_cast<int>((mAa >> b) & 1ull);
+    hc.iBab = static_cast<int>((mBa >> b) & 1ull);
+    hc.fa = t.isc[0] - t.iuA[a] - t.iuA[b] + hc.iAab;
+    hc.fb = t.isc[1] - t.iuB[a] - t.iuB[b] + hc.iBab;
+    hc.Phh = popc64(mAa & mBa) + popc64(mAa & mBb) + popc64(mAb & mBa) + popc64(mAb & mBb);
+    hc.wd = t.iw[a] + t.iw[b];
+    hc.dd = t.id[a] + t.id[b];
+    return hc;
+}
+
+SSB_CR3_HD long long c2_at(const HandCount &hc, int a, int b, int x, int y, const Tables &t) {
+    const unsigned long long mAa = t.mA[a], mAb = t.mA[b], mBa = t.mB[a], mBb = t.mB[b];
+    const unsigned long long mAx = t.mA[x], mAy = t.mA[y], mBx = t.mB[x], mBy = t.mB[y];
+    const int Aax = static_cast<int>((mAx >> a) & 1ull), Aay = static_cast<int>((mAy >> a) & 1ull);
+    const int Abx = static_cast<int>((mAx >> b) & 1ull), Aby = static_cast<int>((mAy >> b) & 1ull);
+    const int Bax = static_cast<int>((mBx >> a) & 1ull), Bay = static_cast<int>((mBy >> a) & 1ull);
+    const int Bbx = static_cast<int>((mBx >> b) & 1ull), Bby = static_cast<int>((mBy >> b) & 1ull);
+    const int Axy = static_cast<int>((mAx >> y) & 1ull), Bxy = static_cast<int>((mBx >> y) & 1ull);
+    const int Px = popc64(mAx & mBa) + popc64(mAx & mBb) + popc64(mAa & mBx) + popc64(mAb & mBx);
+    const int Py = popc64(mAy & mBa) + popc64(mAy & mBb) + popc64(mAa & mBy) + popc64(mAb & mBy);
+    const int Poo = popc64(mAx & mBx) + popc64(mAx & mBy) + popc64(mAy & mBx) + popc64(mAy & mBy);
+    const long long FAS = hc.fa - t.iuA[x] - t.iuA[y] + Axy + (Aax + Aay + Abx + Aby);
+    const long long FBS = hc.fb - t.iuB[x] - t.iuB[y] + Bxy + (Bax + Bay + Bbx + Bby);
+    const long long ua = t.iuA[a] - hc.iAab - Aax - Aay, ub = t.iuA[b] - hc.iAab - Abx - Aby;
+    const long long ux = t.iuA[x] - Axy - Aax - Abx, uy = t.iuA[y] - Axy - Aay - Aby;
+    const long long va = t.iuB[a] - hc.iBab - Bax - Bay, vb = t.iuB[b] - hc.iBab - Bbx - Bby;
+    const long long vx = t.iuB[x] - Bxy - Bax - Bbx, vy = t.iuB[y] - Bxy - Bay - Bby;
+    const long long QS = t.isc[2] - (hc.wd + t.iw[x] + t.iw[y]) + (hc.Phh + Poo + Px + Py) -
+                         (ua * va + ub * vb + ux * vx + uy * vy);
+    const long long ES = t.isc[3] - (hc.dd + t.id[x] + t.id[y]) + hc.iAab * hc.iBab + Axy * Bxy + Aax * Bax +
+                         Aay * Bay + Abx * Bbx + Aby * Bby;
+    return FAS * FBS - QS + ES;
+}
+
 // the mass of one traverser hand with dense cards (a, b), a board card
 // given as the dummy index (the deck size)
 SSB_CR3_HD double hand_mass(int a, int b, const Tables &t) {
-    const double *A = t.A, *B = t.B, *P = t.P, *PT = t.PT;
-    const double Aab = A[a * kS + b], Bab = B[a * kS + b];
-    const double fa_h = t.sc[0] - t.uA[a] - t.uA[b] + Aab, fb_h = t.sc[1] - t.uB[a] - t.uB[b] + Bab;
-    const double Phh = P[a * kS + a] + P[a * kS + b] + P[b * kS + a] + P[b * kS + b];
-    const double wdh = t.w[a] + t.w[b], ddh = t.d[a] + t.d[b];
-    const double Q = t.sc[2], E = t.sc[3];
+    const HandPart hp = hand_part(a, b, t);
     double mass = 0.0;
     const long long n3 = t.isc[4];
     for (long long k = 0; k < n3; ++k) {
         const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
         if (x == a || x == b || y == a || y == b) continue;   // shares a card with the traverser
-        // cross terms between {a, b} and {x, y}: rows x and y of the
-        // symmetric A, B and of P and P^T
-        const double Aax = A[x * kS + a], Aay = A[y * kS + a], Abx = A[x * kS + b], Aby = A[y * kS + b];
-        const double Bax = B[x * kS + a], Bay = B[y * kS + a], Bbx = B[x * kS + b], Bby = B[y * kS + b];
-        const double Axy = A[x * kS + y], Bxy = B[x * kS + y];
-        const double Px = P[x * kS + a] + P[x * kS + b] + PT[x * kS + a] + PT[x * kS + b];
-        const double Py = P[y * kS + a] + P[y * kS + b] + PT[y * kS + a] + PT[y * kS + b];
-        const double Poo = P[x * kS + x] + P[x * kS + y] + P[y * kS + x] + P[y * kS + y];
-        const double FAS = fa_h - t.uA[x] - t.uA[y] + Axy + (Aax + Aay + Abx + Aby);
-        const double FBS = fb_h - t.uB[x] - t.uB[y] + Bxy + (Bax + Bay + Bbx + Bby);
-        const double ua = t.uA[a] - Aab - Aax - Aay, ub = t.uA[b] - Aab - Abx - Aby;
-        const double ux = t.uA[x] - Axy - Aax - Abx, uy = t.uA[y] - Axy - Aay - Aby;
-        const double va = t.uB[a] - Bab - Bax - Bay, vb = t.uB[b] - Bab - Bbx - Bby;
-        const double vx = t.uB[x] - Bxy - Bax - Bbx, vy = t.uB[y] - Bxy - Bay - Bby;
-        const double QS = Q - (wdh + t.w[x] + t.w[y]) + (Phh + Poo + Px + Py) - (ua * va + ub * vb + ux * vx + uy * vy);
-        const double ES = E - (ddh + t.d[x] + t.d[y]) + Aab * Bab + Axy * Bxy + Aax * Bax + Aay * Bay + Abx * Bbx +
-                          Aby * Bby;
-        mass += t.r3[k] * (FAS * FBS - QS + ES);
+        mass += t.r3[k] * d2_at(hp, a, b, x, y, t);
     }
     return mass;
 }
@@ -219,38 +285,94 @@ SSB_CR3_HD double hand_mass(int a, int b, const Tables &t) {
 // the number of disjoint tuples with positive reach products: the same
 // formula on the 0/1 matrices, exact in integers
 SSB_CR3_HD long long hand_count(int a, int b, const Tables &t) {
-    const unsigned long long mAa = t.mA[a], mAb = t.mA[b], mBa = t.mB[a], mBb = t.mB[b];
-    const int iAab = static_cast<int>((mAa >> b) & 1ull), iBab = static_cast<int>((mBa >> b) & 1ull);
-    const long long fa_h = t.isc[0] - t.iuA[a] - t.iuA[b] + iAab, fb_h = t.isc[1] - t.iuB[a] - t.iuB[b] + iBab;
-    const int Phh = popc64(mAa & mBa) + popc64(mAa & mBb) + popc64(mAb & mBa) + popc64(mAb & mBb);
-    const int wdh = t.iw[a] + t.iw[b], ddh = t.id[a] + t.id[b];
-    const long long Q = t.isc[2], E = t.isc[3];
+    const HandCount hc = hand_count_part(a, b, t);
     long long count = 0;
     const long long n3 = t.isc[4];
     for (long long k = 0; k < n3; ++k) {
         const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
         if (x == a || x == b || y == a || y == b) continue;
-        const unsigned long long mAx = t.mA[x], mAy = t.mA[y], mBx = t.mB[x], mBy = t.mB[y];
-        const int Aax = static_cast<int>((mAx >> a) & 1ull), Aay = static_cast<int>((mAy >> a) & 1ull);
-        const int Abx = static_cast<int>((mAx >> b) & 1ull), Aby = static_cast<int>((mAy >> b) & 1ull);
-        const int Bax = static_cast<int>((mBx >> a) & 1ull), Bay = static_cast<int>((mBy >> a) & 1ull);
-        const int Bbx = static_cast<int>((mBx >> b) & 1ull), Bby = static_cast<int>((mBy >> b) & 1ull);
-        const int Axy = static_cast<int>((mAx >> y) & 1ull), Bxy = static_cast<int>((mBx >> y) & 1ull);
-        const int Px = popc64(mAx & mBa) + popc64(mAx & mBb) + popc64(mAa & mBx) + popc64(mAb & mBx);
-        const int Py = popc64(mAy & mBa) + popc64(mAy & mBb) + popc64(mAa & mBy) + popc64(mAb & mBy);
-        const int Poo = popc64(mAx & mBx) + popc64(mAx & mBy) + popc64(mAy & mBx) + popc64(mAy & mBy);
-        const long long FAS = fa_h - t.iuA[x] - t.iuA[y] + Axy + (Aax + Aay + Abx + Aby);
-        const long long FBS = fb_h - t.iuB[x] - t.iuB[y] + Bxy + (Bax + Bay + Bbx + Bby);
-        const long long ua = t.iuA[a] - iAab - Aax - Aay, ub = t.iuA[b] - iAab - Abx - Aby;
-        const long long ux = t.iuA[x] - Axy - Aax - Abx, uy = t.iuA[y] - Axy - Aay - Aby;
-        const long long va = t.iuB[a] - iBab - Bax - Bay, vb = t.iuB[b] - iBab - Bbx - Bby;
-        const long long vx = t.iuB[x] - Bxy - Bax - Bbx, vy = t.iuB[y] - Bxy - Bay - Bby;
-        const long long QS = Q - (wdh + t.iw[x] + t.iw[y]) + (Phh + Poo + Px + Py) - (ua * va + ub * vb + ux * vx + uy * vy);
-        const long long ES = E - (ddh + t.id[x] + t.id[y]) + iAab * iBab + Axy * Bxy + Aax * Bax + Aay * Bay +
-                             Abx * Bbx + Aby * Bby;
-        count += FAS * FBS - QS + ES;
+        count += c2_at(hc, a, b, x, y, t);
     }
     return count;
+}
+
+// ---------------------------------------------------------------------------
+// four-way showdowns (three live opponents): class masses by rank position
+// ---------------------------------------------------------------------------
+// With the traverser's tie group at rank positions [lo, hi), an opponent
+// hand is weaker (L) below lo and ties (E) inside.  The traverser wins when
+// all three opponents are weaker and splits with the tying ones when none is
+// stronger, so its value is a sum over classes of the reference's
+// coefficient times the mass of the tuples in the class.  Conditioning on
+// the third opponent's class (L or E) and splitting the first two
+// opponents' matrices into their L and E parts gives every class mass as a
+// sum of D2 masses of matrix pairs (X, Y), X, Y in {L, E}; each pair's mass
+// is exact-zeroed by its own count.
+
+// phase 1 for a class pair: A restricted to the first opponent's hands at
+// positions [lo1, hi1), B to the second's at [lo2, hi2) (pos1 / pos2: the
+// opponents' rank positions per hand, -1 for a hand the board blocks)
+template <class T>
+SSB_CR3_HD void phase_gather_cls(int tid, int nt, const Opp3<T> &in, const Tables &t, const int *pos1, int lo1,
+                                 int hi1, const int *pos2, int lo2, int hi2) {
+    for (int i = tid; i < kS * kS; i += nt) {
+        const int c = i / kS, e = i - c * kS;
+        double a = 0.0, b = 0.0;
+        if (c < in.deck && e < in.deck) {
+            const int j1 = in.pair1[c * 52 + e], j2 = in.pair2[c * 52 + e];
+            if (j1 < in.HS && pos1[j1] >= lo1 && pos1[j1] < hi1) a = static_cast<double>(in.r1[j1]);
+            if (j2 < in.HS && pos2[j2] >= lo2 && pos2[j2] < hi2) b = static_cast<double>(in.r2[j2]);
+        }
+        t.A[i] = a;
+        t.B[i] = b;
+    }
+}
+
+// the third opponent's positive-reach live hands in hand order with their
+// rank positions (one item; run once per block)
+template <class T>
+SSB_CR3_HD void compact_third(int tid, const Opp3<T> &in, const Tables &t, const int *pos3, int *p3) {
+    if (tid != 0) return;
+    long long n = 0;
+    double f3 = 0.0;
+    for (int h = 0; h < in.H3; ++h) {
+        const int code = in.code3[h];
+        if ((code & 0x10000) || pos3[h] < 0) continue;
+        const T r = in.r3[h];
+        if (!(r > T(0))) continue;
+        t.r3[n] = static_cast<double>(r);
+        t.xy[n] = static_cast<unsigned short>(((code >> 20) & 63) | (((code >> 26) & 63) << 8));
+        p3[n] = pos3[h];
+        f3 += t.r3[n];
+        ++n;
+    }
+    t.isc[4] = n;
+    t.sc[4] = f3;
+}
+
+// r3 * D2 of the current pair summed over the third opponent's hands:
+// out[0] over positions below lo, out[1] over [lo, hi), out[2] over all;
+// cnt[] the same tuple counts on the 0/1 matrices (only when want_count)
+SSB_CR3_HD void hand_mass_cls(int a, int b, const Tables &t, const int *p3, int lo, int hi, double out[3],
+                              long long cnt[3], bool want_count) {
+    const HandPart hp = hand_part(a, b, t);
+    const HandCount hc = hand_count_part(a, b, t);
+    out[0] = out[1] = out[2] = 0.0;
+    cnt[0] = cnt[1] = cnt[2] = 0;
+    const long long n3 = t.isc[4];
+    for (long long k = 0; k < n3; ++k) {
+        const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
+        if (x == a || x == b || y == a || y == b) continue;
+        const double v = t.r3[k] * d2_at(hp, a, b, x, y, t);
+        const int cls = p3[k] < lo ? 0 : (p3[k] < hi ? 1 : 2);
+        if (cls < 2) out[cls] += v;
+        out[2] += v;
+        if (want_count) {
+            const long long n = c2_at(hc, a, b, x, y, t);
+            if (cls < 2) cnt[cls] += n;
+            cnt[2] += n;
+        }
+    }
 }
 
 // The largest FP64 rounding of hand_mass on a tuple set that is empty: each
@@ -259,6 +381,30 @@ SSB_CR3_HD long long hand_count(int a, int b, const Tables &t) {
 // this bound takes the exact count to decide whether it is 0.
 SSB_CR3_HD double zero_bound(const Tables &t) {
     return 1e-9 * (t.sc[0] + 1.0) * (t.sc[1] + 1.0) * (t.sc[4] + 1.0);
+}
+
+}  // namespace cr3
+}  // namespace ssb
+
+namespace ssb {
+namespace cr3 {
+
+// The traverser's value at a four-way showdown from its class masses:
+// m[pair][cls] with pairs LL, EL, LE, EE (first opponent's class, second's)
+// and cls 0 = third opponent weaker, 1 = tying; total = every tuple's mass.
+// Coefficients as the reference computes them (pot / winners - bet in
+// float, -bet for a loss); a class whose coefficient is 0 adds exactly 0.
+struct Sd3Coef {
+    double win, two, three, four, loss;
+};
+
+SSB_CR3_HD double sd3_value(const double m[4][2], double total, const Sd3Coef &k) {
+    const double win = m[0][0];
+    const double two = (m[1][0] + m[2][0]) + m[0][1];
+    const double three = m[3][0] + (m[1][1] + m[2][1]);
+    const double four = m[3][1];
+    const double loss = total - ((m[0][0] + m[1][0] + m[2][0] + m[3][0]) + (m[0][1] + m[1][1] + m[2][1] + m[3][1]));
+    return k.win * win + k.two * two + k.three * three + k.four * four + k.loss * loss;
 }
 
 }  // namespace cr3

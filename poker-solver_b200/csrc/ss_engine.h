@@ -133,7 +133,8 @@ enum TermKind : int {
     TK_SD2 = 6,      // three-way showdown (two live opponents), ranges without repeated combos
     TK_CR1D = 7,     // TK_CR1 against a range that holds some combo more than once
     TK_CR3 = 8,      // fold / leaf with three counted opponents (large ranges; small ones enumerate)
-    TK_COUNT = 9
+    TK_SD3 = 9,      // four-way showdown (three live opponents), large ranges without repeated combos
+    TK_COUNT = 10
 };
 
 // One terminal for one traverser.  factor: payoff for folds; leaf_off >= 0

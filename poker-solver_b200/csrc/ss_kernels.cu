@@ -1943,6 +1943,147 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     }
 }
 
+// Four-way showdowns (three live opponents): the traverser's class masses
+// (ss_cr3.cuh) in FP64.  One block per (terminal, 256 rank positions), one
+// thread per position (the traverser's hand there, if any).  The block
+// builds the tables of the first two opponents' full matrices once (every
+// tuple's mass, for the loss class and the exact zero), then walks the tie
+// groups that meet its positions and, for a group holding a traverser hand,
+// rebuilds them for the four pairs of the opponents' weaker / tying parts;
+// the group's threads add the third opponent's hands by class.  A class
+// mass within rounding of 0 takes its exact tuple count (0: exactly 0).
+constexpr int kSd3Positions = 1081;   // C(47, 2): rank positions on every river board
+constexpr size_t sd3_smem(int HS) { return cr3_smem(HS) + static_cast<size_t>(HS) * sizeof(int) + 16; }
+
+template <class T>
+__global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                             const TermItem *__restrict__ items, int nchunk,
+                                                             int trav) {
+    extern __shared__ __align__(16) char smem[];
+    const int it = blockIdx.x / nchunk;
+    const int ch = blockIdx.x - it * nchunk;
+    const TermItem I = items[it];
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    const int HS = c.HS;
+    if (HS > c0.HS || c.deck > cr3::kS - 1) return;
+    const size_t hs = static_cast<size_t>(HS);
+    const int tid = threadIdx.x;
+    T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * hs;
+    const int *tpos = c.sd_pos + static_cast<size_t>(trav) * hs;
+    // the first chunk writes the hands without a rank position and the padding
+    if (ch == 0)
+        for (int h = tid; h < HS; h += kTermThreads)
+            if (h >= c.H[trav] || tpos[h] < 0) out[h] = T(0);
+    const int nc = c.ncomb;
+    const int q0 = ch * kTermThreads;
+    if (q0 >= nc) return;
+    const int qend = min(q0 + kTermThreads, nc);
+    Carve cv{smem};
+    cr3::Tables t;
+    t.A = cv.take<double>(cr3::kS * cr3::kS);
+    t.B = cv.take<double>(cr3::kS * cr3::kS);
+    t.P = cv.take<double>(cr3::kS * cr3::kS);
+    t.PT = cv.take<double>(cr3::kS * cr3::kS);
+    t.uA = cv.take<double>(cr3::kS);
+    t.uB = cv.take<double>(cr3::kS);
+    t.w = cv.take<double>(cr3::kS);
+    t.d = cv.take<double>(cr3::kS);
+    t.sc = cv.take<double>(8);
+    t.iuA = cv.take<int>(cr3::kS);
+    t.iuB = cv.take<int>(cr3::kS);
+    t.iw = cv.take<int>(cr3::kS);
+    t.id = cv.take<int>(cr3::kS);
+    t.mA = cv.take<unsigned long long>(cr3::kS);
+    t.mB = cv.take<unsigned long long>(cr3::kS);
+    t.isc = cv.take<long long>(8);
+    t.r3 = cv.take<double>(HS);
+    t.xy = cv.take<unsigned short>(HS);
+    int *p3 = cv.take<int>(HS);
+    const T *reach = reach_rows<T>(c);
+    const int o1 = I.opp_player[0], o2 = I.opp_player[1], o3 = I.opp_player[2];
+    cr3::Opp3<T> in;
+    in.r1 = reach + static_cast<size_t>(I.opp_row[0]) * hs;
+    in.r2 = reach + static_cast<size_t>(I.opp_row[1]) * hs;
+    in.r3 = reach + static_cast<size_t>(I.opp_row[2]) * hs;
+    in.pair1 = c.pair_idx + static_cast<size_t>(o1) * 52 * 52;
+    in.pair2 = c.pair_idx + static_cast<size_t>(o2) * 52 * 52;
+    in.code3 = c.hand_code + static_cast<size_t>(o3) * hs;
+    in.H3 = c.H[o3];
+    in.HS = HS;
+    in.deck = c.deck;
+    const int *posA = c.sd_pos + static_cast<size_t>(o1) * hs;
+    const int *posB = c.sd_pos + static_cast<size_t>(o2) * hs;
+    // this thread's rank position and the traverser's hand there
+    const int q = q0 + tid;
+    const int h = q < qend ? c.pos_hand[static_cast<size_t>(trav) * nc + q] : -1;
+    int a = 0, b = 0, glo = 0, ghi = 0;
+    if (h >= 0) {
+        const int hc = c.hand_code[static_cast<size_t>(trav) * hs + h];
+        a = (hc >> 20) & 63;
+        b = (hc >> 26) & 63;
+        glo = c.sd_combo[q].lo;
+        ghi = c.sd_combo[q].hi;
+    }
+    constexpr int kAll = 1 << 30;
+    auto build = [&](int lo1, int hi1, int lo2, int hi2) {
+        cr3::phase_gather_cls(tid, kTermThreads, in, t, posA, lo1, hi1, posB, lo2, hi2);
+        __syncthreads();
+        cr3::phase_rows(tid, kTermThreads, t);
+        __syncthreads();
+        cr3::phase_product(tid, kTermThreads, t);
+        __syncthreads();
+        cr3::phase_vectors(tid, kTermThreads, in, t, false);
+        __syncthreads();
+        cr3::phase_scalars(tid, t);
+        __syncthreads();
+    };
+    cr3::compact_third(tid, in, t, c.sd_pos + static_cast<size_t>(o3) * hs, p3);
+    build(0, kAll, 0, kAll);
+    double total = 0.0;
+    double o[3];
+    long long cnt[3];
+    if (h >= 0) {
+        cr3::hand_mass_cls(a, b, t, p3, glo, ghi, o, cnt, false);
+        total = o[2];
+        if (fabs(total) <= cr3::zero_bound(t)) {
+            cr3::hand_mass_cls(a, b, t, p3, glo, ghi, o, cnt, true);
+            if (cnt[2] == 0) total = 0.0;
+        }
+    }
+    __syncthreads();
+    double m[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int g = q0; g < qend;) {   // the tie groups meeting [q0, qend), the same walk in every thread
+        const int lo = c.sd_combo[g].lo, hi = c.sd_combo[g].hi;
+        const bool mine = h >= 0 && glo == lo;
+        if (__syncthreads_or(mine)) {
+            // pairs LL, EL, LE, EE of the (first, second) opponent's weaker [0, lo) / tying [lo, hi) hands
+            for (int pr = 0; pr < 4; ++pr) {
+                build((pr & 1) ? lo : 0, (pr & 1) ? hi : lo, (pr & 2) ? lo : 0, (pr & 2) ? hi : lo);
+                if (mine) {
+                    cr3::hand_mass_cls(a, b, t, p3, lo, hi, o, cnt, false);
+                    const double zb = cr3::zero_bound(t);
+                    if (fabs(o[0]) <= zb || fabs(o[1]) <= zb) {
+                        double o2c[3];
+                        cr3::hand_mass_cls(a, b, t, p3, lo, hi, o2c, cnt, true);
+                        for (int k = 0; k < 2; ++k)
+                            if (fabs(o[k]) <= zb && cnt[k] == 0) o[k] = 0.0;
+                    }
+                    m[pr][0] = o[0];
+                    m[pr][1] = o[1];
+                }
+                __syncthreads();
+            }
+        }
+        g = hi;
+    }
+    if (h >= 0) {
+        const cr3::Sd3Coef k{static_cast<double>(I.pot - I.bet), static_cast<double>(I.pot / 2.0f - I.bet),
+                             static_cast<double>(I.pot / 3.0f - I.bet), static_cast<double>(I.pot / 4.0f - I.bet),
+                             -static_cast<double>(I.bet)};
+        out[h] = static_cast<T>(cr3::sd3_value(m, total, k));
+    }
+}
+
 // --------------------------------------------------------------------------
 // best response (FP64): exploitability of an average-strategy profile
 // avg[(di * 8 + a) * max_h + h] (the SSOutput layout)
@@ -2180,6 +2321,15 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
         case TK_ENUM: {
             const int nc = (c.HS + 127) / 128;
             k_term_enum<T><<<n * nc, 128, 0, s>>>(c, ctxs, items, nc, trav);
+            break;
+        }
+        case TK_SD3: {
+            if (c.HS > kMaxHS) return cudaErrorInvalidValue;
+            const int nc = (kSd3Positions + kTermThreads - 1) / kTermThreads;
+            e = cudaFuncSetAttribute(k_term_sd3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(sd3_smem(kMaxHS)));
+            if (e != cudaSuccess) return e;
+            k_term_sd3<T><<<n * nc, kTermThreads, sd3_smem(c.HS), s>>>(c, ctxs, items, nc, trav);
             break;
         }
         case TK_CR3: {

@@ -333,10 +333,10 @@ int build_plan(const Problem &pb, Plan *out) {
                     it.pot = static_cast<float>(n.pot);
                     it.bet = static_cast<float>(n.bets[t]);
                     it.kind_detail = 2;
-                    kind = k == 1 ? TK_SD1
-                           : (k == 2 && !P.dup[t] && !P.dup[it.opp_player[0]] && !P.dup[it.opp_player[1]])
-                               ? TK_SD2
-                               : TK_ENUM;
+                    const bool nodup = !P.dup[t] && !P.dup[it.opp_player[0]] && !P.dup[it.opp_player[1]];
+                    bool large = k == 3;
+                    for (int i = 0; i < k && large; ++i) large = P.H[it.opp_player[i]] >= kCr3MinHands;
+                    kind = k == 1 ? TK_SD1 : (k == 2 && nodup) ? TK_SD2 : (large && nodup) ? TK_SD3 : TK_ENUM;
                     need_sd = true;
                 }
             }

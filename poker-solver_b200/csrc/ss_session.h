@@ -29,7 +29,8 @@ inline int term_class(int kind) {
         case TK_CR1D: return PC_CR1;
         case TK_CR2: return PC_CR2;
         case TK_SD1:
-        case TK_SD2: return PC_SD1;
+        case TK_SD2:
+        case TK_SD3: return PC_SD1;
         case TK_CR3:   // the class of terminals with three or more counted opponents
         default: return PC_ENUM;
     }

@@ -1,9 +1,11 @@
-"""Folds and leaves with three counted opponents (4-player subgames) through
-the closed form k_term_cr3 (ranges of at least 16 hands route there; smaller
-ones enumerate), on the GPU against the oracle:
+"""Terminals with three counted opponents (4-player subgames) through the
+closed forms -- folds and leaves in k_term_cr3, four-way showdowns in
+k_term_sd3 (ranges of at least 16 hands route there; smaller ones
+enumerate) -- on the GPU against the oracle:
 * a 4-player river (125 nodes; 18 and 24 hands, a repeated combo in one
-  range that keeps some terminals on enumeration): the solver against the
-  FP32 oracle at the strict tolerances of the parity tests;
+  range that keeps some terminals on enumeration, a royal-flush board where
+  every showdown splits): the solver against the FP32 oracle at the strict
+  tolerances of the parity tests;
 * a 4-player turn with continuation leaves (5,681 nodes, 16 hands): folds
   and leaves with three counted opponents, against the FP32 oracle;
 * the FP64 best response, whose 4-player deal mass also takes the closed
@@ -18,6 +20,7 @@ import numpy as np
 import pytest
 
 import workloads as wl
+from cards import card_to_int
 from test_exploitability_gpu import gpu_exploitability
 from test_parity_gpu import solve, strict
 
@@ -46,6 +49,15 @@ def test_four_player_river(oracle, seed, hands, iters, dup):
     cfg = four_player("river6", seed, hands, dup)
     ours, lv = solve(cfg, iters)
     strict(ours, oracle_f32(oracle, cfg, iters, lv))
+
+
+def test_four_player_river_every_hand_ties(oracle):
+    # a royal flush on the board: every showdown is a split of all live players
+    cfg = wl.config("river6", seed=26, num_hands=18, num_players=4, bet_sizes=[1.0], max_raises=1)
+    cfg["board"] = [card_to_int(x) for x in ("Ts", "Js", "Qs", "Ks", "As")]
+    cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(26), cfg["board"], 4, 18)
+    ours, lv = solve(cfg, 4)
+    strict(ours, oracle_f32(oracle, cfg, 4, lv))
 
 
 def test_four_player_turn_with_leaves(oracle):

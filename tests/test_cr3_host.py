@@ -1,13 +1,19 @@
-"""Host check of the three-counted-opponent closed form (k_term_cr3, the
-block phases of poker-solver_b200/csrc/ss_cr3.cuh): the phases compiled
-with g++ into tests/native/cr3_emul and run one after another over 256
-emulated threads, against brute-force enumeration of the pairwise disjoint
-opponent tuples for every traverser hand (the reference's rule,
-street_solve.cu:771-823): the FP64 mass to 1e-12 relative, the integer
-tuple count exactly, and exact zeros for hands without a tuple of positive
-products -- on full-size decks (turn 48, river 47, flop 49 cards), with
-zeroed weights, a range the board touches, an opponent without positive
-reach, and tiny decks where most hands have no disjoint tuple."""
+"""Host check of the three-opponent closed forms (k_term_cr3 and
+k_term_sd3, the block phases of poker-solver_b200/csrc/ss_cr3.cuh): the
+phases compiled with g++ (tests/native/cr3_emul, sd3_emul) and run one after
+another over 256 emulated threads, against brute-force enumeration of the
+pairwise disjoint opponent tuples for every traverser hand (the reference's
+rules, street_solve.cu:771-823 folds, :936-1002 showdowns):
+* folds / leaves: the FP64 mass to 1e-12 relative, the integer tuple count
+  exactly, and exact zeros for hands without a tuple of positive products --
+  on full-size decks (turn 48, river 47, flop 49 cards), with zeroed
+  weights, a range the board touches, an opponent without positive reach,
+  and tiny decks where most hands have no disjoint tuple;
+* four-way showdowns: every class mass (win, 2-, 3-, 4-way ties, per pair of
+  the first two opponents' weaker / tying parts and the third opponent's
+  class) and the value, with ties from few rank levels up to every hand
+  tying, a pot / 3 equal to the bet, and a bet of 0; counts exact and the
+  classes without a tuple exactly 0."""
 import json
 import os
 import shutil
@@ -19,15 +25,39 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-@pytest.fixture(scope="module")
-def emul(tmp_path_factory):
+def _build(tmp_path_factory, name):
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    out = str(tmp_path_factory.mktemp("cr3") / "cr3_emul")
+    out = str(tmp_path_factory.mktemp("cr3") / name)
     subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
                     "-I", os.path.join(ROOT, "poker-solver_b200", "csrc"),
-                    os.path.join(HERE, "native", "cr3_emul.cpp"), "-o", out], check=True)
+                    os.path.join(HERE, "native", name + ".cpp"), "-o", out], check=True)
     return out
+
+
+@pytest.fixture(scope="module")
+def emul(tmp_path_factory):
+    return _build(tmp_path_factory, "cr3_emul")
+
+
+@pytest.fixture(scope="module")
+def sd3(tmp_path_factory):
+    return _build(tmp_path_factory, "sd3_emul")
+
+
+@pytest.mark.parametrize("args", [
+    (1, 47, 20, 0.3, 6, 100, 25),     # river deck, some ties
+    (2, 48, 24, 0.0, 3, 150, 50),     # few rank levels: many ties
+    (3, 10, 30, 0.2, 2, 75, 25),      # pot / 3 equals the bet: 3-way ties pay exactly 0
+    (4, 8, 20, 0.0, 1, 90, 30),       # every hand ties
+    (5, 47, 18, 0.5, 40, 300, 0),     # a bet of 0: losses pay exactly 0
+])
+def test_four_way_showdown_classes_against_enumeration(sd3, args):
+    r = subprocess.run([sd3] + [str(a) for a in args], check=True, capture_output=True, text=True)
+    d = json.loads(r.stdout)
+    assert d["zero_bad"] == 0
+    assert d["max_rel_err"] <= 1e-12
+    assert d["hands"] > 0 and d["empty_classes"] > 0
 
 
 @pytest.mark.parametrize("args,min_zero", [

@@ -108,7 +108,7 @@ def test_one_wave_cap(driver):
 
 
 # TermKind values (ss_engine.h)
-ZERO, LEAF0, CR1, CR2, SD1, ENUM, SD2, CR1D, CR3 = range(9)
+ZERO, LEAF0, CR1, CR2, SD1, ENUM, SD2, CR1D, CR3, SD3 = range(10)
 FOLD, SHOWDOWN, LEAF = 1, 2, 4
 CR3_MIN_HANDS = 16   # kCr3MinHands
 
@@ -121,8 +121,9 @@ def expected_kinds(d, np_, river, leaves):
     range and anything else with 3+ counted opponents exact enumeration --
     except folds and leaves with exactly three, which take the conditioning
     closed form when every counted range holds at least 16 hands and the
-    first two repeat no combo."""
-    want = [[0] * 9 for _ in range(np_)]
+    first two repeat no combo, and four-way showdowns, which take theirs on
+    the same condition with the traverser's range repeating no combo either."""
+    want = [[0] * 10 for _ in range(np_)]
     dup = d["dup"]
     nh = d["hands"]
     for typ, leaf_idx, active in d["terminals"]:
@@ -136,8 +137,9 @@ def expected_kinds(d, np_, river, leaves):
                 kind = (LEAF0 if k == 0 else (CR1D if dup[opp[0]] else CR1) if k == 1
                         else CR2 if k == 2 else CR3 if cr3 else ENUM)
             elif typ == SHOWDOWN and river and active[t]:
-                kind = (SD1 if k == 1 else SD2 if k == 2 and not (dup[t] or dup[opp[0]] or dup[opp[1]])
-                        else ENUM)
+                nodup = k >= 2 and not (dup[t] or dup[opp[0]] or dup[opp[1]])
+                sd3 = k == 3 and nodup and all(nh[o] >= CR3_MIN_HANDS for o in opp)
+                kind = SD1 if k == 1 else SD2 if k == 2 and nodup else SD3 if sd3 else ENUM
             want[t][kind] += 1
     return want
 
