@@ -64,10 +64,11 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS),
                     help="subgame of the plain form (the CPU baseline and reference arm cover turn3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf,turn4",
+    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf,four",
                     help="comma list of plain (the headline), batched, served, hu_river (the heads-up river "
                          "beside the reference's CPU solver), leaf (the turn subgame's continuation values "
-                         "produced on the GPU), turn4 (a full-range 4-player turn, three-opponent terminals)")
+                         "produced on the GPU), four (full-range 4-player turn and river, three-opponent "
+                         "terminals)")
     ap.add_argument("--batch-size", type=int, default=512, help="batched form: mixed requests in one batch")
     ap.add_argument("--rate", type=float, default=100.0, help="served form: requests per second")
     ap.add_argument("--duration", type=float, default=3.0, help="served form: seconds of arrivals")
@@ -600,36 +601,41 @@ def run_leaf_producer(seed, calls=3):
                                        f"({bias_s:.2f} s), scaled"}}
 
 
-def run_turn4(seed, device, short=5, long=15):
-    """A 4-player turn subgame with full ranges: 1128 combos per player with
-    U(0,1) weights, pot 150, stacks 500, bets {1.0 pot} + all-in, one raise,
-    continuation leaves with N(0, 0.3 pot) values (5,681 nodes).  Its folds
-    and leaves with three counted opponents take the closed form
-    k_term_cr3.  Time per iteration from solves of `short` and `long`
-    iterations through ss_solve_gpu_ex (their difference removes the set-up
-    and the output copy)."""
+def run_four_player(seed, device, short=5, long=15):
+    """4-player subgames with full ranges, whose terminals with three counted
+    opponents take the closed forms (folds and leaves: k_term_cr3, four-way
+    showdowns: k_term_sd3): a turn with continuation leaves (1128 combos per
+    player, U(0,1) weights with 30% zeroed, pot 150, stacks 500, bets {1.0
+    pot} + all-in, one raise, leaf values N(0, 0.3 pot); 5,681 nodes) and a
+    river (1081 combos per player, U(0,1) weights, pot 300, stacks 1000, the
+    same bets; 125 nodes).  Time per iteration from solves of `short` and
+    `long` iterations through ss_solve_gpu_ex (their difference removes the
+    set-up and the output copy)."""
     import workloads as wl
-    cfg = wl.config("turn3", seed=seed, num_players=4, bet_sizes=[1.0], max_raises=1)
-    cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(seed + 4), cfg["board"], 4, None,
-                                                  zero_frac=0.3)
-    sg = wl.AbiSubgame(cfg)
-    try:
-        sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
-        walls = {}
-        for iters in (short, short, long):
-            t0 = time.perf_counter()
-            rc, _ = sg.solve(iters, device=device)
-            walls[iters] = time.perf_counter() - t0
-            if rc != 0:
-                raise RuntimeError(f"ss_solve_gpu failed ({rc}): {wl.ssg.last_error(sg.lib)}")
-        nodes, nh = sg.td.num_nodes, [len(h) for h in cfg["hands"]]
-    finally:
-        sg.free()
-    per_it = (walls[long] - walls[short]) / (long - short)
-    return {"workload": "4-player turn, 1128 combos per player, bets {1.0} + all-in, 1 raise, continuation leaves",
-            "tree_nodes": nodes, "ms_per_iteration": 1e3 * per_it,
-            "node_hand_updates_per_s": nodes * sum(nh) / per_it if per_it > 0 else None,
-            "solve_1000_iterations_s_est": 1000 * per_it, "sample": f"solves of {short} and {long} iterations"}
+    out = {}
+    for street, name in (("turn", "turn3"), ("river", "river6")):
+        cfg = wl.config(name, seed=seed, num_players=4, bet_sizes=[1.0], max_raises=1)
+        cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(seed + 4), cfg["board"], 4, None,
+                                                      zero_frac=0.3 if street == "turn" else 0.0)
+        sg = wl.AbiSubgame(cfg)
+        try:
+            sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
+            walls = {}
+            for iters in (short, short, long):
+                t0 = time.perf_counter()
+                rc, _ = sg.solve(iters, device=device)
+                walls[iters] = time.perf_counter() - t0
+                if rc != 0:
+                    raise RuntimeError(f"ss_solve_gpu failed ({rc}): {wl.ssg.last_error(sg.lib)}")
+            nodes, nh = sg.td.num_nodes, [len(h) for h in cfg["hands"]]
+        finally:
+            sg.free()
+        per_it = (walls[long] - walls[short]) / (long - short)
+        out[street] = {"tree_nodes": nodes, "hands": nh[0], "ms_per_iteration": 1e3 * per_it,
+                       "node_hand_updates_per_s": nodes * sum(nh) / per_it if per_it > 0 else None,
+                       "solve_1000_iterations_s_est": 1000 * per_it}
+    out["sample"] = f"solves of {short} and {long} iterations each"
+    return out
 
 
 def cpu_model():
@@ -811,12 +817,12 @@ def main():
             leaf = run_leaf_producer(args.seed)
         except Exception as e:  # the solver's line is printed whatever happens here
             leaf = {"error": f"{type(e).__name__}: {e}"}
-    turn4 = None
-    if rank == 0 and world == 1 and "turn4" in forms:
+    four = None
+    if rank == 0 and world == 1 and "four" in forms:
         try:
-            turn4 = run_turn4(args.seed, local)
+            four = run_four_player(args.seed, local)
         except Exception as e:  # the solver's line is printed whatever happens here
-            turn4 = {"error": f"{type(e).__name__}: {e}"}
+            four = {"error": f"{type(e).__name__}: {e}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "turn3":
         r = reference_cpu(args.seed, budget_s=20.0)
@@ -842,7 +848,7 @@ def main():
             "node_hand_updates_per_s": res["value"] * res["nhu_per_solve"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
-            "batched": batched, "served": served, "hu_river": hu, "leaf_producer": leaf, "turn4": turn4,
+            "batched": batched, "served": served, "hu_river": hu, "leaf_producer": leaf, "four_player": four,
         }
         print(json.dumps(line))
     try:
