@@ -2324,7 +2324,8 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             break;
         }
         case TK_SD3: {
-            if (c.HS > kMaxHS) return cudaErrorInvalidValue;
+            // the grid covers the 1081 rank positions of a river board
+            if (c.HS > kMaxHS || c.ncomb > kSd3Positions) return cudaErrorInvalidValue;
             const int nc = (kSd3Positions + kTermThreads - 1) / kTermThreads;
             e = cudaFuncSetAttribute(k_term_sd3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(sd3_smem(kMaxHS)));
