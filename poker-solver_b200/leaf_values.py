@@ -15,7 +15,9 @@ when it cannot (no library, no CUDA device).  What stays in Python is the
 reference's own host logic: the runout draws with numpy's RandomState and
 the leaf descriptors read from the tree.  The blueprint-driven producer
 (compute_flop_leaf_values) and the strategy-biasing helpers are not part
-of this path."""
+of this path.  One difference: a range holding more hands than max_hands
+raises ValueError up front (the reference fails with an IndexError once
+such a hand is live)."""
 import ctypes
 from collections import namedtuple
 from typing import List, Optional, Tuple
