@@ -9,8 +9,11 @@
 * the kernels' per-element functions, compiled for the host with g++ into
   tests/native/leaf_emul and run phase by phase over the library's plan,
   reproduce the reference module's leaf values bit for bit
-  (tests/golden/leaf_values_*.npz) and the oracle's on edge cases (an empty
-  range, a range the board blocks entirely, no runouts);
+  (tests/golden/leaf_values_*.npz), the oracle's on edge cases (an empty
+  range, a range the board blocks entirely, no runouts), and the oracle's
+  numpy form at size (a 3-player turn with 1128 hands, six players with
+  sampled 5-tuples, a 3-player flop with every runout);
+* the leaf descriptors of a 4-player tree match the oracle's walk;
 * malformed inputs are refused before any CUDA call, and a valid call on a
   machine without a GPU raises instead of falling back to the CPU."""
 import glob
@@ -209,3 +212,34 @@ def test_no_cpu_fallback_without_a_gpu():
     ph = [[(20, 21, 1.0), (22, 23, 1.0)], [(24, 25, 1.0)]]
     with pytest.raises(RuntimeError, match="ss_leaf_values_gpu failed"):
         lv.compute_turn_leaf_values(board, [lv.LeafInfo(0, 100, (10, 10))], 2, 100, player_hands=ph)
+
+
+def test_descriptors_of_a_four_player_tree():
+    cfg = wl.config("turn3", seed=24, num_hands=16, num_players=4, bet_sizes=[1.0], max_raises=1)
+    cfg["hands"], cfg["weights"] = wl.make_ranges(np.random.default_rng(24), cfg["board"], 4, 16)
+    sg = wl.AbiSubgame(cfg)
+    try:
+        got = lv.extract_leaf_info_from_tree(sg.td, 4)
+        want = leaf_oracle.leaf_infos(sg.td, 4)
+    finally:
+        sg.free()
+    assert len(got) > 0
+    assert [(i.leaf_idx, i.pot, i.bets) for i in got] == want
+
+
+@pytest.mark.parametrize("seed,num_board,players,hands", [
+    (2, 4, 3, None),     # 3-player turn, 1128 hands: 12 river cards, 2000 sampled opponent pairs
+    (5, 4, 6, 60),       # 6 players: 2000 sampled opponent 5-tuples
+    (7, 3, 3, 30),       # 3-player flop, small ranges: every turn and river card
+])
+def test_element_functions_at_size_against_numpy_oracle(emul, tmp_path, seed, num_board, players, hands):
+    rng = np.random.default_rng(seed)
+    board = [int(c) for c in rng.permutation(52)[:num_board]]
+    hs, ws = wl.make_ranges(rng, board, players, hands)
+    ph = [[(int(h[0]), int(h[1]), float(w)) for h, w in zip(hs[p], ws[p])] for p in range(players)]
+    infos = [(i, int(p)) for i, p in enumerate(rng.integers(60, 900, 3))]
+    mh = max(len(h) for h in hs)
+    runs = runouts_for(board, ph)
+    want = leaf_oracle.leaf_values_vectorised(board, runs, [(i, p, ()) for i, p in infos], mh, ph)
+    got = emulate(emul, tmp_path, board, runs, infos, mh, ph)
+    assert np.array_equal(got, want)
