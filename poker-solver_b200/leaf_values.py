@@ -62,7 +62,7 @@ class SSLeafValueInput(ctypes.Structure):
 
 def _library():
     # the entry point is the same in both builds: reuse one that is loaded already
-    lib = next(iter(ssg._LIBS.values()), None) or ssg.load_library()
+    lib = ssg.loaded_library() or ssg.load_library()
     if not getattr(lib, "_leaf_bound", False):
         ip = ctypes.POINTER(ctypes.c_int)
         lib.ss_leaf_values_gpu.restype = ctypes.c_int

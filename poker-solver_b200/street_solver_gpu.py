@@ -181,6 +181,12 @@ def load_library(max_hands=SS_MAX_HANDS):
     return lib
 
 
+def loaded_library():
+    """A library build already loaded in this process (either layout), or
+    None -- for entry points that do not depend on SS_MAX_HANDS."""
+    return next(iter(_LIBS.values()), None)
+
+
 def last_error(lib):
     msg = lib.ss_last_error()
     return msg.decode() if msg else ""
