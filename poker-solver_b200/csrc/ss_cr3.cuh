@@ -29,6 +29,7 @@
 // tests/native/cr3_emul.cpp).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #if defined(__CUDACC__)
@@ -405,6 +406,101 @@ SSB_CR3_HD double sd3_value(const double m[4][2], double total, const Sd3Coef &k
     const double four = m[3][1];
     const double loss = total - ((m[0][0] + m[1][0] + m[2][0] + m[3][0]) + (m[0][1] + m[1][1] + m[2][1] + m[3][1]));
     return k.win * win + k.two * two + k.three * three + k.four * four + k.loss * loss;
+}
+
+}  // namespace cr3
+}  // namespace ssb
+
+namespace ssb {
+namespace cr3 {
+
+// ---------------------------------------------------------------------------
+// per-thread steps of the four-way showdown block (k_term_sd3), shared with
+// the host check: the kernel runs them between its barriers
+// ---------------------------------------------------------------------------
+
+struct Sd3Thread {
+    int h;               // the traverser's hand at this thread's rank position, -1 if none
+    int a, b;            // its dense cards
+    int glo, ghi;        // its tie group [glo, ghi)
+    double total;        // every tuple's mass (third opponent of any class)
+    double m[4][2];      // class masses: pairs LL, EL, LE, EE x third opponent weaker / tying
+};
+
+// the thread at rank position q (q < qend): hand, cards and tie group from
+// the showdown tables (pos_hand [np][ncomb], hand codes, SdCombo groups)
+template <class Combo>
+SSB_CR3_HD void sd3_thread_init(int q, int qend, const int *pos_hand_t, const int *hand_code_t,
+                                const Combo *sd_combo, Sd3Thread &s) {
+    s.h = q < qend ? pos_hand_t[q] : -1;
+    s.a = s.b = s.glo = s.ghi = 0;
+    s.total = 0.0;
+    for (int p = 0; p < 4; ++p) s.m[p][0] = s.m[p][1] = 0.0;
+    if (s.h >= 0) {
+        const int hc = hand_code_t[s.h];
+        s.a = (hc >> 20) & 63;
+        s.b = (hc >> 26) & 63;
+        s.glo = sd_combo[q].lo;
+        s.ghi = sd_combo[q].hi;
+    }
+}
+
+// after the full pair's tables: the total, exact 0 when no tuple exists
+SSB_CR3_HD void sd3_thread_total(Sd3Thread &s, const Tables &t, const int *p3) {
+    if (s.h < 0) return;
+    double o[3];
+    long long cnt[3];
+    hand_mass_cls(s.a, s.b, t, p3, s.glo, s.ghi, o, cnt, false);
+    s.total = o[2];
+    if (fabs(s.total) <= zero_bound(t)) {
+        hand_mass_cls(s.a, s.b, t, p3, s.glo, s.ghi, o, cnt, true);
+        if (cnt[2] == 0) s.total = 0.0;
+    }
+}
+
+// the first / second opponent's position ranges of pair pr (LL, EL, LE, EE)
+// for the tie group [lo, hi): weaker [0, lo), tying [lo, hi)
+SSB_CR3_HD void sd3_pair_bounds(int pr, int lo, int hi, int *lo1, int *hi1, int *lo2, int *hi2) {
+    *lo1 = (pr & 1) ? lo : 0;
+    *hi1 = (pr & 1) ? hi : lo;
+    *lo2 = (pr & 2) ? lo : 0;
+    *hi2 = (pr & 2) ? hi : lo;
+}
+
+// after pair pr's tables, for a thread of the group [lo, hi): its two class
+// masses, each exact 0 when its count is 0
+SSB_CR3_HD void sd3_thread_pair(Sd3Thread &s, const Tables &t, const int *p3, int pr, int lo, int hi) {
+    double o[3];
+    long long cnt[3];
+    hand_mass_cls(s.a, s.b, t, p3, lo, hi, o, cnt, false);
+    const double zb = zero_bound(t);
+    if (fabs(o[0]) <= zb || fabs(o[1]) <= zb) {
+        double oc[3];
+        hand_mass_cls(s.a, s.b, t, p3, lo, hi, oc, cnt, true);
+        for (int k = 0; k < 2; ++k)
+            if (fabs(o[k]) <= zb && cnt[k] == 0) o[k] = 0.0;
+    }
+    s.m[pr][0] = o[0];
+    s.m[pr][1] = o[1];
+}
+
+// the value from the class masses, with the reference's float coefficients
+SSB_CR3_HD double sd3_thread_value(const Sd3Thread &s, float pot, float bet) {
+    const Sd3Coef k{static_cast<double>(pot - bet), static_cast<double>(pot / 2.0f - bet),
+                    static_cast<double>(pot / 3.0f - bet), static_cast<double>(pot / 4.0f - bet),
+                    -static_cast<double>(bet)};
+    return sd3_value(s.m, s.total, k);
+}
+
+// the three-opponent fold / leaf mass of a traverser hand from its hand code
+// (a board card maps to the zero dummy row `deck`), exact 0 without a tuple
+SSB_CR3_HD double cr3_hand_value_mass(int hand_code, int deck, const Tables &t) {
+    int a = (hand_code >> 20) & 63, b = (hand_code >> 26) & 63;
+    if (a >= deck) a = deck;
+    if (b >= deck) b = deck;
+    double m = hand_mass(a, b, t);
+    if (fabs(m) <= zero_bound(t) && hand_count(a, b, t) == 0) m = 0.0;
+    return m;
 }
 
 }  // namespace cr3

@@ -1931,12 +1931,7 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
         for (int g = 0; g < ng; ++g) val[static_cast<size_t>(I0[g].node) * hs + h] = T(0);
         return;
     }
-    const int hc = c.hand_code[static_cast<size_t>(trav) * hs + h];
-    int a = (hc >> 20) & 63, b = (hc >> 26) & 63;
-    if (a >= c.deck) a = c.deck;   // a board card: the zero dummy row
-    if (b >= c.deck) b = c.deck;
-    double m = cr3::hand_mass(a, b, t);
-    if (fabs(m) <= cr3::zero_bound(t) && cr3::hand_count(a, b, t) == 0) m = 0.0;
+    const double m = cr3::cr3_hand_value_mass(c.hand_code[static_cast<size_t>(trav) * hs + h], c.deck, t);
     for (int g = 0; g < ng; ++g) {
         const TermItem &Ig = I0[g];
         val[static_cast<size_t>(Ig.node) * hs + h] = static_cast<T>(static_cast<double>(term_factor(c, Ig, h)) * m);
@@ -2014,16 +2009,9 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     const int *posA = c.sd_pos + static_cast<size_t>(o1) * hs;
     const int *posB = c.sd_pos + static_cast<size_t>(o2) * hs;
     // this thread's rank position and the traverser's hand there
-    const int q = q0 + tid;
-    const int h = q < qend ? c.pos_hand[static_cast<size_t>(trav) * nc + q] : -1;
-    int a = 0, b = 0, glo = 0, ghi = 0;
-    if (h >= 0) {
-        const int hc = c.hand_code[static_cast<size_t>(trav) * hs + h];
-        a = (hc >> 20) & 63;
-        b = (hc >> 26) & 63;
-        glo = c.sd_combo[q].lo;
-        ghi = c.sd_combo[q].hi;
-    }
+    cr3::Sd3Thread st;
+    cr3::sd3_thread_init(q0 + tid, qend, c.pos_hand + static_cast<size_t>(trav) * nc,
+                         c.hand_code + static_cast<size_t>(trav) * hs, c.sd_combo, st);
     constexpr int kAll = 1 << 30;
     auto build = [&](int lo1, int hi1, int lo2, int hi2) {
         cr3::phase_gather_cls(tid, kTermThreads, in, t, posA, lo1, hi1, posB, lo2, hi2);
@@ -2039,49 +2027,23 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     };
     cr3::compact_third(tid, in, t, c.sd_pos + static_cast<size_t>(o3) * hs, p3);
     build(0, kAll, 0, kAll);
-    double total = 0.0;
-    double o[3];
-    long long cnt[3];
-    if (h >= 0) {
-        cr3::hand_mass_cls(a, b, t, p3, glo, ghi, o, cnt, false);
-        total = o[2];
-        if (fabs(total) <= cr3::zero_bound(t)) {
-            cr3::hand_mass_cls(a, b, t, p3, glo, ghi, o, cnt, true);
-            if (cnt[2] == 0) total = 0.0;
-        }
-    }
+    cr3::sd3_thread_total(st, t, p3);
     __syncthreads();
-    double m[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     for (int g = q0; g < qend;) {   // the tie groups meeting [q0, qend), the same walk in every thread
         const int lo = c.sd_combo[g].lo, hi = c.sd_combo[g].hi;
-        const bool mine = h >= 0 && glo == lo;
+        const bool mine = st.h >= 0 && st.glo == lo;
         if (__syncthreads_or(mine)) {
-            // pairs LL, EL, LE, EE of the (first, second) opponent's weaker [0, lo) / tying [lo, hi) hands
             for (int pr = 0; pr < 4; ++pr) {
-                build((pr & 1) ? lo : 0, (pr & 1) ? hi : lo, (pr & 2) ? lo : 0, (pr & 2) ? hi : lo);
-                if (mine) {
-                    cr3::hand_mass_cls(a, b, t, p3, lo, hi, o, cnt, false);
-                    const double zb = cr3::zero_bound(t);
-                    if (fabs(o[0]) <= zb || fabs(o[1]) <= zb) {
-                        double o2c[3];
-                        cr3::hand_mass_cls(a, b, t, p3, lo, hi, o2c, cnt, true);
-                        for (int k = 0; k < 2; ++k)
-                            if (fabs(o[k]) <= zb && cnt[k] == 0) o[k] = 0.0;
-                    }
-                    m[pr][0] = o[0];
-                    m[pr][1] = o[1];
-                }
+                int lo1, hi1, lo2, hi2;
+                cr3::sd3_pair_bounds(pr, lo, hi, &lo1, &hi1, &lo2, &hi2);
+                build(lo1, hi1, lo2, hi2);
+                if (mine) cr3::sd3_thread_pair(st, t, p3, pr, lo, hi);
                 __syncthreads();
             }
         }
         g = hi;
     }
-    if (h >= 0) {
-        const cr3::Sd3Coef k{static_cast<double>(I.pot - I.bet), static_cast<double>(I.pot / 2.0f - I.bet),
-                             static_cast<double>(I.pot / 3.0f - I.bet), static_cast<double>(I.pot / 4.0f - I.bet),
-                             -static_cast<double>(I.bet)};
-        out[h] = static_cast<T>(cr3::sd3_value(m, total, k));
-    }
+    if (st.h >= 0) out[st.h] = static_cast<T>(cr3::sd3_thread_value(st, I.pot, I.bet));
 }
 
 // --------------------------------------------------------------------------

@@ -13,7 +13,12 @@ rules, street_solve.cu:771-823 folds, :936-1002 showdowns):
   the first two opponents' weaker / tying parts and the third opponent's
   class) and the value, with ties from few rank levels up to every hand
   tying, a pot / 3 equal to the bet, and a bet of 0; counts exact and the
-  classes without a tuple exactly 0."""
+  classes without a tuple exactly 0;
+* both kernels' blocks driven by the planner's own work items and tables
+  for seeded 4-player rivers and a 4-player turn (tests/native/term3_emul,
+  with ss_plan.cpp and ss_tree.cpp): hand codes, pair tables, rank
+  positions, tie-group walk and term groups, every traverser hand against
+  enumeration with the planner's strengths, to 1e-12."""
 import json
 import os
 import shutil
@@ -76,3 +81,29 @@ def test_closed_form_against_enumeration(emul, args, min_zero):
     assert d["max_rel_err"] <= 1e-12
     assert d["zero_bad"] == 0
     assert d["zero_hands"] >= min_zero
+
+
+@pytest.fixture(scope="module")
+def term3(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    out = str(tmp_path_factory.mktemp("cr3") / "term3_emul")
+    csrc = os.path.join(ROOT, "poker-solver_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"), "-I", csrc,
+                    os.path.join(HERE, "native", "term3_emul.cpp"), os.path.join(csrc, "ss_plan.cpp"),
+                    os.path.join(csrc, "ss_tree.cpp"), "-o", out], check=True)
+    return out
+
+
+@pytest.mark.parametrize("args", [
+    (1, 5, 20, 0.2, 20),     # 4-player river: three-opponent folds and four-way showdowns
+    (2, 5, 24, 0.0, 20),
+    (4, 5, 30, 0.5, 10),     # half the reach rows' entries zero
+    (3, 4, 18, 0.3, 12),     # 4-player turn: folds and grouped continuation leaves
+])
+def test_kernel_blocks_on_planned_items(term3, args):
+    r = subprocess.run([term3] + [str(a) for a in args], check=True, capture_output=True, text=True)
+    d = json.loads(r.stdout)
+    assert d["items"] > 0 and d["hands"] > 0
+    assert d["max_rel_err"] <= 1e-12
+    assert d["zero_bad"] == 0
