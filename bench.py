@@ -601,7 +601,7 @@ def run_leaf_producer(seed, calls=3):
                                        f"({bias_s:.2f} s), scaled"}}
 
 
-def run_four_player(seed, device, short=5, long=15):
+def run_four_player(seed, device, short=3, long=8):
     """4-player subgames with full ranges, whose terminals with three counted
     opponents take the closed forms (folds and leaves: k_term_cr3, four-way
     showdowns: k_term_sd3): a turn with continuation leaves (1128 combos per
