@@ -15,6 +15,10 @@ reference's build system:
   libref_street_solve_gpu.so  src/cuda/street_solve.cu unmodified, nvcc sm_100a
                               (stock limits: 200 hands, 3 raises); for parity runs
                               on a B200 at <= 200 hands.
+  wrapper/python/             python/street_solver_gpu.py and python/solver.py,
+                              copied unmodified: the reference's own ctypes
+                              consumer of the C ABI, which the drop-in test runs
+                              against this repository's library.
 
 Everything generated lands under oracle/_ref/, which git ignores.
 """
@@ -105,6 +109,19 @@ def build_gpu():
     return out
 
 
+def build_wrapper():
+    """The reference's Python consumer of the C ABI, unmodified (it imports
+    card helpers from solver.py and loads <root>/build/street_solve.so)."""
+    out = os.path.join(OUT, "wrapper", "python")
+    os.makedirs(out, exist_ok=True)
+    for name in ("street_solver_gpu.py", "solver.py"):
+        src = os.path.join(REF, "python", name)
+        dst = os.path.join(out, name)
+        if not _fresh(dst, [src]):
+            shutil.copyfile(src, dst)
+    return out
+
+
 def main():
     if not os.path.isdir(os.path.join(REF, "src", "cuda")):
         print(f"reference sources not found under {REF}; nothing to build", file=sys.stderr)
@@ -114,6 +131,7 @@ def main():
     for h, r in VARIANTS:
         built.append(build_shim(h, r))
     built.append(build_gpu())
+    built.append(build_wrapper())
     for b in built:
         if b:
             print(os.path.relpath(b, HERE))

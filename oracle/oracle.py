@@ -150,6 +150,7 @@ class Oracle:
         L.orc_eval7_cards.restype = ctypes.c_uint32
         L.orc_solve_f32.restype = ctypes.c_int
         L.orc_solve_f64.restype = ctypes.c_int
+        L.orc_solve_f64_closed.restype = ctypes.c_int
         L.orc_exploitability.restype = ctypes.c_double
         L.orc_profile_cfv.restype = ctypes.c_int
 
@@ -202,7 +203,8 @@ class Oracle:
         reg = np.zeros(N * MAX_ACTIONS * max_h, dt) if want_state else None
         ssum = np.zeros(N * MAX_ACTIONS * max_h, dt) if want_state else None
         t, keep = _tree_to_orc(tree)
-        fn = self.lib.orc_solve_f32 if precision == "f32" else self.lib.orc_solve_f64
+        fn = {"f32": self.lib.orc_solve_f32, "f64": self.lib.orc_solve_f64,
+              "f64_closed": self.lib.orc_solve_f64_closed}[precision]
         rc = fn(ctypes.byref(t), _i32p(hands), _f32p(weights), _i32p(nh), _f32p(lv), _i32p(fz),
                 iterations, ptr(rs), ptr(rev), ptr(avg), _i32p(ids), ptr(reg), ptr(ssum))
         del keep, root

@@ -367,6 +367,17 @@ uint32_t orc_eval7_cards(const int *cards7) { return orc_eval7(cards7); }
 #undef RSUF
 #undef RLIT
 
+int orc_solve_f64_closed(const OrcTree *t, const int *hands, const float *weights,
+                         const int *num_hands, const float *leaf_values, const int *frozen,
+                         int iterations, double *root_strategy, double *root_ev,
+                         double *avg_strategies, int *avg_node_ids, double *regrets_out,
+                         double *strategy_sum_out)
+{
+    return solve_impl_f64(t, hands, weights, num_hands, leaf_values, frozen, iterations,
+                          root_strategy, root_ev, avg_strategies, avg_node_ids, regrets_out,
+                          strategy_sum_out, 1);
+}
+
 /* ------------------------------------------------------------------ */
 /* FP64 best response and exploitability                               */
 /* ------------------------------------------------------------------ */

@@ -86,6 +86,18 @@ int orc_solve_f64(const OrcTree *t, const int *hands, const float *weights,
                   double *avg_strategies, int *avg_node_ids, double *regrets_out,
                   double *strategy_sum_out);
 
+/* orc_solve_f64 with folds and leaves of one or two counted opponents
+ * evaluated by the card-removal closed form (inclusion-exclusion over shared
+ * cards, exact tuple counts for the reference's exact zeros) instead of the
+ * odometer: the same sums in FP64, O(H * 52) per terminal and traverser hand
+ * instead of O(H^2), so the full-size 3-player turn (1128 hands) is checkable.
+ * Every other terminal is evaluated as in orc_solve_f64. */
+int orc_solve_f64_closed(const OrcTree *t, const int *hands, const float *weights,
+                         const int *num_hands, const float *leaf_values, const int *frozen,
+                         int iterations, double *root_strategy, double *root_ev,
+                         double *avg_strategies, int *avg_node_ids, double *regrets_out,
+                         double *strategy_sum_out);
+
 /* FP64 best-response exploitability of the average strategy profile given as
  * avg_strategies [num_dec][8][max_h] (decision nodes in index order).
  * Writes per-player best-response and profile values (sum over own hands of

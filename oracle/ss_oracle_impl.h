@@ -17,6 +17,8 @@ typedef struct {
     REAL *strategy;       /* [N][8][max_h] */
     uint32_t *strength;   /* [num_sd][np][max_h] */
     int *sd_local;        /* [N] */
+    int closed;           /* 1: folds and leaves with 1-2 counted opponents by the
+                             card-removal closed form (terminals_closed) */
 } RSUF(OrcCtx);
 
 #define OH(c, p, h, k) ((c)->hands[(((size_t)(p) * (c)->max_h + (h)) * 2) + (k)])
@@ -347,29 +349,173 @@ static void RSUF(reach_root)(RSUF(OrcCtx) *c, int rp, const float *weights)
     for (int h = 0; h < c->nh[rp]; h++) r[h] = (REAL)weights[(size_t)rp * c->max_h + h];
 }
 
-static void RSUF(terminals)(RSUF(OrcCtx) *c, int trav, const float *leaf_values)
+/* Card-removal aggregates of one counted opponent at one terminal: the
+ * opponent's reach on each combo {x, y} (M, symmetric, zero diagonal), its
+ * card sums u(x) = sum_y M[x][y] and total F = sum u / 2, over the range
+ * entries that share no card with the board; cnt / cu / cF hold the same sums
+ * over 0/1 entries (1 where the reach is positive), in exact integers. */
+typedef struct {
+    double M[52][52], u[52], F;
+    long long cnt[52][52], cu[52], cF;
+} RSUF(OppAgg);
+
+static void RSUF(opp_aggregate)(RSUF(OrcCtx) *c, const OrcNode *x, int node, int p,
+                                RSUF(OppAgg) *g)
+{
+    memset(g, 0, sizeof(*g));
+    for (int o = 0; o < c->nh[p]; o++) {
+        int a0 = OH(c, p, o, 0), a1 = OH(c, p, o, 1);
+        if (a0 == a1 || RSUF(board_blocked)(x, a0, a1)) continue;
+        double r = (double)OREACH(c, p, node, o);
+        long long pos = r > 0;
+        g->M[a0][a1] += r;
+        g->M[a1][a0] += r;
+        g->u[a0] += r;
+        g->u[a1] += r;
+        g->F += r;
+        g->cnt[a0][a1] += pos;
+        g->cnt[a1][a0] += pos;
+        g->cu[a0] += pos;
+        g->cu[a1] += pos;
+        g->cF += pos;
+    }
+}
+
+/* opp_mass for one or two counted opponents and every traverser hand of one
+ * terminal at once, by inclusion-exclusion over shared cards instead of the
+ * odometer (same sum: opponent hands pairwise disjoint, disjoint from the
+ * traverser hand {a, b} and from the board).  With R = F - u(a) - u(b) +
+ * M[a][b] (an opponent's mass avoiding {a, b}) and u'(z) = u(z) - M[z][a] -
+ * M[z][b] (its card sums over hands avoiding {a, b}):
+ *   one opponent:  R
+ *   two opponents: R1 R2 - sum_{z not in {a,b}} u1'(z) u2'(z) + Q',
+ *                  Q' = sum over combos avoiding {a, b} of M1 M2
+ * (pairs sharing one card are counted once by the card sum, pairs on the
+ * same combo twice, hence + Q').  FP64 throughout.  The same formulas on the
+ * 0/1 entries count the contributing tuples exactly; where that count is 0
+ * the mass is exactly 0, as the reference's sum of positive products is. */
+static void RSUF(closed_mass)(RSUF(OrcCtx) *c, const OrcNode *x, int node, const int *opp,
+                              int k, int trav, RSUF(OppAgg) *g, double *mass)
+{
+    for (int i = 0; i < k; i++) RSUF(opp_aggregate)(c, x, node, opp[i], &g[i]);
+    double Q = 0;
+    long long cQ = 0;
+    if (k == 2)
+        for (int y = 0; y < 52; y++)
+            for (int z = y + 1; z < 52; z++) {
+                Q += g[0].M[y][z] * g[1].M[y][z];
+                cQ += g[0].cnt[y][z] * g[1].cnt[y][z];
+            }
+    for (int h = 0; h < c->nh[trav]; h++) {
+        int a = OH(c, trav, h, 0), b = OH(c, trav, h, 1);
+        double R[2];
+        long long cR[2];
+        for (int i = 0; i < k; i++) {
+            R[i] = g[i].F - g[i].u[a] - g[i].u[b] + g[i].M[a][b];
+            cR[i] = g[i].cF - g[i].cu[a] - g[i].cu[b] + g[i].cnt[a][b];
+        }
+        if (k == 1) {
+            mass[h] = cR[0] == 0 ? 0.0 : R[0];
+            continue;
+        }
+        double S = 0;
+        long long cS = 0;
+        for (int z = 0; z < 52; z++) {
+            if (z == a || z == b) continue;
+            double u1 = g[0].u[z] - g[0].M[z][a] - g[0].M[z][b];
+            double u2 = g[1].u[z] - g[1].M[z][a] - g[1].M[z][b];
+            S += u1 * u2;
+            cS += (g[0].cu[z] - g[0].cnt[z][a] - g[0].cnt[z][b]) *
+                  (g[1].cu[z] - g[1].cnt[z][a] - g[1].cnt[z][b]);
+        }
+        double Qab = Q, sa = 0, sb = 0;
+        long long cQab = cQ, ca = 0, cb = 0;
+        for (int z = 0; z < 52; z++) {
+            sa += g[0].M[a][z] * g[1].M[a][z];
+            sb += g[0].M[b][z] * g[1].M[b][z];
+            ca += g[0].cnt[a][z] * g[1].cnt[a][z];
+            cb += g[0].cnt[b][z] * g[1].cnt[b][z];
+        }
+        Qab = Q - sa - sb + g[0].M[a][b] * g[1].M[a][b];
+        cQab = cQ - ca - cb + g[0].cnt[a][b] * g[1].cnt[a][b];
+        long long cnt = cR[0] * cR[1] - cS + cQab;
+        mass[h] = cnt == 0 ? 0.0 : R[0] * R[1] - S + Qab;
+    }
+}
+
+/* terminal values of one traverser pass with closed forms for folds and
+ * leaves with 1-2 counted opponents (the FP64 checker at sizes where the
+ * odometer is out of reach); every other terminal as in terminals().
+ * Terminals write disjoint value rows, so they are spread over threads. */
+static void RSUF(terminals_closed)(RSUF(OrcCtx) *c, int trav, const float *leaf_values)
 {
     const OrcTree *t = c->t;
     memset(c->cfv, 0, (size_t)c->N * c->max_h * sizeof(REAL));
-    for (int i = 0; i < c->N; i++)
-        if (t->nodes[i].type == ORC_NODE_FOLD) RSUF(fold_value)(c, i, trav);
-    if (t->is_river)
-        for (int i = 0; i < c->N; i++)
-            if (t->nodes[i].type == ORC_NODE_SHOWDOWN) RSUF(showdown_value)(c, i, trav);
-    if (leaf_values)
-        for (int i = 0; i < c->N; i++)
-            if (t->nodes[i].type == ORC_NODE_LEAF) RSUF(leaf_value)(c, i, trav, leaf_values);
+#pragma omp parallel
+    {
+        RSUF(OppAgg) *g = (RSUF(OppAgg) *)malloc(2 * sizeof(RSUF(OppAgg)));
+        double *mass = (double *)malloc((size_t)c->max_h * sizeof(double));
+#pragma omp for schedule(dynamic, 8)
+        for (int n = 0; n < c->N; n++) {
+            const OrcNode *x = &t->nodes[n];
+            int opp[ORC_MAX_PLAYERS], k = 0;
+            if (x->type == ORC_NODE_FOLD) {
+                for (int p = 0; p < c->np; p++) if (p != trav) opp[k++] = p;
+                if (k > 2) { RSUF(fold_value)(c, n, trav); continue; }
+                REAL payoff = (trav == x->player) ? (REAL)(x->pot - x->bets[trav])
+                                                   : -(REAL)x->bets[trav];
+                RSUF(closed_mass)(c, x, n, opp, k, trav, g, mass);
+                for (int h = 0; h < c->nh[trav]; h++) OCFV(c, n, h) = payoff * (REAL)mass[h];
+            } else if (x->type == ORC_NODE_SHOWDOWN) {
+                if (t->is_river) RSUF(showdown_value)(c, n, trav);
+            } else if (x->type == ORC_NODE_LEAF && leaf_values) {
+                for (int p = 0; p < c->np; p++)
+                    if (p != trav && x->active_players[p]) opp[k++] = p;
+                if (k == 0 || k > 2 || x->leaf_idx < 0) {
+                    RSUF(leaf_value)(c, n, trav, leaf_values);
+                    continue;
+                }
+                RSUF(closed_mass)(c, x, n, opp, k, trav, g, mass);
+                for (int h = 0; h < c->nh[trav]; h++) {
+                    REAL ev = (REAL)leaf_values[((size_t)x->leaf_idx * c->np + trav) * c->max_h + h];
+                    OCFV(c, n, h) = ev * (REAL)mass[h];
+                }
+            }
+        }
+        free(mass);
+        free(g);
+    }
 }
 
-int RSUF(orc_solve)(const OrcTree *t, const int *hands, const float *weights,
-                    const int *num_hands, const float *leaf_values, const int *frozen,
-                    int iterations, REAL *root_strategy, REAL *root_ev,
-                    REAL *avg_strategies, int *avg_node_ids, REAL *regrets_out,
-                    REAL *strategy_sum_out)
+static void RSUF(terminals)(RSUF(OrcCtx) *c, int trav, const float *leaf_values)
+{
+    const OrcTree *t = c->t;
+    if (c->closed) {
+        RSUF(terminals_closed)(c, trav, leaf_values);
+        return;
+    }
+    memset(c->cfv, 0, (size_t)c->N * c->max_h * sizeof(REAL));
+    /* terminals write disjoint value rows; each row is computed exactly as in
+     * a serial loop, so spreading them over threads changes no bit */
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int i = 0; i < c->N; i++) {
+        int ty = t->nodes[i].type;
+        if (ty == ORC_NODE_FOLD) RSUF(fold_value)(c, i, trav);
+        else if (ty == ORC_NODE_SHOWDOWN && t->is_river) RSUF(showdown_value)(c, i, trav);
+        else if (ty == ORC_NODE_LEAF && leaf_values) RSUF(leaf_value)(c, i, trav, leaf_values);
+    }
+}
+
+static int RSUF(solve_impl)(const OrcTree *t, const int *hands, const float *weights,
+                            const int *num_hands, const float *leaf_values, const int *frozen,
+                            int iterations, REAL *root_strategy, REAL *root_ev,
+                            REAL *avg_strategies, int *avg_node_ids, REAL *regrets_out,
+                            REAL *strategy_sum_out, int closed)
 {
     RSUF(OrcCtx) c;
     int *sd_nodes = NULL, nsd = 0;
     if (RSUF(ctx_init)(&c, t, hands, num_hands, &sd_nodes, &nsd) != 0) return -1;
+    c.closed = closed;
     size_t N = (size_t)c.N, H = (size_t)c.max_h;
     REAL *regrets = (REAL *)calloc(N * ORC_MAX_ACTIONS * H, sizeof(REAL));
     REAL *ssum = (REAL *)calloc(N * ORC_MAX_ACTIONS * H, sizeof(REAL));
@@ -437,6 +583,17 @@ int RSUF(orc_solve)(const OrcTree *t, const int *hands, const float *weights,
     free(sd_nodes);
     RSUF(ctx_free)(&c);
     return 0;
+}
+
+int RSUF(orc_solve)(const OrcTree *t, const int *hands, const float *weights,
+                    const int *num_hands, const float *leaf_values, const int *frozen,
+                    int iterations, REAL *root_strategy, REAL *root_ev,
+                    REAL *avg_strategies, int *avg_node_ids, REAL *regrets_out,
+                    REAL *strategy_sum_out)
+{
+    return RSUF(solve_impl)(t, hands, weights, num_hands, leaf_values, frozen, iterations,
+                            root_strategy, root_ev, avg_strategies, avg_node_ids, regrets_out,
+                            strategy_sum_out, 0);
 }
 
 #undef OH
