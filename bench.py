@@ -64,14 +64,17 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS),
                     help="subgame of the plain form (the CPU baseline and reference arm cover turn3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf,four",
+    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf,four,anchor",
                     help="comma list of plain (the headline), batched, served, hu_river (the heads-up river "
                          "beside the reference's CPU solver), leaf (the turn subgame's continuation values "
                          "produced on the GPU), four (full-range 4-player turn and river, three-opponent "
                          "terminals)")
     ap.add_argument("--batch-size", type=int, default=512, help="batched form: mixed requests in one batch")
-    ap.add_argument("--rate", type=float, default=100.0, help="served form: requests per second")
-    ap.add_argument("--duration", type=float, default=3.0, help="served form: seconds of arrivals")
+    ap.add_argument("--rates", default="50,500,2000", help="served form: request rates per second")
+    ap.add_argument("--served-requests", type=int, default=256, help="served form: requests per rate")
+    ap.add_argument("--ncu-summary", nargs=2, metavar=("CSV", "COMMAND"),
+                    help="no run: summarise an ncu launch list (DRAM bytes per launch and class) of the "
+                         "--workload into profiles/dram_traffic.json, stamped with the kernel sources' hash")
     return ap.parse_args()
 
 
@@ -244,6 +247,65 @@ def flow_bytes_per_iteration(td, H):
     return total
 
 
+KERNEL_SOURCES = ("ss_kernels.cu", "ss_cr3.cuh", "ss_rank.cuh", "ss_kernels.h")
+# kernel name prefix -> profile class of ss_session_profile
+NCU_CLASSES = [("k_term_cr2", "term_cr2"), ("k_term_cr1", "term_cr1"), ("k_term_sd", "term_sd"),
+               ("k_term_enum", "term_enum"), ("k_term_cr3", "term_enum"), ("k_term_fill", "term_fill"),
+               ("k_cfv", "cfv"), ("k_reach", "reach")]
+
+
+def kernel_sources_sha16():
+    """Hash of the kernel sources, stamped on the DRAM-traffic capture so that
+    a capture of older kernels is not reported as this build's traffic."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        with open(os.path.join(PKG, "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def ncu_summary(csv_path, workload, command):
+    """Per profile class: launches captured and mean DRAM bytes (read + write)
+    per launch, from an ncu --csv launch list with dram__bytes_read.sum and
+    dram__bytes_write.sum; merged into profiles/dram_traffic.json."""
+    import csv
+    per = {}
+    with open(csv_path) as f:
+        rows = [r for r in csv.reader(f) if len(r) > 5]
+    head = rows[0]
+    ki, mi, vi, ii = head.index("Kernel Name"), head.index("Metric Name"), head.index("Metric Value"), head.index("ID")
+    launch = {}
+    for r in rows[1:]:
+        if r[mi] not in ("dram__bytes_read.sum", "dram__bytes_write.sum", "gpu__time_duration.sum"):
+            continue
+        d = launch.setdefault(r[ii], {"name": r[ki]})
+        d[r[mi]] = float(r[vi].replace(",", ""))
+    for d in launch.values():
+        cls = next((c for p, c in NCU_CLASSES if d["name"].startswith(p)), None)
+        if cls is None:
+            continue
+        e = per.setdefault(cls, {"launches_captured": 0, "bytes": 0.0})
+        e["launches_captured"] += 1
+        e["bytes"] += d.get("dram__bytes_read.sum", 0.0) + d.get("dram__bytes_write.sum", 0.0)
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        tr = json.load(open(path))
+    except Exception:
+        tr = {}
+    if tr.get("kernel_sources_sha16") != kernel_sources_sha16():
+        tr = {"workloads": {}}
+    tr["kernel_sources_sha16"] = kernel_sources_sha16()
+    tr["source"] = command
+    tr.setdefault("workloads", {})[workload] = {"classes": {
+        c: {"launches_captured": e["launches_captured"],
+            "dram_bytes_per_launch": int(round(e["bytes"] / e["launches_captured"]))}
+        for c, e in sorted(per.items())}}
+    with open(path, "w") as f:
+        json.dump(tr, f, indent=1)
+    return tr
+
+
 def run_ours(args, world, rank, local):
     import torch
     import street_solver_gpu as ssg
@@ -371,12 +433,16 @@ def run_ours(args, world, rank, local):
     # ratio equals bytes per iteration over time per iteration)
     n_launch = max(1, d["launches"])
     achieved = d["bytes"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else 0.0
-    traffic = None
+    traffic, traffic_note = None, "no ncu capture of this workload"
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
-        tcls = tr.get("workloads", {}).get(args.workload, {}).get("classes", {})
-        if dom in tcls:
-            traffic = tcls[dom].get("dram_bytes_per_launch")
+        if tr.get("kernel_sources_sha16") != kernel_sources_sha16():
+            traffic_note = "the ncu capture predates the current kernel sources"
+        else:
+            tcls = tr.get("workloads", {}).get(args.workload, {}).get("classes", {})
+            if dom in tcls:
+                traffic = tcls[dom].get("dram_bytes_per_launch")
+                traffic_note = tr.get("source", "")
     except Exception:
         pass
 
@@ -400,7 +466,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(args.steps * (args.iterations * launches_per_iter + reach_launches)),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "bytes_per_launch": d["bytes"] / n_launch,
+                     "traffic": traffic, "traffic_source": traffic_note,
+                     "bytes_per_launch": d["bytes"] / n_launch,
                      "launch_ms": d["ms"] / n_launch, "launches_per_iteration": d["launches"],
                      "bytes_per_iteration": d["bytes"], "kernel_ms_per_iteration": d["ms"]},
         "profile": {k: {"ms": round(v["ms"], 4), "launches": v["launches"],
@@ -429,12 +496,28 @@ def pct(v, q):
     return v[min(len(v) - 1, int(round(q / 100.0 * (len(v) - 1))))]
 
 
+C4_STREETS = (1 / 3, 1 / 3, 1 / 3)     # flop, turn, river
+C5_STREETS = (0.05, 0.15, 0.80)
+C4_MIX = ("flop / turn / river equally, 2-6 players (flops 2-3, turns 2-4), target tree size log-uniform "
+          "in [50, 20000] nodes by bet-set / raise-cap search, 2-3 players on every combo, 4 players on "
+          "64-128 hands, 5 on 8, 6 on 6, U(0, 0.7) of each range zeroed")
+
+
+def mix_stats(subs):
+    nodes = [sg.td.num_nodes for sg in subs]
+    kinds = {}
+    for sg in subs:
+        kinds[sg.cfg["name"]] = kinds.get(sg.cfg["name"], 0) + 1
+    return {"tree_nodes": {"min": min(nodes), "p50": pct(nodes, 50), "max": max(nodes)}, "kinds": kinds}
+
+
 def run_batched(n, seed, device):
-    """n mixed requests solved to <= 0.5% pot exploitability: one per call
-    (plain form, ss_solve_gpu_ex with the same stopping rule) and all
-    together (ss_batch_solve); wall time from host buffers to host outputs."""
+    """n requests of the batched mix solved to <= 0.5% pot exploitability:
+    one per call (plain form, ss_solve_gpu_ex with the same stopping rule)
+    and all together (ss_batch_solve); wall time from host buffers to host
+    outputs for both."""
     import workloads as wl
-    subs = wl.mix_subgames(n, seed)
+    subs = wl.c4_subgames(n, seed, streets=C4_STREETS)
     sg0 = subs[0]
     rc, _ = sg0.solve(CHECK, target=TARGET, check_every=CHECK)  # warm the library / pool
     t0 = time.perf_counter()
@@ -442,7 +525,7 @@ def run_batched(n, seed, device):
     for sg in subs:
         rc, r = sg.solve(MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
         if rc != 0:
-            raise RuntimeError(f"plain solve failed ({rc})")
+            raise RuntimeError(f"plain solve failed ({rc}): {wl.ssg.last_error(sg.lib)}")
         plain.append(r["stats"])
     t_plain = time.perf_counter() - t0
     # warm the batched path (its kernels load on first use) as the plain
@@ -452,78 +535,88 @@ def run_batched(n, seed, device):
     rc, res = wl.batch_solve(subs, MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
     t_batch = time.perf_counter() - t0
     if rc != 0:
-        raise RuntimeError(f"batch solve failed ({rc})")
+        raise RuntimeError(f"batch solve failed ({rc}): {wl.ssg.last_error(sg0.lib)}")
     its = [r["stats"]["iterations_run"] for r in res]
     expl = [r["stats"]["exploitability_pct"] for r in res]
-    nodes = [sg.td.num_nodes for sg in subs]
     per_it = [float(sg.td.num_nodes) * float(sum(sg.nh)) for sg in subs]   # node-hand updates per iteration
-    nhu_batch = sum(n * k for n, k in zip(per_it, its))
-    nhu_plain = sum(n * p["iterations_run"] for n, p in zip(per_it, plain))
+    nhu_batch = sum(n_ * k for n_, k in zip(per_it, its))
+    nhu_plain = sum(n_ * p["iterations_run"] for n_, p in zip(per_it, plain))
+    gpu_ms = res[0]["stats"]["solve_ms"]
+    mix = mix_stats(subs)
     for sg in subs:
         sg.free()
-    return {"subgames": n, "target_pct": TARGET, "check_every": CHECK,
-            "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch,
-            "speedup_vs_plain": t_plain / t_batch,
-            "plain_node_hand_updates_per_s": nhu_plain / t_plain,
-            "batched_node_hand_updates_per_s": nhu_batch / t_batch,
-            "iterations_p50": pct(its, 50), "iterations_max": max(its),
-            "exploitability_max_pct": max(expl),
-            "plain_iterations_p50": pct([p["iterations_run"] for p in plain], 50),
-            "tree_nodes": {"min": min(nodes), "p50": pct(nodes, 50), "max": max(nodes)},
-            "mix": "80% river (70% 2p, 30% 3p) / 15% turn (2-3p) / 5% flop (2p), full ranges, 0-70% zero weights"}
+    out = {"subgames": n, "target_pct": TARGET, "check_every": CHECK,
+           "plain_solves_per_s": n / t_plain, "batched_solves_per_s": n / t_batch,
+           "speedup_vs_plain": t_plain / t_batch,
+           "plain_node_hand_updates_per_s": nhu_plain / t_plain,
+           "batched_node_hand_updates_per_s": nhu_batch / t_batch,
+           "batched_wall_s": t_batch, "batched_gpu_iterations_s": gpu_ms / 1e3,
+           "plain_wall_s": t_plain,
+           "iterations_p50": pct(its, 50), "iterations_max": max(its),
+           "exploitability_max_pct": max(expl),
+           "plain_iterations_p50": pct([p["iterations_run"] for p in plain], 50),
+           "mix": C4_MIX}
+    out.update(mix)
+    return out
 
 
-def run_served(rate, duration, seed, device):
-    """Poisson arrivals at `rate` for `duration` seconds into the server
-    (continuous batching, retirement at <= 0.5% pot); latency = submission
-    to retirement.  The plain form's service time of the same requests
-    (one solve per call, no queueing) is reported beside it."""
+def run_served(rates, n, seed, device):
+    """Poisson arrivals of n requests of the served mix (80% river, 15% turn,
+    5% flop) at each rate into the server (continuous batching, retirement at
+    <= 0.5% pot); latency = submission to retirement.  The plain form's
+    service time of the same requests (one solve per call, no queueing) is
+    reported beside it."""
     import workloads as wl
-    rng = np.random.default_rng(seed + 7)
-    n = max(8, int(rate * duration))
-    subs = wl.mix_subgames(n, seed + 1)
+    subs = wl.c4_subgames(n, seed + 1, streets=C5_STREETS)
     lib = subs[0].lib
-    gaps = rng.exponential(1.0 / rate, n)
-    srv = wl.Server(lib, device=device, block_iterations=CHECK, target_exploitability=TARGET,
-                    max_iterations=MAX_ITERS, memory_budget_gb=40.0)
-    ids = [None] * n
-    t_start = time.perf_counter()
+    per_rate = []
+    for rate in rates:
+        rng = np.random.default_rng(seed + 7)
+        gaps = rng.exponential(1.0 / rate, n)
+        srv = wl.Server(lib, device=device, block_iterations=CHECK, target_exploitability=TARGET,
+                        max_iterations=MAX_ITERS, memory_budget_gb=60.0)
+        ids = [None] * n
+        t_start = time.perf_counter()
 
-    def feeder():
-        t = t_start
+        def feeder():
+            t = t_start
+            for i, sg in enumerate(subs):
+                t += gaps[i]
+                d = t - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(sg)
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        lat, its, nhu = [], [], []
         for i, sg in enumerate(subs):
-            t += gaps[i]
-            d = t - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            ids[i] = srv.submit(sg)
-
-    th = threading.Thread(target=feeder)
-    th.start()
-    lat, its, nhu = [], [], []
-    for i, sg in enumerate(subs):
-        while ids[i] is None:
-            time.sleep(0.0005)
-        r = srv.wait(ids[i], sg.nh)
-        lat.append(r["latency_ms"])
-        its.append(r["stats"]["iterations_run"])
-        nhu.append(float(sg.td.num_nodes) * float(sum(sg.nh)) * r["stats"]["iterations_run"])
-    th.join()
-    wall = time.perf_counter() - t_start
-    srv.close()
+            while ids[i] is None:
+                time.sleep(0.0005)
+            r = srv.wait(ids[i], sg.nh)
+            lat.append(r["latency_ms"])
+            its.append(r["stats"]["iterations_run"])
+            nhu.append(float(sg.td.num_nodes) * float(sum(sg.nh)) * r["stats"]["iterations_run"])
+        th.join()
+        wall = time.perf_counter() - t_start
+        srv.close()
+        per_rate.append({"rate_per_s": rate, "requests": n, "arrivals_s": float(gaps.sum()),
+                         "solves_per_s": n / wall, "node_hand_updates_per_s": sum(nhu) / wall,
+                         "latency_p50_ms": pct(lat, 50), "latency_p99_ms": pct(lat, 99),
+                         "iterations_p50": pct(its, 50)})
     service = []
     for sg in subs[:min(n, 64)]:
         t0 = time.perf_counter()
         rc, _ = sg.solve(MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
         service.append((time.perf_counter() - t0) * 1e3)
+    out = {"rates": per_rate,
+           "plain_service_p50_ms": pct(service, 50), "plain_service_p99_ms": pct(service, 99),
+           "plain_solves_per_s": 1e3 * len(service) / sum(service),
+           "mix": "the batched mix with streets 5% flop / 15% turn / 80% river"}
+    out.update(mix_stats(subs))
     for sg in subs:
         sg.free()
-    return {"rate_per_s": rate, "requests": n, "solves_per_s": n / wall,
-            "node_hand_updates_per_s": sum(nhu) / wall,
-            "latency_p50_ms": pct(lat, 50), "latency_p99_ms": pct(lat, 99),
-            "iterations_p50": pct(its, 50),
-            "plain_service_p50_ms": pct(service, 50), "plain_service_p99_ms": pct(service, 99),
-            "plain_solves_per_s": 1e3 * len(service) / sum(service)}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -762,8 +855,70 @@ def reference_cpu(seed, budget_s=25.0):
             "solves_per_s": 1.0 / (s_iter_full * 1000)}
 
 
+ANCHOR = {"hands": 10, "iterations": 20}
+
+
+def anchor_config(seed):
+    import workloads as wl
+    cfg = wl.config(WORKLOAD, seed=seed, num_hands=ANCHOR["hands"])
+    return cfg, (f"3-player turn subgame with continuation leaves, the benchmark's 21,436-node tree, "
+                 f"{ANCHOR['hands']} combos/player, {ANCHOR['iterations']} Linear-CFR iterations")
+
+
+def anchor_reference(seed):
+    """The same small configuration solved by the reference's kernels on the
+    host (oracle/_ref), one solve per core at once: measured, not modelled."""
+    import workloads as wl
+    from oracle.oracle import RefStreetSolve, ref_available
+    if not ref_available(200, 3):
+        return None
+    ref = RefStreetSolve(200, 3, "cpu")
+    cores = os.cpu_count() or 1
+    cfg, name = anchor_config(seed)
+    Hm, Wm, nh = wl.padded(cfg)
+
+    def one(i):
+        td = ref.build(cfg["board"], cfg["pot"], cfg["stack"], cfg["bet_sizes"], 3)
+        lv = wl.leaf_values_for(cfg, td.num_leaves)
+        ref.solve(td, Hm, Wm, nh, ANCHOR["iterations"], leaf_values=lv)
+        ref.free(td)
+
+    with _Quiet():
+        th = [threading.Thread(target=one, args=(i,)) for i in range(cores)]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+    return {"workload": name, "solves_per_s": cores / wall, "wall_s": wall, "solves": cores, "cores": cores,
+            "kind": "reference kernels on the host (oracle/_ref), one solve per core"}
+
+
+def anchor_gpu(seed, device, solves=20):
+    """The same small configuration through ss_solve_gpu from host buffers."""
+    import workloads as wl
+    cfg, name = anchor_config(seed)
+    sg = wl.AbiSubgame(cfg, max_hands=200)
+    sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
+    rc, _ = sg.solve(ANCHOR["iterations"], device=device)   # warm
+    t0 = time.perf_counter()
+    for _ in range(solves):
+        rc, _ = sg.solve(ANCHOR["iterations"], device=device)
+        if rc != 0:
+            raise RuntimeError(f"anchor solve failed ({rc})")
+    wall = time.perf_counter() - t0
+    sg.free()
+    return {"workload": name, "solves_per_s": solves / wall, "wall_s": wall, "solves": solves,
+            "kind": "ss_solve_gpu from host buffers (e2e), one B200"}
+
+
 def main():
     args = parse()
+    if args.ncu_summary:
+        tr = ncu_summary(args.ncu_summary[0], args.workload, args.ncu_summary[1])
+        print(json.dumps(tr["workloads"][args.workload]))
+        return 0
     world, rank, local = dist_init()
     if args.impl == "reference":
         if rank == 0:
@@ -792,6 +947,10 @@ def main():
                                                f"extrapolated to 1128 with exponent "
                                                f"{r['exponent']:.2f}; median of {len(r['samples'])} samples"},
                     "samples": r["samples"],
+                    "value_is_model": "full-size rate extrapolated from measured small-range iterations "
+                                      "(the reference's O(H^3) terminals cannot run 1128 hands in bounded "
+                                      "time); anchor_same_config is measured on a config both arms run",
+                    "anchor_same_config": anchor_reference(args.seed),
                     "e2e": {"value": r["solves_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
                             "d2h_bytes_per_step": 0},
                 }
@@ -804,7 +963,7 @@ def main():
     if rank == 0 and world == 1 and "batched" in forms:
         batched = run_batched(args.batch_size, args.seed, local)
     if rank == 0 and world == 1 and "served" in forms:
-        served = run_served(args.rate, args.duration, args.seed, local)
+        served = run_served([float(r) for r in args.rates.split(",")], args.served_requests, args.seed, local)
     hu = None
     if rank == 0 and world == 1 and "hu_river" in forms:
         try:
@@ -823,6 +982,14 @@ def main():
             four = run_four_player(args.seed, local)
         except Exception as e:  # the solver's line is printed whatever happens here
             four = {"error": f"{type(e).__name__}: {e}"}
+    anchor = None
+    if rank == 0 and world == 1 and "anchor" in forms and args.workload == "turn3":
+        try:
+            anchor = {"gpu": anchor_gpu(args.seed, local), "reference": anchor_reference(args.seed)}
+            if anchor["reference"]:
+                anchor["speedup"] = anchor["gpu"]["solves_per_s"] / anchor["reference"]["solves_per_s"]
+        except Exception as e:  # the solver's line is printed whatever happens here
+            anchor = {"error": f"{type(e).__name__}: {e}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "turn3":
         r = reference_cpu(args.seed, budget_s=20.0)
@@ -849,6 +1016,10 @@ def main():
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
             "batched": batched, "served": served, "hu_river": hu, "leaf_producer": leaf, "four_player": four,
+            "anchor_same_config": anchor,
+            "hu_river_vs_reference_cpu": None if not hu or "error" in hu else {
+                "gpu_solves_per_s": hu.get("gpu_solves_per_s"),
+                "reference_cpu_solves_per_s": (hu.get("cpu_baseline") or {}).get("solves_per_s")},
         }
         print(json.dumps(line))
     try:

@@ -276,6 +276,25 @@ void *ss_session_stream(SSSession *session);
 int ss_session_exploitability(SSSession *session, double *exploitability_pct, double *nashconv,
                               double *br_value, double *cur_value, double *deal_mass);
 
+/* EXTENSION (GPU form of the reference's between-street range update,
+ * python/hud_solver.py:345-362 with python/range_narrowing.py:83-130):
+ * narrow a range of num_hands entries (hand_cards [num_hands][2], weights
+ * [num_hands], host arrays, weights updated in place) by the session's
+ * current average strategy of `player` at decision node `node` (-1: the
+ * player's first decision node, as get_avg_strategy reads it), for the action
+ * label carried by the node's actions in action_mask (bit a = action a; the
+ * last of them with a frequency above 0.001 counts, as in the reference's
+ * label dictionary).  P(action | combo) is that frequency (0 at or below
+ * 0.001); a combo the session's range does not hold (or an entry with
+ * c0 > c1) gets 1 / max(number of distinct P values, 2); w' = w * P, raised
+ * to 0.005 where w > 0, then divided by the largest w'.  FP64 throughout, bit
+ * for bit the reference's Python.  *applied = 1 when some P is positive, else
+ * 0 and the weights are left unchanged (the reference then falls back to
+ * other sources).  The strategy sums are read where the solve left them;
+ * nothing but the range crosses to the host. */
+int ss_session_narrow(SSSession *session, int player, int node, unsigned int action_mask, int num_hands,
+                      const int *hand_cards, double *weights, int *applied);
+
 /* EXTENSION: release the session. */
 void ss_session_destroy(SSSession *session);
 
@@ -332,6 +351,13 @@ int ss_server_submit(SSServer *server, const SSTreeData *tree_data, long long *r
  * or running, < 0 = failed (the request is dropped). */
 int ss_server_poll(SSServer *server, long long request_id, SSOutput *output, SSSolveStats *stats,
                    double *latency_ms);
+
+/* EXTENSION: where a request stands without taking its result: *state 0 =
+ * queued (not yet in the batch), 1 = in the batch, 2 = done (fetch it with
+ * ss_server_poll / ss_server_wait); *iterations_run = CFR iterations it has
+ * run so far (any pointer may be NULL).  Returns SS_OK, or SS_ERR_INVALID
+ * for an unknown id, or the request's failure code. */
+int ss_server_progress(SSServer *server, long long request_id, int *state, int *iterations_run);
 
 /* EXTENSION: like ss_server_poll but blocks until the request is done. */
 int ss_server_wait(SSServer *server, long long request_id, SSOutput *output, SSSolveStats *stats,

@@ -30,6 +30,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+# the reference checkout: REF_ROOT, else where this build keeps it (the only
+# place any script of the repository names that location)
 REF = os.environ.get("REF_ROOT", "/root/reference")
 
 # (SS_MAX_HANDS, SS_MAX_RAISES) variants of the CPU-shim build

@@ -21,7 +21,7 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
 ENGINE = ["ss_tree.cpp", "ss_plan.cpp", "ss_kernels.cu", "ss_engine.cu", "ss_rank_kernels.cu", "ss_noalloc.cu", "ss_batch.cu",
-          "ss_leaf_plan.cpp", "ss_leaf.cu"]
+          "ss_leaf_plan.cpp", "ss_leaf.cu", "ss_narrow.cu"]
 HEADERS = ["ss_engine.h", "ss_kernels.h", "ss_rank.cuh", "ss_session.h", "ss_leaf.h", "ss_leaf.cuh"]
 VARIANTS = {"libstreet_solve.so": 200, "libstreet_solve_wide.so": 1326}
 

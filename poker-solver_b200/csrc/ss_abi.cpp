@@ -311,6 +311,12 @@ int ss_session_exploitability(SSSession *s, double *pct, double *nash, double *b
     return ssb::session_exploitability(s->impl, nullptr, pct, nash, br, cur, z);
 }
 
+int ss_session_narrow(SSSession *s, int player, int node, unsigned int action_mask, int num_hands,
+                      const int *hand_cards, double *weights, int *applied) {
+    if (!s) return SS_ERR_INVALID;
+    return ssb::session_narrow(s->impl, player, node, action_mask, num_hands, hand_cards, weights, applied);
+}
+
 void *ss_session_stream(SSSession *s) { return s ? ssb::session_stream(s->impl) : nullptr; }
 
 void ss_session_destroy(SSSession *s) {
@@ -400,6 +406,11 @@ int ss_server_submit(SSServer *s, const SSTreeData *td, long long *id) {
 int ss_server_poll(SSServer *s, long long id, SSOutput *out, SSSolveStats *stats, double *latency_ms) {
     if (!s) return SS_ERR_INVALID;
     return ssb::server_poll(s->impl, id, out, stats, latency_ms, 0);
+}
+
+int ss_server_progress(SSServer *s, long long id, int *state, int *iterations_run) {
+    if (!s) return SS_ERR_INVALID;
+    return ssb::server_progress(s->impl, id, state, iterations_run);
 }
 
 int ss_server_wait(SSServer *s, long long id, SSOutput *out, SSSolveStats *stats, double *latency_ms) {

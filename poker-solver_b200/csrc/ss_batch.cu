@@ -18,7 +18,9 @@
 #include "ss_session.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cstddef>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -48,12 +50,15 @@ class Batch {
 
     ~Batch() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (br_graph) cudaGraphExecDestroy(br_graph);
         if (stream) {
             if (dctx) cudaFreeAsync(dctx, stream);
             if (dlists) cudaFreeAsync(dlists, stream);
+            if (dsc) cudaFreeAsync(dsc, stream);
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
         }
+        if (hsc) cudaFreeHost(hsc);
         for (Session *s : subs) delete s;
     }
 
@@ -65,18 +70,34 @@ class Batch {
         return SS_OK;
     }
 
-    int add(Session *s) {
+    // a member gets its best-response buffers here, so that every check of
+    // the batch is one merged launch sequence
+    int add(Session *s, int *slot) {
+        int rc = s->ensure_br();
+        if (rc != SS_OK) return rc;
         subs.push_back(s);
         active.push_back(1);
         iters_run.push_back(0);
+        work.push_back(0.0);
         dirty = true;
-        return static_cast<int>(subs.size()) - 1;
+        *slot = static_cast<int>(subs.size()) - 1;
+        return SS_OK;
     }
 
-    // stop iterating member i (its state stays readable until released)
-    void retire(int i) {
+    // stop iterating member i (its state stays readable until released): its
+    // live flag in the device context array turns 0, so its items in the
+    // captured graphs return at once; the graphs are rebuilt without the
+    // retired members only once they hold most of the captured work
+    int retire(int i) {
         active[i] = 0;
-        dirty = true;
+        if (dctx && i < built_members) {
+            static const int zero = 0;
+            BCK(cudaMemcpyAsync(reinterpret_cast<char *>(dctx + i) + offsetof(DevCtx, live), &zero, sizeof(int),
+                                cudaMemcpyHostToDevice, stream));
+        }
+        live_work -= work[i];
+        if (live_work < 0.5 * built_work) dirty = true;
+        return SS_OK;
     }
 
     void release(int i) {
@@ -118,10 +139,34 @@ class Batch {
         return SS_OK;
     }
 
+    // FP64 exploitability of every active member's average strategy: one
+    // replay of the merged best-response graph, one copy of the root sums,
+    // one synchronisation.  pct / nash are indexed by member.
+    int check(std::vector<double> &pct, std::vector<double> &nash) {
+        if (num_active() == 0) return SS_OK;
+        BCK(cudaSetDevice(device));
+        if (dirty) {
+            int rc = rebuild();
+            if (rc != SS_OK) return rc;
+        }
+        BCK(cudaGraphLaunch(br_graph, stream));
+        BCK(cudaMemcpyAsync(hsc, dsc, static_cast<size_t>(built_members) * kSlots * sizeof(double),
+                            cudaMemcpyDeviceToHost, stream));
+        BCK(cudaStreamSynchronize(stream));
+        pct.resize(subs.size(), -1.0);
+        nash.resize(subs.size(), -1.0);
+        for (size_t i = 0; i < subs.size(); ++i)
+            if (active[i])
+                subs[i]->nashconv_from_sums(hsc + i * kSlots, &pct[i], &nash[i], nullptr, nullptr, nullptr);
+        return SS_OK;
+    }
+
   private:
+    static constexpr int kSlots = 2 * SS_MAX_PLAYERS + 2;   // root sums per member (nashconv_from_sums)
+    enum LaunchType { L_BUMP, L_SNAP, L_TERM, L_CFV, L_REACH, L_AVG, L_BR_REACH, L_BR_TERM, L_BR_VALUE, L_BR_ROOT };
     struct Launch {
-        int type;   // 0 bump, 1 snapshot, 2 terminals, 3 cfv, 4 reach
-        int kind;   // terminal kind; value/regret launches: number of long items (at the end)
+        int type;
+        int kind;   // terminal kind; value/regret launches: long items at the end; best-response values: mode
         int t;      // traverser / player
         size_t off; // item offset in dlists
         int n;
@@ -129,24 +174,42 @@ class Batch {
     };
     DevCtx *dctx = nullptr;
     char *dlists = nullptr;
+    double *dsc = nullptr, *hsc = nullptr;
     DevCtx cmax{};
-    std::vector<Launch> seq;
-    cudaGraphExec_t graph = nullptr;
+    std::vector<Launch> seq, br_seq;
+    cudaGraphExec_t graph = nullptr, br_graph = nullptr;
     bool dirty = true;
+    int built_members = 0;
+    std::vector<double> work;      // per member: work items in the captured launches
+    double built_work = 0, live_work = 0;
 
     cudaError_t launch(const Launch &L) {
         switch (L.type) {
-            case 0: return launch_bump_many(dctx, reinterpret_cast<const int *>(dlists + L.off), L.n, stream);
-            case 1: return launch_snapshot_many(dctx, reinterpret_cast<const int *>(dlists + L.off), L.n, stream);
-            case 2:
+            case L_BUMP: return launch_bump_many(dctx, reinterpret_cast<const int *>(dlists + L.off), L.n, stream);
+            case L_SNAP: return launch_snapshot_many(dctx, reinterpret_cast<const int *>(dlists + L.off), L.n, stream);
+            case L_TERM:
                 return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
                                     stream, dctx);
-            case 3:
+            case L_CFV:
                 return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.kind, L.H, stream,
                                   dctx, L.t);
-            default:
+            case L_REACH:
                 return launch_reach(cmax, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H, stream,
                                     dctx, L.t);
+            case L_AVG:
+                return launch_avg_many(dctx, reinterpret_cast<const AvgItem *>(dlists + L.off), L.n, L.H, stream);
+            case L_BR_REACH:
+                return launch_br_reach_many(dctx, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H,
+                                            L.t, stream);
+            case L_BR_TERM:
+                return launch_terms_fp64(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
+                                         stream, dctx);
+            case L_BR_VALUE:
+                return launch_br_value_many(dctx, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.H, L.t,
+                                            L.kind, stream);
+            default:
+                return launch_br_root_many(dctx, reinterpret_cast<const RootItem *>(dlists + L.off), L.n, dsc,
+                                           stream);
         }
     }
 
@@ -158,10 +221,39 @@ class Batch {
         return cudaSuccess;
     }
 
+    cudaError_t br_pass() {
+        for (const Launch &L : br_seq) {
+            cudaError_t e = launch(L);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
+    int capture(cudaError_t (Batch::*body_fn)(), int reps, cudaGraphExec_t *exec) {
+        cudaGraph_t g = nullptr;
+        BCK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t body = cudaSuccess;
+        for (int r = 0; r < reps && body == cudaSuccess; ++r) body = (this->*body_fn)();
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (body != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            BCK(body);
+        }
+        BCK(e);
+        e = cudaGraphInstantiate(exec, g, 0);
+        cudaGraphDestroy(g);
+        BCK(e);
+        return SS_OK;
+    }
+
     int rebuild() {
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
+        }
+        if (br_graph) {
+            cudaGraphExecDestroy(br_graph);
+            br_graph = nullptr;
         }
         const int K = static_cast<int>(subs.size());
         std::vector<DevCtx> ctx(K);
@@ -169,6 +261,7 @@ class Batch {
         for (int i = 0; i < K; ++i)
             if (subs[i]) {
                 ctx[i] = subs[i]->c;
+                ctx[i].live = active[i];
                 // launch-time sizes (grids, dynamic shared memory) come from
                 // cmax: the largest row stride, rank table and sweep run of the batch
                 cmax.HS = std::max(cmax.HS, subs[i]->c.HS);
@@ -179,6 +272,7 @@ class Batch {
         // merged lists, in launch order
         std::vector<char> blob;
         seq.clear();
+        br_seq.clear();
         auto put = [&](const void *src, size_t bytes) {
             size_t off = (blob.size() + 255) & ~static_cast<size_t>(255);
             blob.resize(off + bytes);
@@ -186,19 +280,24 @@ class Batch {
             return off;
         };
         std::vector<int> act;
-        int maxnp = 0;
-        for (int i = 0; i < K; ++i)
+        int maxnp = 0, maxh = 0;
+        for (int i = 0; i < K; ++i) {
+            work[i] = 0.0;
             if (active[i]) {
                 act.push_back(i);
                 maxnp = std::max(maxnp, subs[i]->P.np);
+                maxh = std::max(maxh, subs[i]->P.max_h);
             }
-        seq.push_back({0, 0, 0, put(act.data(), act.size() * sizeof(int)), static_cast<int>(act.size()), 0});
+        }
+        auto add_work = [&](int i, size_t n) { work[i] += static_cast<double>(n); };
+        seq.push_back({L_BUMP, 0, 0, put(act.data(), act.size() * sizeof(int)), static_cast<int>(act.size()), 0});
         for (int t = 0; t < maxnp; ++t) {
             std::vector<int> snap;
             for (int i : act)
                 if (subs[i]->P.np - 1 == t) snap.push_back(i);
             if (!snap.empty())
-                seq.push_back({1, 0, t, put(snap.data(), snap.size() * sizeof(int)), static_cast<int>(snap.size()), 0});
+                seq.push_back({L_SNAP, 0, t, put(snap.data(), snap.size() * sizeof(int)), static_cast<int>(snap.size()),
+                               0});
             for (int k = 0; k < TK_COUNT; ++k) {
                 std::vector<TermItem> items;
                 for (int i : act) {
@@ -207,9 +306,10 @@ class Batch {
                         it.sg = i;
                         items.push_back(it);
                     }
+                    add_work(i, subs[i]->P.term[t][k].size());
                 }
                 if (!items.empty())
-                    seq.push_back({2, k, t, put(items.data(), items.size() * sizeof(TermItem)),
+                    seq.push_back({L_TERM, k, t, put(items.data(), items.size() * sizeof(TermItem)),
                                    static_cast<int>(items.size()), 0});
             }
             size_t lv = 0;
@@ -229,12 +329,13 @@ class Batch {
                         it.sg = i;
                         (j < n_short ? items : longs).push_back(it);
                     }
+                    add_work(i, v.size());
                     H = std::max(H, P.H[t]);
                 }
                 const int n_long = static_cast<int>(longs.size());
                 items.insert(items.end(), longs.begin(), longs.end());
                 if (!items.empty())
-                    seq.push_back({3, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
+                    seq.push_back({L_CFV, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
                                    static_cast<int>(items.size()), H});
             }
             lv = 0;
@@ -250,37 +351,138 @@ class Batch {
                         it.sg = i;
                         items.push_back(it);
                     }
+                    add_work(i, P.reach_levels[t][l].size());
                     H = std::max(H, P.H[t]);
                 }
                 if (!items.empty())
-                    seq.push_back({4, 0, t, put(items.data(), items.size() * sizeof(ReachItem)),
+                    seq.push_back({L_REACH, 0, t, put(items.data(), items.size() * sizeof(ReachItem)),
                                    static_cast<int>(items.size()), H});
             }
         }
+        // the merged best response (Session::exploitability for every member)
+        {
+            std::vector<AvgItem> avg;
+            for (int i : act)
+                for (int di = 0; di < subs[i]->P.num_dec; ++di) avg.push_back({i, di});
+            if (!avg.empty())
+                br_seq.push_back({L_AVG, 0, 0, put(avg.data(), avg.size() * sizeof(AvgItem)),
+                                  static_cast<int>(avg.size()), maxh});
+        }
+        for (int p = 0; p < maxnp; ++p) {
+            size_t lv = 0;
+            for (int i : act)
+                if (subs[i]->P.np > p) lv = std::max(lv, subs[i]->P.reach_levels[p].size());
+            for (size_t l = 0; l < lv; ++l) {
+                std::vector<ReachItem> items;
+                int H = 0;
+                for (int i : act) {
+                    const Plan &P = subs[i]->P;
+                    if (P.np <= p || l >= P.reach_levels[p].size()) continue;
+                    for (ReachItem it : P.reach_levels[p][l]) {
+                        it.sg = i;
+                        items.push_back(it);
+                    }
+                    H = std::max(H, P.H[p]);
+                }
+                if (!items.empty())
+                    br_seq.push_back({L_BR_REACH, 0, p, put(items.data(), items.size() * sizeof(ReachItem)),
+                                      static_cast<int>(items.size()), H});
+            }
+        }
+        for (int t = 0; t < maxnp; ++t) {
+            for (int k = 0; k < TK_COUNT; ++k) {
+                std::vector<TermItem> items;
+                for (int i : act) {
+                    if (subs[i]->P.np <= t) continue;
+                    for (TermItem it : subs[i]->P.term[t][k]) {
+                        it.sg = i;
+                        items.push_back(it);
+                    }
+                }
+                if (!items.empty())
+                    br_seq.push_back({L_BR_TERM, k, t, put(items.data(), items.size() * sizeof(TermItem)),
+                                      static_cast<int>(items.size()), 0});
+            }
+            size_t lv = 0;
+            for (int i : act)
+                if (subs[i]->P.np > t) lv = std::max(lv, subs[i]->P.cfv_levels[t].size());
+            for (int mode = 0; mode < 2; ++mode) {
+                for (size_t l = 0; l < lv; ++l) {
+                    std::vector<CfvItem> items;
+                    int H = 0;
+                    for (int i : act) {
+                        const Plan &P = subs[i]->P;
+                        if (P.np <= t || l >= P.cfv_levels[t].size()) continue;
+                        for (CfvItem it : P.cfv_levels[t][l]) {
+                            it.sg = i;
+                            items.push_back(it);
+                        }
+                        H = std::max(H, P.H[t]);
+                    }
+                    if (!items.empty())
+                        br_seq.push_back({L_BR_VALUE, mode, t, put(items.data(), items.size() * sizeof(CfvItem)),
+                                          static_cast<int>(items.size()), H});
+                }
+                std::vector<RootItem> roots;
+                for (int i : act) {
+                    const Plan &P = subs[i]->P;
+                    if (P.np <= t) continue;
+                    roots.push_back({subs[i]->root_fr[t], static_cast<int>(P.root_fr[t].size()), i, t, P.E + t, 0,
+                                     i * kSlots + 2 * t + mode});
+                }
+                if (!roots.empty())
+                    br_seq.push_back({L_BR_ROOT, 0, t, put(roots.data(), roots.size() * sizeof(RootItem)),
+                                      static_cast<int>(roots.size()), 0});
+            }
+        }
+        {
+            // deal mass: each member's own item, merged by kind
+            std::vector<RootItem> roots;
+            for (int k = 0; k < TK_COUNT; ++k) {
+                std::vector<TermItem> items;
+                for (int i : act)
+                    if (subs[i]->deal_kind == k) {
+                        TermItem it = subs[i]->deal;
+                        it.sg = i;
+                        items.push_back(it);
+                    }
+                if (!items.empty())
+                    br_seq.push_back({L_BR_TERM, k, 0, put(items.data(), items.size() * sizeof(TermItem)),
+                                      static_cast<int>(items.size()), 0});
+            }
+            for (int i : act)
+                roots.push_back({subs[i]->br_row, 1, i, 0, subs[i]->P.E, 1, i * kSlots + 2 * SS_MAX_PLAYERS});
+            if (!roots.empty())
+                br_seq.push_back({L_BR_ROOT, 0, 0, put(roots.data(), roots.size() * sizeof(RootItem)),
+                                  static_cast<int>(roots.size()), 0});
+        }
+        built_work = live_work = 0;
+        for (int i : act) built_work += work[i];
+        live_work = built_work;
         if (dctx) cudaFreeAsync(dctx, stream);
         if (dlists) cudaFreeAsync(dlists, stream);
+        if (dsc) cudaFreeAsync(dsc, stream);
         dctx = nullptr;
         dlists = nullptr;
+        dsc = nullptr;
+        if (hsc && built_members < K) {
+            cudaFreeHost(hsc);
+            hsc = nullptr;
+        }
+        built_members = K;
         BCK(cudaMallocAsync(reinterpret_cast<void **>(&dctx), std::max(1, K) * sizeof(DevCtx), stream));
         BCK(cudaMallocAsync(reinterpret_cast<void **>(&dlists), std::max<size_t>(blob.size(), 256), stream));
+        BCK(cudaMallocAsync(reinterpret_cast<void **>(&dsc), std::max(1, K) * kSlots * sizeof(double), stream));
+        BCK(cudaMemsetAsync(dsc, 0, std::max(1, K) * kSlots * sizeof(double), stream));
+        if (!hsc) BCK(cudaMallocHost(reinterpret_cast<void **>(&hsc), std::max(1, K) * kSlots * sizeof(double)));
         BCK(cudaMemcpyAsync(dctx, ctx.data(), K * sizeof(DevCtx), cudaMemcpyHostToDevice, stream));
         BCK(cudaMemcpyAsync(dlists, blob.data(), blob.size(), cudaMemcpyHostToDevice, stream));
         // members were initialised on their own streams
         for (int i : act) BCK(cudaStreamSynchronize(subs[i]->stream));
         BCK(cudaStreamSynchronize(stream));  // host staging must outlive the copies
-        cudaGraph_t g = nullptr;
-        BCK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t body = cudaSuccess;
-        for (int r = 0; r < graph_iters && body == cudaSuccess; ++r) body = iteration();
-        cudaError_t e = cudaStreamEndCapture(stream, &g);
-        if (body != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            BCK(body);
-        }
-        BCK(e);
-        e = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        BCK(e);
+        int rc = capture(&Batch::iteration, graph_iters, &graph);
+        if (rc == SS_OK) rc = capture(&Batch::br_pass, 1, &br_graph);
+        if (rc != SS_OK) return rc;
         dirty = false;
         return SS_OK;
     }
@@ -289,6 +491,38 @@ class Batch {
 // ---------------------------------------------------------------------------
 // batched form: solve n subgames together
 // ---------------------------------------------------------------------------
+
+// Sessions of many subgames, created on several host threads (the host plan
+// dominates their creation); the first failure is returned.
+int create_sessions(const std::vector<const Problem *> &pbs, const SolveConfig &cfg, std::vector<Session *> *out) {
+    const size_t n = pbs.size();
+    out->assign(n, nullptr);
+    std::vector<int> rcs(n, SS_OK);
+    std::vector<std::string> errs(n);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(n, std::min(16u, hw));
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (;;) {
+            const size_t i = next++;
+            if (i >= n) return;
+            rcs[i] = session_create(*pbs[i], cfg, &(*out)[i]);
+            if (rcs[i] != SS_OK) errs[i] = last_error();
+        }
+    };
+    std::vector<std::thread> th;
+    for (size_t k = 1; k < nt; ++k) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+    for (size_t i = 0; i < n; ++i)
+        if (rcs[i] != SS_OK) {
+            for (Session *s : *out) delete s;
+            out->assign(n, nullptr);
+            set_error(errs[i]);
+            return rcs[i];
+        }
+    return SS_OK;
+}
 
 int batch_solve(const std::vector<Problem> &pbs, int max_iterations, const SolveConfig &cfg, SSOutput *outs,
                 SSSolveStats *stats) {
@@ -307,11 +541,22 @@ int batch_solve(const std::vector<Problem> &pbs, int max_iterations, const Solve
     Batch b;
     int rc = b.init(cfg.device, cfg.graph_iterations);
     if (rc != SS_OK) return rc;
-    for (const Problem &pb : pbs) {
-        Session *s = nullptr;
-        rc = session_create(pb, cfg, &s);
+    {
+        std::vector<const Problem *> ptrs;
+        for (const Problem &pb : pbs) ptrs.push_back(&pb);
+        SolveConfig mcfg = cfg;
+        mcfg.batch_member = 1;
+        std::vector<Session *> made;
+        rc = create_sessions(ptrs, mcfg, &made);
         if (rc != SS_OK) return rc;
-        b.add(s);
+        for (size_t i = 0; i < made.size(); ++i) {
+            int slot = -1;
+            rc = b.add(made[i], &slot);
+            if (rc != SS_OK) {
+                for (size_t j = i; j < made.size(); ++j) delete made[j];
+                return rc;
+            }
+        }
     }
     const bool target = cfg.target_exploitability > 0.f;
     const int step = target ? std::max(1, cfg.check_every) : std::max(1, max_iterations);
@@ -329,21 +574,27 @@ int batch_solve(const std::vector<Problem> &pbs, int max_iterations, const Solve
         rc = b.run(n);
         if (rc != SS_OK) break;
         BCK(cudaEventRecord(e1, b.stream));
-        rc = b.sync();
+        bool any_last = false;
+        for (size_t i = 0; i < pbs.size(); ++i)
+            if (b.active[i] && b.iters_run[i] >= max_iterations) any_last = true;
+        if (target || (any_last && cfg.compute_exploitability))
+            rc = b.check(pct, nash);
+        else
+            rc = b.sync();
         if (rc != SS_OK) break;
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) total_ms += ms;
         for (size_t i = 0; i < pbs.size() && rc == SS_OK; ++i) {
             if (!b.active[i]) continue;
             const bool last = b.iters_run[i] >= max_iterations;
-            if (target || (last && cfg.compute_exploitability))
-                rc = b.subs[i]->exploitability(nullptr, &pct[i], &nash[i], nullptr, nullptr, nullptr);
-            if (last || (target && pct[i] <= cfg.target_exploitability)) b.retire(static_cast<int>(i));
+            if (last || (target && pct[i] <= cfg.target_exploitability)) rc = b.retire(static_cast<int>(i));
         }
         if (rc != SS_OK) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (rc != SS_OK) return rc;
+    rc = b.sync();
     if (rc != SS_OK) return rc;
     for (size_t i = 0; i < pbs.size(); ++i) {
         rc = b.subs[i]->output(&outs[i]);
@@ -387,6 +638,7 @@ struct Request {
     size_t bytes = 0;
     std::chrono::steady_clock::time_point t_submit, t_done;
     int slot = -1;
+    int iters_done = 0;  // iterations run so far (updated after each block)
     int state = 0;  // 0 pending, 1 running, 2 done, <0 failed with that code
     std::string error;
     SSOutput out{};
@@ -413,14 +665,16 @@ class Server {
     SSServerOptions opt{};
     Batch batch;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
-    std::deque<Request *> pending;
+    std::condition_variable cv_work, cv_done, cv_admit;
+    std::deque<Request *> pending;                     // submitted, not yet admitted
+    std::deque<std::pair<Request *, Session *>> ready;  // admitted, session built, not yet in the batch
     std::map<long long, std::unique_ptr<Request>> reqs;
     std::vector<Request *> slot_req;
     size_t used = 0;
+    int building = 0;                                  // requests whose session is being built
     long long next_id = 1;
     bool stop = false;
-    std::thread worker;
+    std::thread worker, admitter;
     int fatal = SS_OK;
     std::string fatal_msg;
 
@@ -429,6 +683,7 @@ class Server {
         int rc = batch.init(o.device, o.graph_iterations);
         if (rc != SS_OK) return rc;
         worker = std::thread([this] { loop(); });
+        admitter = std::thread([this] { admit_loop(); });
         return SS_OK;
     }
 
@@ -438,7 +693,10 @@ class Server {
             stop = true;
         }
         cv_work.notify_all();
+        cv_admit.notify_all();
+        if (admitter.joinable()) admitter.join();
         if (worker.joinable()) worker.join();
+        for (auto &rs : ready) delete rs.second;
         for (auto &kv : reqs) {
             SSOutput &o = kv.second->out;
             std::free(o.root_strategy);
@@ -482,7 +740,7 @@ class Server {
         *id = r->id;
         pending.push_back(r.get());
         reqs[r->id] = std::move(r);
-        cv_work.notify_one();
+        cv_admit.notify_one();
         return SS_OK;
     }
 
@@ -525,86 +783,155 @@ class Server {
         return 0;
     }
 
+    int progress(long long id, int *state, int *iters) {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = reqs.find(id);
+        if (it == reqs.end()) {
+            set_error("unknown request id");
+            return SS_ERR_INVALID;
+        }
+        const Request *r = it->second.get();
+        if (r->state < 0) {
+            set_error(r->error);
+            return r->state;
+        }
+        if (state) *state = r->state;
+        if (iters) *iters = r->iters_done;
+        return SS_OK;
+    }
+
   private:
-    void fail(Request *r, int rc) {
+    void fail(Request *r, int rc, const std::string &msg) {
         r->state = rc;
-        r->error = last_error();
+        r->error = msg;
         r->t_done = std::chrono::steady_clock::now();
+    }
+
+    // Admission: takes pending requests in order while their estimated
+    // footprint fits the memory budget (or nothing else is resident) and
+    // builds their sessions -- host plan, allocation, upload on the session's
+    // own stream -- off the worker thread, so the batch keeps running
+    // meanwhile; the worker adds them between iteration blocks.
+    void admit_loop() {
+        cudaSetDevice(opt.device);
+        const size_t budget = static_cast<size_t>(opt.memory_budget_gb * 1e9);
+        SolveConfig cfg;
+        cfg.device = opt.device;
+        cfg.graph_iterations = opt.graph_iterations;
+        cfg.batch_member = 1;
+        for (;;) {
+            Request *r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_admit.wait(lk, [&] {
+                    if (stop || fatal != SS_OK) return true;
+                    if (pending.empty()) return false;
+                    const bool alone = used == 0;
+                    return alone || used + pending.front()->bytes <= budget;
+                });
+                if (stop || fatal != SS_OK) return;
+                r = pending.front();
+                pending.pop_front();
+                used += r->bytes;
+                ++building;
+            }
+            Session *s = nullptr;
+            int rc = session_create(r->pb, cfg, &s);
+            if (rc == SS_OK) rc = s->ensure_br();
+            std::string msg = rc == SS_OK ? std::string() : std::string(last_error());
+            std::lock_guard<std::mutex> lk(mu);
+            --building;
+            if (rc != SS_OK) {
+                delete s;
+                used -= r->bytes;
+                fail(r, rc, msg);
+                cv_done.notify_all();
+                cv_admit.notify_all();
+                continue;
+            }
+            ready.emplace_back(r, s);
+            cv_work.notify_one();
+        }
     }
 
     void loop() {
         cudaSetDevice(opt.device);
-        const size_t budget = static_cast<size_t>(opt.memory_budget_gb * 1e9);
         const int block = std::max(1, opt.block_iterations);
+        std::vector<double> pct, nash;
         for (;;) {
-            std::vector<Request *> admit;
+            std::vector<std::pair<Request *, Session *>> add;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stop || !pending.empty() || batch.num_active() > 0; });
+                cv_work.wait(lk, [&] { return stop || !ready.empty() || batch.num_active() > 0; });
                 if (stop) return;
-                while (!pending.empty()) {
-                    Request *r = pending.front();
-                    if (batch.num_active() + static_cast<int>(admit.size()) > 0 && used + r->bytes > budget) break;
-                    pending.pop_front();
-                    used += r->bytes;
-                    admit.push_back(r);
+                while (!ready.empty()) {
+                    add.push_back(ready.front());
+                    ready.pop_front();
                 }
             }
-            for (Request *r : admit) {
-                SolveConfig cfg;
-                cfg.device = opt.device;
-                cfg.graph_iterations = opt.graph_iterations;
-                Session *s = nullptr;
-                int rc = session_create(r->pb, cfg, &s);
+            for (auto &rs : add) {
+                Request *r = rs.first;
+                int slot = -1;
+                int rc = batch.add(rs.second, &slot);
                 std::lock_guard<std::mutex> lk(mu);
                 if (rc != SS_OK) {
+                    delete rs.second;
                     used -= r->bytes;
-                    fail(r, rc);
+                    fail(r, rc, last_error());
                     cv_done.notify_all();
+                    cv_admit.notify_all();
                     continue;
                 }
-                r->slot = batch.add(s);
+                r->slot = slot;
                 r->state = 1;
-                if (static_cast<int>(slot_req.size()) <= r->slot) slot_req.resize(r->slot + 1, nullptr);
-                slot_req[r->slot] = r;
+                if (static_cast<int>(slot_req.size()) <= slot) slot_req.resize(slot + 1, nullptr);
+                slot_req[slot] = r;
             }
             if (batch.num_active() == 0) continue;
             int rc = batch.run(block);
-            if (rc == SS_OK) rc = batch.sync();
+            if (rc == SS_OK) rc = batch.check(pct, nash);
             if (rc != SS_OK) {
                 std::lock_guard<std::mutex> lk(mu);
                 fatal = rc;
                 fatal_msg = last_error();
+                for (Request *r : slot_req)
+                    if (r && r->state == 1) fail(r, rc, fatal_msg);
                 cv_done.notify_all();
+                cv_admit.notify_all();
                 return;
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                for (size_t i = 0; i < batch.subs.size(); ++i)
+                    if (batch.active[i]) slot_req[i]->iters_done = batch.iters_run[i];
             }
             for (size_t i = 0; i < batch.subs.size(); ++i) {
                 if (!batch.active[i]) continue;
                 Request *r = slot_req[i];
-                double pct = -1, nash = -1;
-                rc = batch.subs[i]->exploitability(nullptr, &pct, &nash, nullptr, nullptr, nullptr);
                 const bool cap = batch.iters_run[i] >= opt.max_iterations;
-                if (rc == SS_OK && !(cap || pct <= opt.target_exploitability)) continue;
-                batch.retire(static_cast<int>(i));
+                if (!(cap || pct[i] <= opt.target_exploitability)) continue;
+                rc = batch.retire(static_cast<int>(i));
                 SSOutput o{};
                 if (rc == SS_OK) rc = batch.subs[i]->output(&o);
+                const std::string msg = rc == SS_OK ? std::string() : std::string(last_error());
                 const double nhu = batch.subs[i]->P.node_hands * batch.iters_run[i];
                 batch.release(static_cast<int>(i));
                 std::lock_guard<std::mutex> lk(mu);
                 used -= r->bytes;
                 if (rc != SS_OK) {
-                    fail(r, rc);
+                    fail(r, rc, msg);
                 } else {
                     r->out = o;
                     r->stats.iterations_run = batch.iters_run[i];
-                    r->stats.exploitability_pct = pct;
-                    r->stats.nashconv = nash;
+                    r->stats.exploitability_pct = pct[i];
+                    r->stats.nashconv = nash[i];
                     r->stats.node_hand_updates = nhu;
                     r->t_done = std::chrono::steady_clock::now();
                     r->state = 2;
                 }
                 slot_req[i] = nullptr;
                 cv_done.notify_all();
+                cv_admit.notify_all();
             }
         }
     }
@@ -624,6 +951,8 @@ int server_submit(Server *s, const Problem &pb, long long *id) { return s->submi
 int server_poll(Server *s, long long id, SSOutput *out, SSSolveStats *stats, double *lat, int wait) {
     return s->poll(id, out, stats, lat, wait != 0);
 }
+
+int server_progress(Server *s, long long id, int *state, int *iters) { return s->progress(id, state, iters); }
 
 void server_destroy(Server *s) { delete s; }
 

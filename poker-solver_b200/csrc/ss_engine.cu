@@ -180,10 +180,14 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     CK(cudaSetDevice(device));
     keep_pool_warm(device);
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    for (int k = 0; k < TK_COUNT; ++k) {
-        CK(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    if (!cfg.batch_member) {
+        // side streams of the session's own captured iterations (a batch
+        // member's launches are the batch's)
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        for (int k = 0; k < TK_COUNT; ++k) {
+            CK(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+        }
     }
     const int np = P.np;
     const size_t HS = static_cast<size_t>(P.HS);
@@ -247,6 +251,8 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
         dpl.push_back(pb.nodes[x].player);
     }
     const size_t o_dfe = b.add(dfe), o_dna = b.add(dna), o_dpl = b.add(dpl);
+    dec_na_host = dna;
+    dec_player_host = dpl;
     CK(cudaMallocAsync(reinterpret_cast<void **>(&dbase), std::max<size_t>(b.host.size(), 256), stream));
     CK(cudaMemcpyAsync(dbase, b.host.data(), b.host.size(), cudaMemcpyHostToDevice, stream));
     for (int p = 0; p < np; ++p) {
@@ -259,6 +265,10 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     dec_fe = reinterpret_cast<const int *>(dbase + o_dfe);
     dec_na = reinterpret_cast<const int *>(dbase + o_dna);
     dec_pl = reinterpret_cast<const int *>(dbase + o_dpl);
+    c.dec_fe = dec_fe;
+    c.dec_na = dec_na;
+    c.dec_pl = dec_pl;
+    c.live = 1;
 
     // ---- state: regrets, strategy sums, reach (weights in the last np rows), values
     nR = E * HS;
@@ -449,20 +459,16 @@ int Session::profile(SSKernelProfile *prof) {
     return SS_OK;
 }
 
-// NashConv of an average-strategy profile (the session's own when host_avg is
-// null, else avg given in the SSOutput layout), FP64 throughout: every
-// player's reach under the profile, then per player the terminal values
-// (same closed forms as the CFR path, in double), the profile value and the
-// best-response value at its own nodes, and the root sums weighted by the
-// player's range.  Exploitability = NashConv / np / starting pot * 100.
-int Session::exploitability(const float *host_avg, double *pct, double *nash, double *br, double *cur,
-                            double *deal_mass) {
-    CK(cudaSetDevice(device));
+// Best-response buffers (FP64 reach and values, the profile, the edge ->
+// decision table, the deal-mass item and the root sums), allocated on first
+// use and kept; also points the context at them, so that the batched checks
+// can run this session's best response from the batch's context array.
+int Session::ensure_br() {
+    if (dbr) return SS_OK;
     const int np = P.np;
     const size_t HS = static_cast<size_t>(P.HS), E = static_cast<size_t>(P.E), N = static_cast<size_t>(P.N);
     const size_t n_avg = static_cast<size_t>(P.num_dec) * SS_MAX_ACTIONS * P.max_h;
     // deal mass term: the players' ranges against each other (valid deals)
-    TermItem deal;
     std::memset(&deal, 0, sizeof(deal));
     deal.node = P.N;
     deal.leaf_off = -1;
@@ -474,11 +480,11 @@ int Session::exploitability(const float *host_avg, double *pct, double *nash, do
     }
     const bool deal_cr3 = np == 4 && !P.dup[1] && !P.dup[2] && P.H[1] >= kCr3MinHands &&
                           P.H[2] >= kCr3MinHands && P.H[3] >= kCr3MinHands;
-    const int deal_kind = np == 1   ? TK_LEAF0
-                          : np == 2 ? (P.dup[1] ? TK_CR1D : TK_CR1)
-                          : np == 3 ? TK_CR2
-                          : deal_cr3 ? TK_CR3
-                                     : TK_ENUM;
+    deal_kind = np == 1   ? TK_LEAF0
+                : np == 2 ? (P.dup[1] ? TK_CR1D : TK_CR1)
+                : np == 3 ? TK_CR2
+                : deal_cr3 ? TK_CR3
+                           : TK_ENUM;
     if (deal_kind == TK_ENUM) {
         double w = P.H[0];
         for (int o = 1; o < np; ++o) w *= std::max(1, P.H[o]);
@@ -488,40 +494,49 @@ int Session::exploitability(const float *host_avg, double *pct, double *nash, do
             return SS_ERR_UNSUPPORTED;
         }
     }
-    if (!dbr) {
-        CK(cudaMallocAsync(reinterpret_cast<void **>(&dbr), ((E + np) + (N + 1)) * HS * sizeof(double), stream));
-        CK(cudaMemsetAsync(dbr, 0, ((E + np) + (N + 1)) * HS * sizeof(double), stream));
-        std::vector<double> w(host_w.begin(), host_w.end());
-        CK(cudaMemcpyAsync(dbr + E * HS, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-        Blob t;
-        std::vector<int> node_di(P.N, -1), edge_di(P.E);
-        for (int i = 0; i < P.num_dec; ++i) node_di[P.dec_nodes[i]] = i;
-        for (int e = 0; e < P.E; ++e) edge_di[e] = node_di[P.edge_node[e]];
-        t.add(edge_di);
-        t.add(&deal, sizeof(deal));
-        const int nrow = P.N;
-        t.add(&nrow, sizeof(int));
-        t.add(nullptr, (2 * SS_MAX_PLAYERS + 2) * sizeof(double));
-        CK(cudaMallocAsync(reinterpret_cast<void **>(&dbr_tab), t.host.size(), stream));
-        CK(cudaMemcpyAsync(dbr_tab, t.host.data(), t.host.size(), cudaMemcpyHostToDevice, stream));
-        CK(cudaMallocAsync(reinterpret_cast<void **>(&davg_br), std::max<size_t>(n_avg, 1) * sizeof(float), stream));
-        CK(cudaStreamSynchronize(stream));  // host staging must outlive the copies
-    }
+    CK(cudaSetDevice(device));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dbr), ((E + np) + (N + 1)) * HS * sizeof(double), stream));
+    CK(cudaMemsetAsync(dbr, 0, ((E + np) + (N + 1)) * HS * sizeof(double), stream));
+    std::vector<double> w(host_w.begin(), host_w.end());
+    CK(cudaMemcpyAsync(dbr + E * HS, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    Blob t;
+    std::vector<int> node_di(P.N, -1), edge_di(P.E);
+    for (int i = 0; i < P.num_dec; ++i) node_di[P.dec_nodes[i]] = i;
+    for (int e = 0; e < P.E; ++e) edge_di[e] = node_di[P.edge_node[e]];
+    const size_t o_edge = t.add(edge_di);
+    const size_t o_deal = t.add(&deal, sizeof(deal));
+    const int nrow = P.N;
+    const size_t o_row = t.add(&nrow, sizeof(int));
+    const size_t o_sc = t.add(nullptr, (2 * SS_MAX_PLAYERS + 2) * sizeof(double));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&dbr_tab), t.host.size(), stream));
+    CK(cudaMemcpyAsync(dbr_tab, t.host.data(), t.host.size(), cudaMemcpyHostToDevice, stream));
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&davg_br), std::max<size_t>(n_avg, 1) * sizeof(float), stream));
+    CK(cudaStreamSynchronize(stream));  // host staging must outlive the copies
+    br_edge_di = reinterpret_cast<const int *>(dbr_tab + o_edge);
+    br_deal = reinterpret_cast<const TermItem *>(dbr_tab + o_deal);
+    br_row = reinterpret_cast<const int *>(dbr_tab + o_row);
+    br_sc = reinterpret_cast<double *>(dbr_tab + o_sc);
     c.reach_d = dbr;
     c.val_d = dbr + (E + np) * HS;
-    // table offsets (same order as written above)
-    size_t off = 0;
-    auto next = [&](size_t bytes) {
-        off = (off + 255) & ~static_cast<size_t>(255);
-        size_t r = off;
-        off += bytes;
-        return r;
-    };
-    const int *edge_di = reinterpret_cast<const int *>(dbr_tab + next(P.E * sizeof(int)));
-    const TermItem *d_deal = reinterpret_cast<const TermItem *>(dbr_tab + next(sizeof(TermItem)));
-    const int *d_row = reinterpret_cast<const int *>(dbr_tab + next(sizeof(int)));
-    double *d_sc = reinterpret_cast<double *>(dbr_tab + next((2 * SS_MAX_PLAYERS + 2) * sizeof(double)));
+    c.avg_br = davg_br;
+    c.edge_di = br_edge_di;
+    c.max_h = P.max_h;
+    return SS_OK;
+}
 
+// NashConv of an average-strategy profile (the session's own when host_avg is
+// null, else avg given in the SSOutput layout), FP64 throughout: every
+// player's reach under the profile, then per player the terminal values
+// (same closed forms as the CFR path, in double), the profile value and the
+// best-response value at its own nodes, and the root sums weighted by the
+// player's range.  Exploitability = NashConv / np / starting pot * 100.
+int Session::exploitability(const float *host_avg, double *pct, double *nash, double *br, double *cur,
+                            double *deal_mass) {
+    int rc = ensure_br();
+    if (rc != SS_OK) return rc;
+    CK(cudaSetDevice(device));
+    const int np = P.np;
+    const size_t n_avg = static_cast<size_t>(P.num_dec) * SS_MAX_ACTIONS * P.max_h;
     if (host_avg)
         CK(cudaMemcpyAsync(davg_br, host_avg, n_avg * sizeof(float), cudaMemcpyHostToDevice, stream));
     else
@@ -529,23 +544,32 @@ int Session::exploitability(const float *host_avg, double *pct, double *nash, do
     for (int p = 0; p < np; ++p)
         for (size_t l = 0; l < reach_lv[p].size(); ++l)
             CK(launch_br_reach(c, reach_items[p] + reach_lv[p][l].first, reach_lv[p][l].second, P.H[p],
-                               davg_br, edge_di, P.max_h, stream));
+                               davg_br, br_edge_di, P.max_h, stream));
     for (int t = 0; t < np; ++t) {
         for (int k = 0; k < TK_COUNT; ++k)
             CK(launch_terms_fp64(c, k, term_items[t][k], static_cast<int>(P.term[t][k].size()), t, stream));
         for (int mode = 0; mode < 2; ++mode) {
             for (size_t l = 0; l < cfv_lv[t].size(); ++l)
                 CK(launch_br_value(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.H[t],
-                                   davg_br, edge_di, P.max_h, mode, stream));
+                                   davg_br, br_edge_di, P.max_h, mode, stream));
             CK(launch_br_root(c, root_fr[t], static_cast<int>(P.root_fr[t].size()), P.H[t], P.E + t, t, 0,
-                              d_sc + 2 * t + mode, stream));
+                              br_sc + 2 * t + mode, stream));
         }
     }
-    CK(launch_terms_fp64(c, deal_kind, d_deal, 1, 0, stream));
-    CK(launch_br_root(c, d_row, 1, P.H[0], P.E, 0, 1, d_sc + 2 * SS_MAX_PLAYERS, stream));
+    CK(launch_terms_fp64(c, deal_kind, br_deal, 1, 0, stream));
+    CK(launch_br_root(c, br_row, 1, P.H[0], P.E, 0, 1, br_sc + 2 * SS_MAX_PLAYERS, stream));
     double sc[2 * SS_MAX_PLAYERS + 2] = {};
-    CK(cudaMemcpyAsync(sc, d_sc, sizeof(sc), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(sc, br_sc, sizeof(sc), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    nashconv_from_sums(sc, pct, nash, br, cur, deal_mass);
+    return SS_OK;
+}
+
+// sc: per traverser t, [2t] profile value and [2t + 1] best-response value;
+// [2 * SS_MAX_PLAYERS] the deal mass
+void Session::nashconv_from_sums(const double *sc, double *pct, double *nash, double *br, double *cur,
+                                 double *deal_mass) const {
+    const int np = P.np;
     double nc = 0.0;
     for (int t = 0; t < np; ++t) {
         if (cur) cur[t] = sc[2 * t];
@@ -557,7 +581,6 @@ int Session::exploitability(const float *host_avg, double *pct, double *nash, do
     const double nash_v = z > 0 ? nc / z : 0.0;
     if (nash) *nash = nash_v;
     if (pct) *pct = P.starting_pot > 0 ? nash_v / np / P.starting_pot * 100.0 : 0.0;
-    return SS_OK;
 }
 
 // ---------------------------------------------------------------------------

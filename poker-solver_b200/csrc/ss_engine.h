@@ -244,6 +244,7 @@ struct SolveConfig {
     float target_exploitability = -1.f;
     int check_every = 50;
     int compute_exploitability = 0;
+    int batch_member = 0;    // the session only runs inside a batch (no launches of its own iterations)
 };
 
 int solve(const Problem &pb, int iterations, const SolveConfig &cfg, SSOutput *out,
@@ -262,6 +263,9 @@ void session_destroy(Session *s);
 void *session_stream(Session *s);
 int session_exploitability(Session *s, const float *host_avg, double *pct, double *nash, double *br,
                            double *cur, double *z);
+// ss_narrow.cu: the reference's range update from the session's average strategy
+int session_narrow(Session *s, int player, int node, unsigned action_mask, int n, const int *hand_cards,
+                   double *weights, int *applied);
 
 // ss_batch.cu: batched and served forms
 int batch_solve(const std::vector<Problem> &pbs, int max_iterations, const SolveConfig &cfg, SSOutput *outs,
@@ -270,6 +274,7 @@ class Server;
 int server_create(const SSServerOptions &o, Server **out);
 int server_submit(Server *s, const Problem &pb, long long *id);
 int server_poll(Server *s, long long id, SSOutput *out, SSSolveStats *stats, double *latency_ms, int wait);
+int server_progress(Server *s, long long id, int *state, int *iterations_run);
 void server_destroy(Server *s);
 
 // ss_noalloc.cu: solve with all device state in a static device array

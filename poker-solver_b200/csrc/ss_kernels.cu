@@ -75,6 +75,11 @@ __device__ __forceinline__ void regret_match4(const float *__restrict__ R, size_
 // reach: reach[first_edge + a] = reach[parent_row] * sigma_a
 // (street_solve.cu:650-683, stored per sequence instead of per node)
 // --------------------------------------------------------------------------
+// Batched form: a subgame that has left the batch keeps its items in the
+// captured launches; their blocks return at once.  Every block serves one
+// subgame, so the test is block-uniform (ahead of any barrier).
+__device__ __forceinline__ bool retired(const DevCtx *ctxs, int sg) { return ctxs && !ctxs[sg].live; }
+
 __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                         const ReachItem *__restrict__ items, int nchunk, int H,
                                                         int p) {
@@ -82,6 +87,7 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
     const ReachItem I = items[it];
+    if (retired(ctxs, I.sg)) return;
     // context fields in registers (a reference to either the parameter or a
     // batch entry would send every field read through local memory)
     float *R, *reach;
@@ -151,6 +157,7 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const CfvItem I = items[it];
+    if (retired(ctxs, I.sg)) return;
     const CfvView V = ctxs ? cfv_view(ctxs[I.sg], ctxs[I.sg].H[trav]) : cfv_view(c0, Hl);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int h0 = (S == 1 ? ch * (kCfvThreads / 32) + warp : ch) * 64 + lane * 2;
@@ -324,6 +331,7 @@ __global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c0, const Dev
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
     const TermItem I = items[it];
+    if (retired(ctxs, I.sg)) return;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     if (h0 >= c.HS) return;
     const int Ht = c.H[trav];
@@ -442,6 +450,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1_dup(DevCtx c0, const 
     double *F = cv.take<double>(1);
     int *npos = cv.take<int>(1);
     const TermItem I = items[blockIdx.x];
+    if (retired(ctxs, I.sg)) return;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     zero_matrix(M);
@@ -786,6 +795,7 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     extern __shared__ __align__(16) char smem[];
     const TermItem *I0 = items + blockIdx.x;
     if (I0->follow) return;   // written by the block of its group's first item
+    if (retired(ctxs, I0->sg)) return;
     const int ng = I0->gextra + 1;
     const int o0 = I0->opp_player[0], o1 = I0->opp_player[1];
     const Cr2View<T> V = ctxs ? cr2_view<T>(ctxs[I0->sg], trav, o0, o1) : cr2_view<T>(c0, trav, o0, o1);
@@ -981,6 +991,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevC
     extern __shared__ __align__(16) char smem[];
     const TermItem *I0 = items + blockIdx.x;
     if (I0->follow) return;   // written by the block of its group's first item
+    if (retired(ctxs, I0->sg)) return;
     const int ng = I0->gextra + 1;
     const int o = I0->opp_player[0];
     const Cr2View<T> V = ctxs ? cr2_view<T>(ctxs[I0->sg], trav, o, o) : cr2_view<T>(c0, trav, o, o);
@@ -1108,6 +1119,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
     unsigned long long *B = cv.take<unsigned long long>(52);
     int *npos = cv.take<int>(1);
     const TermItem I = items[blockIdx.x];
+    if (retired(ctxs, I.sg)) return;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nc = c.ncomb;
@@ -1582,6 +1594,7 @@ __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const D
     extern __shared__ __align__(16) char smem[];
     const int per = kSd2Chunks >> lgm;
     const TermItem I = items[blockIdx.x / per];
+    if (retired(ctxs, I.sg)) return;
     const int grp = blockIdx.x % per;
     const int o1 = I.opp_player[0], o2 = I.opp_player[1];
     const T *reach;
@@ -1771,6 +1784,7 @@ __global__ void __launch_bounds__(128) k_term_enum(DevCtx c0, const DevCtx *__re
     const int ch = blockIdx.x - it * nchunk;
     const int h = ch * blockDim.x + threadIdx.x;
     const TermItem I = items[it];
+    if (retired(ctxs, I.sg)) return;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     if (h >= c.HS) return;
     T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
@@ -1873,6 +1887,7 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     const int ch = blockIdx.x - it * nchunk;
     const TermItem *I0 = items + it;
     if (I0->follow) return;   // written by the blocks of its group's first item
+    if (retired(ctxs, I0->sg)) return;
     const int ng = I0->gextra + 1;
     const TermItem I = *I0;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
@@ -1958,6 +1973,7 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const TermItem I = items[it];
+    if (retired(ctxs, I.sg)) return;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
     const int HS = c.HS;
     if (HS > c0.HS || c.deck > cr3::kS - 1) return;
@@ -2125,10 +2141,110 @@ __global__ void __launch_bounds__(1024) k_br_root(DevCtx c, const int *__restric
     }
 }
 
+// Batched best response: the kernels above with every item reading its own
+// subgame's context (its FP64 rows, profile and tables); blocks of subgames
+// that have left the batch return at once.
+__global__ void __launch_bounds__(128) k_avg_many(const DevCtx *__restrict__ ctxs,
+                                                  const AvgItem *__restrict__ items, int nchunk) {
+    const int it = blockIdx.x / nchunk;
+    const AvgItem I = items[it];
+    if (!ctxs[I.sg].live) return;
+    const DevCtx &c = ctxs[I.sg];
+    const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
+    const int max_h = c.max_h;
+    if (h >= max_h) return;
+    const int fe = c.dec_fe[I.di], na = c.dec_na[I.di], p = c.dec_pl[I.di];
+    float *o = c.avg_br + static_cast<size_t>(I.di) * SS_MAX_ACTIONS * max_h;
+    if (h >= c.H[p]) {
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) o[static_cast<size_t>(a) * max_h + h] = 0.f;
+        return;
+    }
+    float v[SS_MAX_ACTIONS];
+    float sum = 0.f;
+    for (int a = 0; a < na; ++a) {
+        float x = c.S[static_cast<size_t>(fe + a) * c.HS + h];
+        x = x < 0.f ? 0.f : x;
+        v[a] = x;
+        sum += x;
+    }
+    const float inv = sum > 0.f ? 1.0f / sum : 1.0f / static_cast<float>(na);
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+        o[static_cast<size_t>(a) * max_h + h] = a < na ? (sum > 0.f ? v[a] * inv : inv) : 0.f;
+}
+
+__global__ void __launch_bounds__(128) k_br_reach_many(const DevCtx *__restrict__ ctxs,
+                                                       const ReachItem *__restrict__ items, int nchunk, int p) {
+    const int it = blockIdx.x / nchunk;
+    const ReachItem I = items[it];
+    if (!ctxs[I.sg].live) return;
+    const DevCtx &c = ctxs[I.sg];
+    const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
+    if (h >= c.H[p]) return;
+    const size_t HS = static_cast<size_t>(c.HS);
+    const int di = c.edge_di[I.first_edge];
+    const double pr = c.reach_d[static_cast<size_t>(I.parent_row) * HS + h];
+    for (int a = 0; a < I.na; ++a)
+        c.reach_d[static_cast<size_t>(I.first_edge + a) * HS + h] = pr * avg_sigma(c.avg_br, di, a, h, c.max_h, I.frozen);
+}
+
+__global__ void __launch_bounds__(128) k_br_value_many(const DevCtx *__restrict__ ctxs,
+                                                       const CfvItem *__restrict__ items, int nchunk, int trav,
+                                                       int mode) {
+    const int it = blockIdx.x / nchunk;
+    const CfvItem I = items[it];
+    if (!ctxs[I.sg].live) return;
+    const DevCtx &c = ctxs[I.sg];
+    const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
+    if (h >= c.H[trav]) return;
+    const size_t HS = static_cast<size_t>(c.HS);
+    const int di = c.edge_di[I.first_edge];
+    double v = mode == 1 ? -1e300 : 0.0;
+    double vf = 0.0;
+    for (int a = 0; a < I.na; ++a) {
+        double e = 0.0;
+        for (int k = c.fr_off[I.first_edge + a]; k < c.fr_off[I.first_edge + a + 1]; ++k)
+            e += c.val_d[static_cast<size_t>(c.fr_items[k]) * HS + h];
+        if (mode == 1) {
+            v = e > v ? e : v;
+            if (a == I.frozen) vf = e;
+        } else {
+            v += avg_sigma(c.avg_br, di, a, h, c.max_h, I.frozen) * e;
+        }
+    }
+    if (mode == 1 && I.frozen >= 0 && I.frozen < I.na) v = vf;
+    c.val_d[static_cast<size_t>(I.node) * HS + h] = v;
+}
+
+// one block per item, same fixed reduction order as k_br_root
+__global__ void __launch_bounds__(1024) k_br_root_many(const DevCtx *__restrict__ ctxs,
+                                                       const RootItem *__restrict__ items, double *out) {
+    __shared__ double part[32];
+    const RootItem I = items[blockIdx.x];
+    if (!ctxs[I.sg].live) return;
+    const DevCtx &c = ctxs[I.sg];
+    const size_t HS = static_cast<size_t>(c.HS);
+    const int H = c.H[I.trav];
+    double acc = 0.0;
+    for (int h = threadIdx.x; h < H; h += blockDim.x) {
+        if (I.skip_blocked && (c.hand_code[I.trav * HS + h] & 0x10000)) continue;
+        double s = 0.0;
+        for (int k = 0; k < I.n; ++k) s += c.val_d[static_cast<size_t>(I.rows[k]) * HS + h];
+        acc += c.reach_d[static_cast<size_t>(I.weight_row) * HS + h] * s;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < blockDim.x / 32 ? part[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) out[I.slot] = v;
+    }
+}
+
 // batched form: advance the iteration counter of every listed subgame
 __global__ void k_bump_many(const DevCtx *__restrict__ ctxs, const int *__restrict__ sgs, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) *const_cast<int *>(ctxs[sgs[i]].iter) += 1;
+    if (i < n && ctxs[sgs[i]].live) *const_cast<int *>(ctxs[sgs[i]].iter) += 1;
 }
 
 // batched form: root strategy snapshot (regret matching of the root node)
@@ -2136,6 +2252,7 @@ __global__ void k_bump_many(const DevCtx *__restrict__ ctxs, const int *__restri
 __global__ void __launch_bounds__(128) k_snapshot_many(const DevCtx *__restrict__ ctxs,
                                                        const int *__restrict__ sgs) {
     const DevCtx &c = ctxs[sgs[blockIdx.x]];
+    if (!c.live) return;
     const int H = c.H[c.root_player];
     for (int h0 = threadIdx.x * 4; h0 < H; h0 += blockDim.x * 4) {
         float r[SS_MAX_ACTIONS][4], sig[SS_MAX_ACTIONS][4];
@@ -2316,8 +2433,37 @@ cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n
 }
 
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                              cudaStream_t s) {
-    return launch_terms_t<double>(c, kind, items, n, trav, s, nullptr);
+                              cudaStream_t s, const DevCtx *ctxs) {
+    return launch_terms_t<double>(c, kind, items, n, trav, s, ctxs);
+}
+
+cudaError_t launch_avg_many(const DevCtx *ctxs, const AvgItem *items, int n, int max_h, cudaStream_t s) {
+    if (n <= 0 || max_h <= 0) return cudaSuccess;
+    const int nc = (max_h + 127) / 128;
+    k_avg_many<<<n * nc, 128, 0, s>>>(ctxs, items, nc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_br_reach_many(const DevCtx *ctxs, const ReachItem *items, int n, int H, int player,
+                                 cudaStream_t s) {
+    if (n <= 0 || H <= 0) return cudaSuccess;
+    const int nc = (H + 127) / 128;
+    k_br_reach_many<<<n * nc, 128, 0, s>>>(ctxs, items, nc, player);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_br_value_many(const DevCtx *ctxs, const CfvItem *items, int n, int H, int trav, int mode,
+                                 cudaStream_t s) {
+    if (n <= 0 || H <= 0) return cudaSuccess;
+    const int nc = (H + 127) / 128;
+    k_br_value_many<<<n * nc, 128, 0, s>>>(ctxs, items, nc, trav, mode);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_br_root_many(const DevCtx *ctxs, const RootItem *items, int n, double *out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_br_root_many<<<n, 1024, 0, s>>>(ctxs, items, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_bump(int *iter, cudaStream_t s) {

@@ -40,6 +40,35 @@ struct DevCtx {
     // root strategy snapshot (batched form: one launch covers many subgames)
     float *snap;
     int root_fe, root_na, root_frozen, root_player;
+    // batched form: 0 once the subgame has left the batch; its items stay in
+    // the captured launches and their blocks return at once
+    int live;
+    // best response (FP64 exploitability; set once its buffers exist)
+    float *avg_br;            // profile in the output layout [num_dec][8][max_h]
+    const int *edge_di;       // [E] decision index of each edge's node
+    const int *dec_fe;        // [num_dec] first edge, actions, acting player
+    const int *dec_na;
+    const int *dec_pl;
+    int max_h;
+};
+
+// Batched best response: the root sums of one subgame, one block each.
+// out[slot] = sum over hands h of the traverser's range weight (reach_d row
+// weight_row) x the sum of val_d over rows[0 .. n).
+struct alignas(16) RootItem {
+    const int *rows;
+    int n;
+    int sg;
+    int trav;
+    int weight_row;
+    int skip_blocked;         // hands touching the board do not count
+    int slot;
+};
+
+// Batched average strategy: decision node di of subgame sg.
+struct alignas(8) AvgItem {
+    int sg;
+    int di;
 };
 
 // threads per block of the per-hand kernels; each thread covers 4 hands
@@ -64,7 +93,14 @@ cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long,
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s, const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                              cudaStream_t s);
+                              cudaStream_t s, const DevCtx *ctxs = nullptr);
+// batched best response: every item reads the context of its subgame (item.sg)
+cudaError_t launch_avg_many(const DevCtx *ctxs, const AvgItem *items, int n, int max_h, cudaStream_t s);
+cudaError_t launch_br_reach_many(const DevCtx *ctxs, const ReachItem *items, int n, int H, int player,
+                                 cudaStream_t s);
+cudaError_t launch_br_value_many(const DevCtx *ctxs, const CfvItem *items, int n, int H, int trav, int mode,
+                                 cudaStream_t s);
+cudaError_t launch_br_root_many(const DevCtx *ctxs, const RootItem *items, int n, double *out, cudaStream_t s);
 cudaError_t launch_bump(int *iter, cudaStream_t s);
 cudaError_t launch_bump_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s);
 cudaError_t launch_snapshot_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s);

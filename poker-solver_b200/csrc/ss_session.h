@@ -58,15 +58,22 @@ class Session {
     const TermItem *term_items[SS_MAX_PLAYERS][TK_COUNT] = {};
     const int *root_fr[SS_MAX_PLAYERS] = {};
     const int *dec_fe = nullptr, *dec_na = nullptr, *dec_pl = nullptr;
+    std::vector<int> dec_na_host, dec_player_host;   // per decision node (index order): actions, acting player
     // per (player, level) / (traverser, kind) minimum bytes, for the profile
     std::vector<double> reach_bytes[SS_MAX_PLAYERS], cfv_bytes[SS_MAX_PLAYERS];
     double term_bytes[SS_MAX_PLAYERS][TK_COUNT] = {};
     cudaGraphExec_t gA = nullptr, gC = nullptr, gB = nullptr;  // G iters, 1 iter, 1 iter + snapshot
-    // best response state (allocated on first use)
+    // best response state (allocated on first use, ensure_br)
     std::vector<float> host_w;          // range weights [np][HS]
     double *dbr = nullptr;              // reach_d [E + np][HS], val_d [N + 1][HS]
     char *dbr_tab = nullptr;            // edge -> decision index, deal item, row list, scalars
     float *davg_br = nullptr;           // profile in the output layout
+    const int *br_edge_di = nullptr;    // in dbr_tab: [E] decision index of each edge's node
+    const TermItem *br_deal = nullptr;  // in dbr_tab: the deal-mass item (val_d row N)
+    const int *br_row = nullptr;        // in dbr_tab: {N}
+    double *br_sc = nullptr;            // in dbr_tab: root sums (nashconv_from_sums layout)
+    TermItem deal{};
+    int deal_kind = TK_ENUM;
 
     // profiling hook: when set, every launch is preceded by an event record
     struct Mark {
@@ -203,8 +210,11 @@ class Session {
     }
 
     int init(const Problem &pb, const SolveConfig &cfg);
+    int ensure_br();
     int exploitability(const float *host_avg, double *pct, double *nash, double *br, double *cur,
                        double *deal_mass);
+    void nashconv_from_sums(const double *sc, double *pct, double *nash, double *br, double *cur,
+                            double *deal_mass) const;
     int reset();
     int run(int iters);
     int output(SSOutput *out);

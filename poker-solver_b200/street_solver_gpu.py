@@ -181,6 +181,22 @@ def load_library(max_hands=SS_MAX_HANDS):
     return lib
 
 
+def _session_api(lib):
+    """ctypes signatures of the resident-session entry points."""
+    vp = ctypes.c_void_p
+    lib.ss_session_create.restype = ctypes.c_int
+    lib.ss_session_run.restype = ctypes.c_int
+    lib.ss_session_run.argtypes = [vp, ctypes.c_int]
+    lib.ss_session_output.restype = ctypes.c_int
+    lib.ss_session_output.argtypes = [vp, ctypes.POINTER(SSOutput)]
+    lib.ss_session_destroy.restype = None
+    lib.ss_session_destroy.argtypes = [vp]
+    lib.ss_session_narrow.restype = ctypes.c_int
+    lib.ss_session_narrow.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_int)]
+
+
 def loaded_library():
     """A library build already loaded in this process (either layout), or
     None -- for entry points that do not depend on SS_MAX_HANDS."""
@@ -337,7 +353,10 @@ class StreetSolverGPU:
 
     # ── solving ──────────────────────────────────────────────────────────
     def solve(self, iterations=200, target_exploitability=None, graph_iterations=10, device=0,
-              compute_exploitability=False):
+              compute_exploitability=False, resident=False):
+        """resident=True keeps the solve's state on the GPU as a session (for
+        narrow_weights, more iterations, reads); otherwise one ss_solve_gpu_ex
+        call that allocates and releases everything."""
         if self._solved:
             self.lib.ss_free_output(ctypes.byref(self._output))
             self._solved = False
@@ -345,6 +364,24 @@ class StreetSolverGPU:
                               -1.0 if target_exploitability is None else float(target_exploitability),
                               50, 1 if compute_exploitability else 0)
         stats = SSSolveStats()
+        if resident:
+            self._drop_session()
+            _session_api(self.lib)
+            sess = ctypes.c_void_p()
+            err = self.lib.ss_session_create(ctypes.byref(self._tree), ctypes.byref(opts), ctypes.byref(sess))
+            if err != 0:
+                raise RuntimeError(f"ss_session_create failed ({err}): {last_error(self.lib)}")
+            self._session = sess
+            err = self.lib.ss_session_run(sess, int(iterations))
+            if err == 0:
+                err = self.lib.ss_session_output(sess, ctypes.byref(self._output))
+            if err != 0:
+                raise RuntimeError(f"session solve failed ({err}): {last_error(self.lib)}")
+            stats.iterations_run = int(iterations)
+            stats.exploitability_pct = -1.0
+            self._solved = True
+            self.stats = stats
+            return stats
         err = self.lib.ss_solve_gpu_ex(ctypes.byref(self._tree), int(iterations), ctypes.byref(opts),
                                        ctypes.byref(self._output), ctypes.byref(stats))
         if err != 0:
@@ -500,10 +537,44 @@ class StreetSolverGPU:
                 return i
         raise ValueError(f"Hand {hand_str} not in player {player_idx}'s range")
 
+    def narrow_weights(self, player, action_label, hand_cards, weights, node=None):
+        """The reference's between-street range update (python/hud_solver.py:
+        345-362 with python/range_narrowing.py:83-130) on the GPU from this
+        resident solve: P(action_label | hand) from `player`'s average strategy
+        at its first decision node (or `node`), applied to the entries
+        (hand_cards[i], weights[i]).  Returns (applied, new weights)."""
+        if getattr(self, "_session", None) is None:
+            raise RuntimeError("narrow_weights needs solve(..., resident=True)")
+        pi = self._resolve_player(player)
+        nidx = node
+        if nidx is None:
+            nidx = next((int(self._output.avg_strategy_node_ids[di]) for di in range(self._output.num_avg_nodes)
+                         if self._tree.nodes[self._output.avg_strategy_node_ids[di]].player == pi), -1)
+        if nidx < 0:
+            return False, list(weights)
+        labels = _build_labels_at_node(self._tree, nidx)
+        mask = sum(1 << a for a, lbl in enumerate(labels) if lbl == action_label)
+        if mask == 0:
+            return False, list(weights)
+        n = len(hand_cards)
+        cards = (ctypes.c_int * max(2 * n, 1))(*[c for hc in hand_cards for c in hc])
+        w = (ctypes.c_double * max(n, 1))(*weights)
+        applied = ctypes.c_int()
+        err = self.lib.ss_session_narrow(self._session, pi, nidx, mask, n, cards, w, ctypes.byref(applied))
+        if err != 0:
+            raise RuntimeError(f"ss_session_narrow failed ({err}): {last_error(self.lib)}")
+        return bool(applied.value), list(w)[:n]
+
+    def _drop_session(self):
+        if getattr(self, "_session", None) is not None:
+            self.lib.ss_session_destroy(self._session)
+            self._session = None
+
     def free(self):
         if getattr(self, "_freed", True):
             return
         self._freed = True
+        self._drop_session()
         if getattr(self, "_solved", False):
             self.lib.ss_free_output(ctypes.byref(self._output))
             self._solved = False

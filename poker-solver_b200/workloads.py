@@ -262,6 +262,15 @@ class Server:
             raise RuntimeError(f"ss_server_submit failed ({rc}): {ssg.last_error(self.lib)}")
         return rid.value
 
+    def progress(self, rid):
+        """(state, iterations run so far): state 0 queued, 1 in the batch, 2 done."""
+        st, it = ctypes.c_int(), ctypes.c_int()
+        self.lib.ss_server_progress.restype = ctypes.c_int
+        rc = self.lib.ss_server_progress(self.h, ctypes.c_longlong(rid), ctypes.byref(st), ctypes.byref(it))
+        if rc != 0:
+            raise RuntimeError(f"request {rid} failed ({rc}): {ssg.last_error(self.lib)}")
+        return st.value, it.value
+
     def wait(self, rid, num_hands):
         out, stats, lat = ssg.SSOutput(), ssg.SSSolveStats(), ctypes.c_double()
         rc = self.lib.ss_server_wait(self.h, ctypes.c_longlong(rid), ctypes.byref(out), ctypes.byref(stats),
@@ -311,6 +320,94 @@ def mix_config(rng, river=0.8, turn=0.15, river3=0.3):
                leaf_sigma=0.3 * pot, name=f"{street}{np_}")
     cfg["hands"], cfg["weights"] = make_ranges(rng, board, np_, None, zero_frac=float(rng.uniform(0, 0.7)))
     return cfg
+
+
+# ---------------------------------------------------------------------------
+# the batched benchmark's request mix: flop / turn / river, 2-6 players, tree
+# sizes log-uniform in [50, 20000] nodes, 0-70% of each range zeroed
+# ---------------------------------------------------------------------------
+
+SIZE_BETS = [[1.0], [0.75], [0.5], [0.5, 1.0], [0.33, 0.75], [0.33, 0.75, 1.5], [0.25, 0.5, 1.0, 2.0]]
+SIZE_RAISES = (1, 2, 3)
+# players per street: continuation leaves multiply a leaf by 4^N profiles, so
+# flops stay at 2-3 players and turns at 2-4; rivers take 2-6
+STREET_PLAYERS = {"flop": (2, 3), "turn": (2, 3, 4), "river": (2, 3, 4, 5, 6)}
+_SIZE_TABLE = {}
+
+
+def _tree_nodes(lib, nb, np_, bets, raises, pot=100, stack=400):
+    td = ssg.tree_struct(ssg.SS_MAX_HANDS_WIDE)()
+    b = (ctypes.c_int * nb)(*range(0, 4 * nb, 4))
+    s = (ctypes.c_float * len(bets))(*bets)
+    o = (ctypes.c_int * np_)(*range(np_))
+    rc = lib.ss_build_tree_ex(b, nb, pot, stack, s, len(bets), np_, o, int(nb == 5), int(nb < 5), raises,
+                              ctypes.byref(td))
+    if rc != 0:
+        raise RuntimeError(f"ss_build_tree_ex failed ({rc})")
+    n = td.num_nodes
+    lib.ss_free_tree(ctypes.byref(td))
+    return n
+
+
+def size_table(street, np_):
+    """[(nodes, bet_sizes, max_raises)] of every candidate shape (stack = 4 pots)."""
+    key = (street, np_)
+    if key not in _SIZE_TABLE:
+        lib = ssg.load_library(ssg.SS_MAX_HANDS_WIDE)
+        nb = {"flop": 3, "turn": 4, "river": 5}[street]
+        _SIZE_TABLE[key] = sorted((_tree_nodes(lib, nb, np_, b, r), b, r) for b in SIZE_BETS for r in SIZE_RAISES)
+    return _SIZE_TABLE[key]
+
+
+def range_size(np_, rng):
+    """Hands per player: every combo for 2-3 players; multiway ranges are
+    narrow (4 players 64-128 hands, 5 players 8, 6 players 6), which keeps the
+    terminals without a closed form (4-5 counted opponents) enumerable."""
+    if np_ <= 3:
+        return None
+    if np_ == 4:
+        return int(rng.integers(64, 129))
+    return 8 if np_ == 5 else 6
+
+
+def c4_config(rng, streets=(1 / 3, 1 / 3, 1 / 3), size=(50, 20000)):
+    """One seeded request of the batched mix.  A target size is drawn
+    log-uniform in `size`, then a street (weights flop, turn, river) and a
+    player count whose trees can come near the target; the bet set and raise
+    cap are the candidate shape nearest the target (log scale)."""
+    target = float(np.exp(rng.uniform(np.log(size[0]), np.log(size[1]))))
+    street = ["flop", "turn", "river"][int(rng.choice(3, p=np.asarray(streets) / np.sum(streets)))]
+    cands = []
+    for np_ in STREET_PLAYERS[street]:
+        tab = size_table(street, np_)
+        lo, hi = tab[0][0], tab[-1][0]
+        miss = 0.0 if lo <= target <= hi else min(abs(np.log(target / lo)), abs(np.log(target / hi)))
+        cands.append((miss, np_))
+    best = min(m for m, _ in cands)
+    players = [p for m, p in cands if m <= best + 1e-9]
+    np_ = int(players[int(rng.integers(len(players)))])
+    tab = size_table(street, np_)
+    nodes, sizes, raises = min(tab, key=lambda e: abs(np.log(e[0] / target)))
+    nb = {"flop": 3, "turn": 4, "river": 5}[street]
+    board = [int(c) for c in rng.permutation(52)[:nb]]
+    pot = int(rng.integers(50, 400))
+    cfg = dict(board=board, pot=pot, stack=4 * pot, bet_sizes=list(sizes), max_raises=int(raises),
+               num_players=np_, seed=int(rng.integers(1 << 30)), leaf_sigma=0.3 * pot,
+               name=f"{street}{np_}", target_nodes=target)
+    cfg["hands"], cfg["weights"] = make_ranges(rng, board, np_, range_size(np_, rng),
+                                               zero_frac=float(rng.uniform(0, 0.7)))
+    return cfg
+
+
+def c4_subgames(n, seed=0, streets=(1 / 3, 1 / 3, 1 / 3)):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        cfg = c4_config(rng, streets)
+        sg = AbiSubgame(cfg, max_hands=ssg.SS_MAX_HANDS_WIDE)
+        sg.set_leaf_values(leaf_values_for(cfg, sg.num_leaves))
+        out.append(sg)
+    return out
 
 
 def mix_subgames(n, seed=0):

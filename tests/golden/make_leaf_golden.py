@@ -25,7 +25,18 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "poker-solver_b200")]
 import workloads as wl  # noqa: E402
 from oracle.oracle import Oracle  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT", "/root/reference")
+def _ref_root():
+    """The reference checkout: argv[1], else the one place it is configured
+    (oracle/build_ref.py: REF_ROOT or its default location)."""
+    if len(sys.argv) > 1:
+        return sys.argv[1]
+    spec = importlib.util.spec_from_file_location("oracle_build_ref", os.path.join(ROOT, "oracle", "build_ref.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.REF
+
+
+REF = _ref_root()
 
 # name, seed, board cards, players, hands per player, bet sizes, raise cap
 CASES = [

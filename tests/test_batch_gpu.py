@@ -121,6 +121,43 @@ def test_server_alone_equals_mix():
 
 
 @pytest.mark.gpu
+def test_server_arrival_while_running_equals_alone():
+    """Continuous batching: the second request is submitted only once the
+    first has run at least one block on the GPU (and is still running), so
+    it joins a batch in flight; both results equal their solo results."""
+    subs = mixed_subgames()
+    first, second = subs[1], subs[6]
+    lib = first.lib
+    kw = dict(block_iterations=25, target_exploitability=0.05, max_iterations=400)
+    alone = []
+    for sg in (first, second):
+        srv = wl.Server(lib, **kw)
+        alone.append(srv.wait(srv.submit(sg), sg.nh))
+        srv.close()
+    assert alone[0]["stats"]["iterations_run"] >= 75   # the first runs several blocks alone
+    srv = wl.Server(lib, **kw)
+    a = srv.submit(first)
+    import time
+    t0 = time.time()
+    while True:
+        state, its = srv.progress(a)
+        if its >= 25:
+            break
+        assert time.time() - t0 < 60, "first request never ran a block"
+        time.sleep(0.001)
+    assert state == 1 and its < alone[0]["stats"]["iterations_run"]
+    b = srv.submit(second)
+    mixed = [srv.wait(a, first.nh), srv.wait(b, second.nh)]
+    srv.close()
+    for x, m in zip(alone, mixed):
+        identical(x, m)
+        assert x["stats"]["iterations_run"] == m["stats"]["iterations_run"]
+        assert x["stats"]["exploitability_pct"] == pytest.approx(m["stats"]["exploitability_pct"], rel=1e-9)
+    for sg in subs:
+        sg.free()
+
+
+@pytest.mark.gpu
 def test_server_memory_budget_queues_requests():
     # a tiny budget admits one request at a time; all still finish
     subs = mixed_subgames()[:3]
