@@ -376,6 +376,32 @@ SSB_CR3_HD void hand_mass_cls(int a, int b, const Tables &t, const int *p3, int 
     }
 }
 
+// The class masses of hand_mass_cls below a tie group (out[0]: third
+// opponent weaker, out[1]: tying), summed over the third opponent's entries
+// k = k0, k0 + kstep, ... only; entries stronger than the group are skipped
+// (no class of a pair uses them).  k_term_sd3 spreads a tie group's hands
+// and these slices over its warps; slices combined in a fixed order give the
+// same sums up to the order of the additions.
+SSB_CR3_HD void hand_mass_cls_slice(int a, int b, const Tables &t, const int *p3, int lo, int hi, long long k0,
+                                    long long kstep, double out[2], long long cnt[2], bool want_count) {
+    const HandPart hp = hand_part(a, b, t);
+    HandCount hc{};
+    if (want_count) hc = hand_count_part(a, b, t);
+    out[0] = out[1] = 0.0;
+    cnt[0] = cnt[1] = 0;
+    const long long n3 = t.isc[4];
+    for (long long k = k0; k < n3; k += kstep) {
+        if (p3[k] >= hi) continue;
+        const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
+        if (x == a || x == b || y == a || y == b) continue;
+        const int cls = p3[k] < lo ? 0 : 1;
+        if (want_count)
+            cnt[cls] += c2_at(hc, a, b, x, y, t);
+        else
+            out[cls] += t.r3[k] * d2_at(hp, a, b, x, y, t);
+    }
+}
+
 // The largest FP64 rounding of hand_mass on a tuple set that is empty: each
 // of its ~H3 terms is a few F_A F_B in size times r3 <= F3, so 1e-9 of
 // F_A F_B F3 bounds it with a wide margin; a hand whose mass is at or below

@@ -1963,7 +1963,11 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
 // the group's threads add the third opponent's hands by class.  A class
 // mass within rounding of 0 takes its exact tuple count (0: exactly 0).
 constexpr int kSd3Positions = 1081;   // C(47, 2): rank positions on every river board
-constexpr size_t sd3_smem(int HS) { return cr3_smem(HS) + static_cast<size_t>(HS) * sizeof(int) + 16; }
+constexpr int kSd3Warps = kTermThreads / 32;
+constexpr size_t sd3_smem(int HS) {
+    return cr3_smem(HS) + static_cast<size_t>(HS) * sizeof(int) + 16 + 3 * kTermThreads +
+           2 * kSd3Warps * (sizeof(double) + sizeof(long long)) + 64;
+}
 
 template <class T>
 __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const DevCtx *__restrict__ ctxs,
@@ -2010,6 +2014,14 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     t.r3 = cv.take<double>(HS);
     t.xy = cv.take<unsigned short>(HS);
     int *p3 = cv.take<int>(HS);
+    // per warp: the two class partials of one (hand, slice) of a tie group
+    double *part = cv.take<double>(2 * kSd3Warps);
+    long long *partc = cv.take<long long>(2 * kSd3Warps);
+    // the traverser hand at each of the block's rank positions
+    unsigned char *ga = cv.take<unsigned char>(kTermThreads);
+    unsigned char *gb = cv.take<unsigned char>(kTermThreads);
+    unsigned char *ghas = cv.take<unsigned char>(kTermThreads);
+    const int lane = tid & 31, warp = tid >> 5;
     const T *reach = reach_rows<T>(c);
     const int o1 = I.opp_player[0], o2 = I.opp_player[1], o3 = I.opp_player[2];
     cr3::Opp3<T> in;
@@ -2028,6 +2040,9 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     cr3::Sd3Thread st;
     cr3::sd3_thread_init(q0 + tid, qend, c.pos_hand + static_cast<size_t>(trav) * nc,
                          c.hand_code + static_cast<size_t>(trav) * hs, c.sd_combo, st);
+    ga[tid] = static_cast<unsigned char>(st.a);
+    gb[tid] = static_cast<unsigned char>(st.b);
+    ghas[tid] = st.h >= 0;
     constexpr int kAll = 1 << 30;
     auto build = [&](int lo1, int hi1, int lo2, int hi2) {
         cr3::phase_gather_cls(tid, kTermThreads, in, t, posA, lo1, hi1, posB, lo2, hi2);
@@ -2045,16 +2060,75 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     build(0, kAll, 0, kAll);
     cr3::sd3_thread_total(st, t, p3);
     __syncthreads();
-    for (int g = q0; g < qend;) {   // the tie groups meeting [q0, qend), the same walk in every thread
+    // The tie groups meeting [q0, qend), the same walk in every thread.  For
+    // each of a group's four pairs, its hands' class masses are sums over the
+    // third opponent's list: the group's hands and slices of that list are
+    // spread over the block's warps (per warps per hand, lanes splitting a
+    // slice), and each hand's owner thread combines its warps' partials in
+    // warp order.  A mass within rounding of 0 takes the exact tuple count
+    // (a second pass of the same shape over the 0/1 tables).
+    for (int g = q0; g < qend;) {
         const int lo = c.sd_combo[g].lo, hi = c.sd_combo[g].hi;
         const bool mine = st.h >= 0 && st.glo == lo;
         if (__syncthreads_or(mine)) {
+            const int j0 = max(lo, q0) - q0, ng = min(hi, qend) - q0 - j0;
+            const int per = ng >= kSd3Warps ? 1 : kSd3Warps / ng;   // warps per hand
+            const int hpr = kSd3Warps / per;                          // hands per round
+            const int r = warp / per, sl = warp - r * per;
+            const int jl = tid - j0;                                  // this thread's index in the group
+            auto walk = [&](int base, bool want_count) {
+                const int j = j0 + base + r;
+                double o[2] = {0.0, 0.0};
+                long long n[2] = {0, 0};
+                if (r < hpr && base + r < ng && ghas[j])
+                    cr3::hand_mass_cls_slice(ga[j], gb[j], t, p3, lo, hi, sl * 32 + lane, per * 32, o, n,
+                                             want_count);
+                for (int off = 16; off > 0; off >>= 1) {
+                    o[0] += __shfl_xor_sync(0xffffffffu, o[0], off);
+                    o[1] += __shfl_xor_sync(0xffffffffu, o[1], off);
+                    n[0] += __shfl_xor_sync(0xffffffffu, n[0], off);
+                    n[1] += __shfl_xor_sync(0xffffffffu, n[1], off);
+                }
+                if (lane == 0) {
+                    part[2 * warp] = o[0];
+                    part[2 * warp + 1] = o[1];
+                    partc[2 * warp] = n[0];
+                    partc[2 * warp + 1] = n[1];
+                }
+                __syncthreads();
+            };
             for (int pr = 0; pr < 4; ++pr) {
                 int lo1, hi1, lo2, hi2;
                 cr3::sd3_pair_bounds(pr, lo, hi, &lo1, &hi1, &lo2, &hi2);
                 build(lo1, hi1, lo2, hi2);
-                if (mine) cr3::sd3_thread_pair(st, t, p3, pr, lo, hi);
-                __syncthreads();
+                const double zb = cr3::zero_bound(t);
+                bool near_zero = false;
+                for (int base = 0; base < ng; base += hpr) {
+                    walk(base, false);
+                    if (mine && jl >= base && jl < base + hpr) {
+                        double m0 = 0.0, m1 = 0.0;
+                        for (int k = 0; k < per; ++k) {
+                            m0 += part[2 * ((jl - base) * per + k)];
+                            m1 += part[2 * ((jl - base) * per + k) + 1];
+                        }
+                        st.m[pr][0] = m0;
+                        st.m[pr][1] = m1;
+                        near_zero = fabs(m0) <= zb || fabs(m1) <= zb;
+                    }
+                    __syncthreads();
+                }
+                if (__syncthreads_or(near_zero)) {
+                    for (int base = 0; base < ng; base += hpr) {
+                        walk(base, true);
+                        if (mine && jl >= base && jl < base + hpr)
+                            for (int cls = 0; cls < 2; ++cls) {
+                                long long n = 0;
+                                for (int k = 0; k < per; ++k) n += partc[2 * ((jl - base) * per + k) + cls];
+                                if (fabs(st.m[pr][cls]) <= zb && n == 0) st.m[pr][cls] = 0.0;
+                            }
+                        __syncthreads();
+                    }
+                }
             }
         }
         g = hi;

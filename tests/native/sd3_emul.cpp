@@ -148,6 +148,26 @@ int main(int argc, char **argv) {
             double o[3];
             long long c[3];
             hand_mass_cls(a, b, t, p3.data(), v, v + 1, o, c, true);
+            // the kernel's split of the same sums: per warps of 32 lanes, each
+            // lane every (per * 32)-th entry of the third opponent's list
+            for (int per = 1; per <= 8; per *= 2) {
+                double so[2] = {0.0, 0.0};
+                long long sc[2] = {0, 0};
+                for (int k0 = 0; k0 < per * 32; ++k0) {
+                    double po[2], unused_o[2];
+                    long long pc[2], unused_c[2];
+                    hand_mass_cls_slice(a, b, t, p3.data(), v, v + 1, k0, per * 32, po, unused_c, false);
+                    hand_mass_cls_slice(a, b, t, p3.data(), v, v + 1, k0, per * 32, unused_o, pc, true);
+                    for (int cl = 0; cl < 2; ++cl) {
+                        so[cl] += po[cl];
+                        sc[cl] += pc[cl];
+                    }
+                }
+                for (int cl = 0; cl < 2; ++cl) {
+                    if (sc[cl] != c[cl]) ++zero_bad;
+                    max_rel = std::max(max_rel, std::fabs(so[cl] - o[cl]) / (1.0 + std::fabs(o[cl])));
+                }
+            }
             const double zb = zero_bound(t);
             for (int cl = 0; cl < 2; ++cl) {
                 m[pr][cl] = (std::fabs(o[cl]) <= zb && c[cl] == 0) ? 0.0 : o[cl];
