@@ -15,6 +15,9 @@ reference's build system:
   libref_street_solve_gpu.so  src/cuda/street_solve.cu unmodified, nvcc sm_100a
                               (stock limits: 200 hands, 3 raises); for parity runs
                               on a B200 at <= 200 hands.
+  libref_flop_solve_gpu.so    src/cuda/flop_solve.cu unmodified, nvcc sm_100a: its
+                              tree builder (host code) pins fs_build_tree here,
+                              its solve pins fs_solve_gpu on a B200.
   wrapper/python/             python/street_solver_gpu.py and python/solver.py,
                               copied unmodified: the reference's own ctypes
                               consumer of the C ABI, which the drop-in test runs
@@ -111,6 +114,18 @@ def build_gpu():
     return out
 
 
+def build_flop_gpu():
+    out = os.path.join(OUT, "libref_flop_solve_gpu.so")
+    cu = os.path.join(REF, "src", "cuda", "flop_solve.cu")
+    if _fresh(out, [cu]):
+        return out
+    if shutil.which("nvcc") is None:
+        return None
+    _run(["nvcc", "-O2", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+          "-Xcompiler", "-fPIC", "-w", cu, "-o", out])
+    return out
+
+
 def build_wrapper():
     """The reference's Python consumer of the C ABI, unmodified (it imports
     card helpers from solver.py and loads <root>/build/street_solve.so)."""
@@ -133,6 +148,7 @@ def main():
     for h, r in VARIANTS:
         built.append(build_shim(h, r))
     built.append(build_gpu())
+    built.append(build_flop_gpu())
     built.append(build_wrapper())
     for b in built:
         if b:

@@ -3,7 +3,7 @@
   poker-solver_b200/lib/libstreet_solve.so       SS_MAX_HANDS = 200  (reference struct layout)
   poker-solver_b200/lib/libstreet_solve_wide.so  SS_MAX_HANDS = 1326 (every 2-card combo)
 
-Both export the C ABI of include/street_solve.h.  The engine objects are
+Both export the C ABIs of include/street_solve.h and include/flop_solve.h.  The engine objects are
 compiled once and linked into both; only the ABI translation unit differs.
 The CUDA runtime is linked statically, so each library is self-contained.
 """
@@ -21,8 +21,8 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
 ENGINE = ["ss_tree.cpp", "ss_plan.cpp", "ss_kernels.cu", "ss_engine.cu", "ss_rank_kernels.cu", "ss_noalloc.cu", "ss_batch.cu",
-          "ss_leaf_plan.cpp", "ss_leaf.cu", "ss_narrow.cu"]
-HEADERS = ["ss_engine.h", "ss_kernels.h", "ss_rank.cuh", "ss_session.h", "ss_leaf.h", "ss_leaf.cuh"]
+          "ss_leaf_plan.cpp", "ss_leaf.cu", "ss_narrow.cu", "fs_tree.cpp", "fs_engine.cu", "fs_abi.cpp"]
+HEADERS = ["ss_engine.h", "ss_kernels.h", "ss_rank.cuh", "ss_session.h", "ss_leaf.h", "ss_leaf.cuh", "fs_engine.h"]
 VARIANTS = {"libstreet_solve.so": 200, "libstreet_solve_wide.so": 1326}
 
 
@@ -43,7 +43,8 @@ def _nvcc(args, verbose):
 def build(verbose=False, force=False, ptxas_info=False):
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "street_solve.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, h) for h in ("street_solve.h",
+                                                                                          "flop_solve.h")]
     objs = []
     for src in ENGINE:
         s = os.path.join(CSRC, src)

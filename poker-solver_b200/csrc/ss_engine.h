@@ -93,7 +93,8 @@ struct alignas(16) CfvItem {
     int frozen;
     int node;
     int sg = 0;               // subgame of a batch (0 for a single subgame)
-    int pad_[3] = {0, 0, 0};
+    float scale = 1.f;        // the node's value row is stored times this (chance weights; 1 on one street)
+    int pad_[2] = {0, 0};
 };
 
 // A value/regret item whose edges' frontiers hold at least this many rows in

@@ -300,7 +300,9 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
             st2(V.S + off, ns);
         }
     }
-    st2(V.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0, v1));
+    // scale 1 on a single street (exact: the row equals v); below chance
+    // nodes the row carries their 1 / cards weights for the parent's frontier
+    st2(V.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0 * I.scale, v1 * I.scale));
 }
 
 // --------------------------------------------------------------------------
