@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS),
                     help="subgame of the plain form (the CPU baseline and reference arm cover turn3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf,four,anchor",
+    ap.add_argument("--forms", default="plain,batched,served,hu_river,leaf,four,anchor,flop",
                     help="comma list of plain (the headline), batched, served, hu_river (the heads-up river "
                          "beside the reference's CPU solver), leaf (the turn subgame's continuation values "
                          "produced on the GPU), four (full-range 4-player turn and river, three-opponent "
@@ -855,6 +855,43 @@ def reference_cpu(seed, budget_s=25.0):
             "solves_per_s": 1.0 / (s_iter_full * 1000)}
 
 
+FLOP = {"flop": [0, 13, 26], "pot": 1000, "stack": 5000, "bet_sizes": [0.75], "hands": 200, "iterations": 100}
+
+
+def run_flop(seed, device, solves=3):
+    """The multi-street (flop through river) solver against the reference's
+    own sm_100a build of src/cuda/flop_solve.cu on the same tree, ranges and
+    iterations, both through fs_solve_gpu from host buffers on this GPU:
+    median wall time per solve."""
+    import flop_solve as fsm
+    import street_solver_gpu as ssg
+    import workloads as wl
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libref_flop_solve_gpu.so")
+    rng = np.random.default_rng(seed + 11)
+    h, w = wl.make_ranges(rng, FLOP["flop"], 2, FLOP["hands"])
+    out = {"workload": f"flop-through-river 2 players, flop {FLOP['flop']}, pot {FLOP['pot']}, stack {FLOP['stack']}, "
+                       f"flop bets {FLOP['bet_sizes']} (turn / river 0.75), {FLOP['hands']} hands each, "
+                       f"{FLOP['iterations']} Linear-CFR iterations"}
+    libs = [("ours", ssg.load_library(200))]
+    if os.path.exists(ref_path):
+        libs.append(("reference_gpu", ctypes.CDLL(ref_path)))
+    for name, lib in libs:
+        sg = fsm.FlopSubgame(lib, FLOP["flop"], FLOP["pot"], FLOP["stack"], FLOP["bet_sizes"], h, w)
+        out["tree_nodes"] = sg.td.num_nodes
+        times = []
+        with _Quiet():
+            for _ in range(solves + 1):
+                t0 = time.perf_counter()
+                sg.solve(FLOP["iterations"])
+                times.append(time.perf_counter() - t0)
+        sg.free()
+        times = sorted(times[1:])
+        out[name + "_s_per_solve"] = times[len(times) // 2]
+    if "reference_gpu_s_per_solve" in out:
+        out["speedup_vs_reference_gpu"] = out["reference_gpu_s_per_solve"] / out["ours_s_per_solve"]
+    return out
+
+
 ANCHOR = {"hands": 10, "iterations": 20}
 
 
@@ -982,6 +1019,12 @@ def main():
             four = run_four_player(args.seed, local)
         except Exception as e:  # the solver's line is printed whatever happens here
             four = {"error": f"{type(e).__name__}: {e}"}
+    flop = None
+    if rank == 0 and world == 1 and "flop" in forms:
+        try:
+            flop = run_flop(args.seed, local)
+        except Exception as e:  # the solver's line is printed whatever happens here
+            flop = {"error": f"{type(e).__name__}: {e}"}
     anchor = None
     if rank == 0 and world == 1 and "anchor" in forms and args.workload == "turn3":
         try:
@@ -1016,7 +1059,7 @@ def main():
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
             "batched": batched, "served": served, "hu_river": hu, "leaf_producer": leaf, "four_player": four,
-            "anchor_same_config": anchor,
+            "anchor_same_config": anchor, "flop_solver": flop,
             "hu_river_vs_reference_cpu": None if not hu or "error" in hu else {
                 "gpu_solves_per_s": hu.get("gpu_solves_per_s"),
                 "reference_cpu_solves_per_s": (hu.get("cpu_baseline") or {}).get("solves_per_s")},

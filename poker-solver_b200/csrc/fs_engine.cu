@@ -278,11 +278,101 @@ int build_plan(const FSTreeData &td, FsPlan *out) {
             for (int b = 0; b < n.num_board; ++b) it.board[b] = n.board_cards[b];
             P.term[t].push_back(it);
         }
+        // folds first, then showdowns (one launch each)
+        std::stable_partition(P.term[t].begin(), P.term[t].end(), [](const FsTermItem &i) { return i.kind == 0; });
+        P.nfold[t] = static_cast<int>(std::count_if(P.term[t].begin(), P.term[t].end(),
+                                                    [](const FsTermItem &i) { return i.kind == 0; }));
     }
-    // hands
-    P.hand_cards.assign(2 * static_cast<size_t>(P.HS), -1);
+    // hands, and per player the hands holding each card (folds)
+    const int HSi = P.HS;
+    P.hand_cards.assign(2 * static_cast<size_t>(HSi), -1);
     for (int p = 0; p < 2; ++p)
-        for (int h = 0; h < P.H[p]; ++h) P.hand_cards[p * P.HS + h] = td.hands[p][h][0] | (td.hands[p][h][1] << 8);
+        for (int h = 0; h < P.H[p]; ++h) P.hand_cards[p * HSi + h] = td.hands[p][h][0] | (td.hands[p][h][1] << 8);
+    P.f_coff.assign(2 * 53, 0);
+    P.f_clist.assign(2 * 2 * static_cast<size_t>(HSi), 0);
+    for (int p = 0; p < 2; ++p) {
+        std::vector<std::vector<int>> byc(52);
+        for (int h = 0; h < P.H[p]; ++h) {
+            byc[td.hands[p][h][0]].push_back(h);
+            byc[td.hands[p][h][1]].push_back(h);
+        }
+        int at = 0;
+        for (int c = 0; c < 52; ++c) {
+            P.f_coff[p * 53 + c] = at;
+            for (int h : byc[c]) P.f_clist[p * 2 * HSi + at++] = h;
+        }
+        P.f_coff[p * 53 + 52] = at;
+    }
+    // showdown tables per river board (see fs_engine.h)
+    const int nsb = static_cast<int>(P.sboards.size() / 5);
+    P.sd_str.assign(static_cast<size_t>(nsb) * 2 * HSi, 0u);
+    P.sd_ord.assign(static_cast<size_t>(nsb) * 2 * HSi, -1);
+    P.sd_hpos.assign(static_cast<size_t>(nsb) * 2 * HSi * 4, 0);
+    P.sd_coff.assign(static_cast<size_t>(nsb) * 2 * 53, 0);
+    P.sd_clist.assign(static_cast<size_t>(nsb) * 2 * 2 * HSi, 0);
+    for (int bi = 0; bi < nsb; ++bi) {
+        const int *bd = &P.sboards[5 * bi];
+        std::vector<unsigned> srt[2];
+        for (int p = 0; p < 2; ++p) {
+            unsigned *str = &P.sd_str[(static_cast<size_t>(bi) * 2 + p) * HSi];
+            for (int h = 0; h < P.H[p]; ++h) str[h] = rank7_host(bd, td.hands[p][h][0], td.hands[p][h][1]);
+            int *ord = &P.sd_ord[(static_cast<size_t>(bi) * 2 + p) * HSi];
+            std::vector<int> idx(P.H[p]);
+            for (int h = 0; h < P.H[p]; ++h) idx[h] = h;
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return str[x] < str[y]; });
+            std::vector<int> pos(P.H[p]);
+            for (int k = 0; k < P.H[p]; ++k) {
+                ord[k] = idx[k];
+                pos[idx[k]] = k;
+                srt[p].push_back(str[idx[k]]);
+            }
+            // card lists of this player as the opponent, by position
+            std::vector<std::vector<int>> byc(52);
+            for (int k = 0; k < P.H[p]; ++k) {
+                byc[td.hands[p][idx[k]][0]].push_back(k);
+                byc[td.hands[p][idx[k]][1]].push_back(k);
+            }
+            int *coff = &P.sd_coff[(static_cast<size_t>(bi) * 2 + p) * 53];
+            int *cl = &P.sd_clist[(static_cast<size_t>(bi) * 2 + p) * 2 * HSi];
+            int at = 0;
+            for (int c = 0; c < 52; ++c) {
+                coff[c] = at;
+                for (int k : byc[c]) cl[at++] = k;
+            }
+            coff[52] = at;
+        }
+        for (int t = 0; t < 2; ++t) {
+            const int o = 1 - t;
+            const unsigned *st = &P.sd_str[(static_cast<size_t>(bi) * 2 + t) * HSi];
+            const unsigned *so = &P.sd_str[(static_cast<size_t>(bi) * 2 + o) * HSi];
+            const int *coff = &P.sd_coff[(static_cast<size_t>(bi) * 2 + o) * 53];
+            const int *cl = &P.sd_clist[(static_cast<size_t>(bi) * 2 + o) * 2 * HSi];
+            const int *ordo = &P.sd_ord[(static_cast<size_t>(bi) * 2 + o) * HSi];
+            for (int h = 0; h < P.H[t]; ++h) {
+                const unsigned s = st[h];
+                const int lo = static_cast<int>(std::lower_bound(srt[o].begin(), srt[o].end(), s) - srt[o].begin());
+                const int hi = static_cast<int>(std::upper_bound(srt[o].begin(), srt[o].end(), s) - srt[o].begin());
+                const int c1 = td.hands[t][h][0], c2 = td.hands[t][h][1];
+                int cnt[2][2];
+                const int cs[2] = {c1, c2};
+                for (int j = 0; j < 2; ++j) {
+                    int below = 0, upto = 0;
+                    for (int k = coff[cs[j]]; k < coff[cs[j] + 1]; ++k) {
+                        const unsigned x = so[ordo[cl[k]]];
+                        below += x < s;
+                        upto += x <= s;
+                    }
+                    cnt[j][0] = below;
+                    cnt[j][1] = upto;
+                }
+                int *hp = &P.sd_hpos[((static_cast<size_t>(bi) * 2 + t) * HSi + h) * 4];
+                hp[0] = lo | (hi << 16);
+                hp[1] = c1 | (c2 << 8);
+                hp[2] = cnt[0][0] | (cnt[0][1] << 16);
+                hp[3] = cnt[1][0] | (cnt[1][1] << 16);
+            }
+        }
+    }
     // read-out levels: BFS depth, deepest first
     int maxd = 0;
     for (int x = 0; x < N; ++x) maxd = std::max(maxd, depth[x]);
@@ -304,82 +394,202 @@ namespace {
 
 constexpr int kFsThreads = 256;
 
-// strengths [nsb][2][HS] of both players' hands on every showdown board
-// (0: the board blocks the hand)
-__global__ void k_fs_strengths(const int *__restrict__ sboards, int nsb, const int *__restrict__ hand_cards, int HS,
-                               int H0, int H1, unsigned *__restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nsb * 2 * HS) return;
-    const int b = i / (2 * HS), r = i - b * 2 * HS, p = r / HS, h = r - p * HS;
-    unsigned s = 0;
-    if (h < (p == 0 ? H0 : H1)) {
-        const int code = hand_cards[p * HS + h];
-        int c[7] = {sboards[5 * b], sboards[5 * b + 1], sboards[5 * b + 2], sboards[5 * b + 3], sboards[5 * b + 4],
-                    code & 0xff, (code >> 8) & 0xff};
-        bool clash = false;
-        for (int k = 0; k < 5; ++k) clash |= c[k] == c[5] || c[k] == c[6];
-        s = clash ? 0u : rank7(c);
-    }
-    out[i] = s;
-}
+// Folds (flop_solve.cu:731-779): payoff x the opponent's reach over hands
+// sharing no card with the traverser's hand {a, b} or with the node's board.
+// One block per terminal: the opponent's hands the board leaves are staged
+// (reach in FP64, and whether it is positive); per card c their sums u(c),
+// and F in all; then per traverser hand
+//   mass = F - u(a) - u(b) + (the opponent's reach on the combo {a, b}),
+// the last term from the opponent's list of card a.  The same sums over 0/1
+// count the opponent hands with positive reach; none gives exactly 0, as the
+// reference's sum of zeros does.
+struct FsTables {
+    const int *hand_cards;                    // [2][HS]
+    const int *f_coff, *f_clist;              // [2][53], [2][2 HS]
+    const unsigned *sd_str;                   // [nsb][2][HS]
+    const int *sd_ord, *sd_hpos, *sd_coff, *sd_clist;
+    int HS, H0, H1;
+};
 
-// one block per terminal (flop_solve.cu:731-833 semantics): the opponent's
-// reach row, cards and strengths staged in shared memory, one traverser hand
-// per thread, opponent hands summed in hand order
-__global__ void __launch_bounds__(kFsThreads) k_fs_term(const FsTermItem *__restrict__ items, int trav,
-                                                       const float *__restrict__ reach,
-                                                       const int *__restrict__ hand_cards,
-                                                       const unsigned *__restrict__ str, int HS, int H0, int H1,
+__global__ void __launch_bounds__(kFsThreads) k_fs_fold(const FsTermItem *__restrict__ items, int trav,
+                                                       const float *__restrict__ reach, FsTables T,
                                                        float *__restrict__ out, int scaled) {
-    __shared__ float r_o[FS_MAX_HANDS];
-    __shared__ int c_o[FS_MAX_HANDS];
-    __shared__ unsigned s_o[FS_MAX_HANDS];
+    __shared__ double r_o[FS_MAX_HANDS];
+    __shared__ double u[52];
+    __shared__ int cu[52];
+    __shared__ double tot[kFsThreads / 32];
+    __shared__ int ctot[kFsThreads / 32];
     const FsTermItem I = items[blockIdx.x];
     const int opp = 1 - trav;
-    const int Ho = opp == 0 ? H0 : H1, Ht = trav == 0 ? H0 : H1;
-    const size_t hs = static_cast<size_t>(HS);
-    for (int o = threadIdx.x; o < Ho; o += blockDim.x) {
-        const int code = hand_cards[opp * HS + o];
-        const int a = code & 0xff, b = (code >> 8) & 0xff;
-        r_o[o] = reach[static_cast<size_t>(I.opp_row) * hs + o];
+    const int Ho = opp == 0 ? T.H0 : T.H1, Ht = trav == 0 ? T.H0 : T.H1;
+    const size_t hs = static_cast<size_t>(T.HS);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double f = 0.0;
+    int cf = 0;
+    for (int o = tid; o < Ho; o += blockDim.x) {
+        const int code = T.hand_cards[opp * T.HS + o];
+        const int x = code & 0xff, y = (code >> 8) & 0xff;
         bool blocked = false;
-        if (I.kind == 0)
-            for (int k = 0; k < I.nb; ++k) blocked |= a == I.board[k] || b == I.board[k];
-        c_o[o] = blocked ? -1 : code;   // a fold skips opponent hands the node's board blocks
-        s_o[o] = I.kind == 1 ? str[(static_cast<size_t>(I.sboard) * 2 + opp) * hs + o] : 0u;
+        for (int k = 0; k < I.nb; ++k) blocked |= x == I.board[k] || y == I.board[k];
+        const double r = blocked ? 0.0 : static_cast<double>(reach[static_cast<size_t>(I.opp_row) * hs + o]);
+        r_o[o] = blocked ? -1.0 : r;   // -1: the board blocks the hand
+        f += r;
+        cf += (!blocked && r > 0.0) ? 1 : 0;
+    }
+    for (int k = 16; k > 0; k >>= 1) {
+        f += __shfl_xor_sync(0xffffffffu, f, k);
+        cf += __shfl_xor_sync(0xffffffffu, cf, k);
+    }
+    if (lane == 0) {
+        tot[warp] = f;
+        ctot[warp] = cf;
+    }
+    __syncthreads();
+    if (tid < 52) {
+        double s = 0.0;
+        int n = 0;
+        const int *cl = T.f_clist + opp * 2 * T.HS;
+        for (int k = T.f_coff[opp * 53 + tid]; k < T.f_coff[opp * 53 + tid + 1]; ++k) {
+            const double r = r_o[cl[k]];
+            if (r >= 0.0) {
+                s += r;
+                n += r > 0.0 ? 1 : 0;
+            }
+        }
+        u[tid] = s;
+        cu[tid] = n;
+    }
+    __syncthreads();
+    double F = 0.0;
+    int CF = 0;
+    for (int w = 0; w < kFsThreads / 32; ++w) {
+        F += tot[w];
+        CF += ctot[w];
+    }
+    const float sc = scaled ? I.scale : 1.0f;
+    const int *cl = T.f_clist + opp * 2 * T.HS;
+    for (int h = tid; h < Ht; h += blockDim.x) {
+        const int code = T.hand_cards[trav * T.HS + h];
+        const int a = code & 0xff, b = (code >> 8) & 0xff;
+        double same = 0.0;
+        int csame = 0;
+        for (int k = T.f_coff[opp * 53 + a]; k < T.f_coff[opp * 53 + a + 1]; ++k) {
+            const int o = cl[k];
+            const int oc = T.hand_cards[opp * T.HS + o];
+            if ((oc & 0xff) != b && ((oc >> 8) & 0xff) != b) continue;
+            const double r = r_o[o];
+            if (r >= 0.0) {
+                same += r;
+                csame += r > 0.0 ? 1 : 0;
+            }
+        }
+        const int cnt = CF - cu[a] - cu[b] + csame;
+        const double mass = cnt == 0 ? 0.0 : F - u[a] - u[b] + same;
+        out[static_cast<size_t>(I.node) * hs + h] = static_cast<float>(mass) * I.payoff * sc;
+    }
+}
+
+// Showdowns (flop_solve.cu:781-833): +-half_pot per opponent hand that is
+// weaker / stronger, ties 0, hands the board blocks 0.  With the opponent's
+// hands in ascending strength on this river board, W = the reach below the
+// traverser hand's strength and L = above it, each less the opponent hands
+// holding one of its two cards (their own prefix sums along each card's
+// list); value = (W - L) x half_pot, FP64 sums.  The same on 0/1 counts
+// gives exactly 0 where no positive-reach opponent hand wins or loses.
+__global__ void __launch_bounds__(kFsThreads) k_fs_showdown(const FsTermItem *__restrict__ items, int trav,
+                                                           const float *__restrict__ reach, FsTables T,
+                                                           float *__restrict__ out, int scaled) {
+    __shared__ double P[FS_MAX_HANDS + 1];
+    __shared__ int Pc[FS_MAX_HANDS + 1];
+    __shared__ double PC[2 * FS_MAX_HANDS + 52];
+    __shared__ int PCc[2 * FS_MAX_HANDS + 52];
+    __shared__ double x_s[FS_MAX_HANDS];
+    const FsTermItem I = items[blockIdx.x];
+    const int opp = 1 - trav;
+    const int Ho = opp == 0 ? T.H0 : T.H1, Ht = trav == 0 ? T.H0 : T.H1;
+    const size_t hs = static_cast<size_t>(T.HS);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const size_t bo = static_cast<size_t>(I.sboard) * 2 + opp, bt = static_cast<size_t>(I.sboard) * 2 + trav;
+    const int *ord = T.sd_ord + bo * hs;
+    const unsigned *so = T.sd_str + bo * hs;
+    // the opponent's reach by position (0 where the board blocks the hand)
+    for (int k = tid; k < Ho; k += blockDim.x) {
+        const int o = ord[k];
+        x_s[k] = so[o] == 0u ? 0.0 : static_cast<double>(reach[static_cast<size_t>(I.opp_row) * hs + o]);
+    }
+    __syncthreads();
+    if (tid < 32) {
+        // prefix sums over positions: each lane a run of consecutive
+        // positions, lane totals scanned across the warp (fixed order)
+        constexpr int kRun = (FS_MAX_HANDS + 31) / 32;
+        const int k0 = lane * kRun;
+        double s = 0.0;
+        int n = 0;
+        for (int i = 0; i < kRun; ++i)
+            if (k0 + i < Ho) {
+                s += x_s[k0 + i];
+                n += x_s[k0 + i] > 0.0 ? 1 : 0;
+            }
+        double incl = s;
+        int nincl = n;
+        for (int d = 1; d < 32; d <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, incl, d);
+            const int m = __shfl_up_sync(0xffffffffu, nincl, d);
+            if (lane >= d) {
+                incl += v;
+                nincl += m;
+            }
+        }
+        double run = incl - s;
+        int nrun = nincl - n;
+        for (int i = 0; i < kRun; ++i)
+            if (k0 + i < Ho) {
+                P[k0 + i] = run;
+                Pc[k0 + i] = nrun;
+                run += x_s[k0 + i];
+                nrun += x_s[k0 + i] > 0.0 ? 1 : 0;
+            }
+        if (lane == 31) {
+            P[Ho] = incl;
+            Pc[Ho] = nincl;
+        }
+    } else if (tid >= 64 && tid < 64 + 52) {
+        // per card: prefix sums along the opponent's hands holding it
+        const int c = tid - 64;
+        const int *coff = T.sd_coff + bo * 53;
+        const int *cl = T.sd_clist + bo * 2 * hs;
+        const int base = coff[c] + c;
+        double s = 0.0;
+        int n = 0;
+        PC[base] = 0.0;
+        PCc[base] = 0;
+        for (int k = coff[c]; k < coff[c + 1]; ++k) {
+            const double v = x_s[cl[k]];
+            s += v;
+            n += v > 0.0 ? 1 : 0;
+            PC[base + (k - coff[c]) + 1] = s;
+            PCc[base + (k - coff[c]) + 1] = n;
+        }
     }
     __syncthreads();
     const float sc = scaled ? I.scale : 1.0f;
-    for (int h = threadIdx.x; h < Ht; h += blockDim.x) {
-        const int code = hand_cards[trav * HS + h];
-        const int a = code & 0xff, b = (code >> 8) & 0xff;
+    const unsigned *st = T.sd_str + bt * hs;
+    const int *coff = T.sd_coff + bo * 53;
+    for (int h = tid; h < Ht; h += blockDim.x) {
         float v = 0.f;
-        if (I.kind == 0) {
-            float s = 0.f;
-            for (int o = 0; o < Ho; ++o) {
-                const int oc = c_o[o];
-                if (oc < 0) continue;
-                const int x = oc & 0xff, y = (oc >> 8) & 0xff;
-                if (a == x || a == y || b == x || b == y) continue;
-                s += r_o[o];
-            }
-            v = s * I.payoff;
-        } else {
-            const unsigned hsv = str[(static_cast<size_t>(I.sboard) * 2 + trav) * hs + h];
-            if (hsv != 0u) {
-                for (int o = 0; o < Ho; ++o) {
-                    const int oc = c_o[o];
-                    const int x = oc & 0xff, y = (oc >> 8) & 0xff;
-                    if (a == x || a == y || b == x || b == y) continue;
-                    const unsigned os = s_o[o];
-                    if (os == 0u) continue;
-                    const float wgt = r_o[o];
-                    if (hsv > os)
-                        v += wgt * I.half_pot;
-                    else if (hsv < os)
-                        v -= wgt * I.half_pot;
-                }
-            }
+        if (st[h] != 0u) {
+            const int4 hp = reinterpret_cast<const int4 *>(T.sd_hpos)[bt * hs + h];
+            const int lo = hp.x & 0xffff, hi = hp.x >> 16;
+            const int c1 = hp.y & 0xff, c2 = (hp.y >> 8) & 0xff;
+            const int b1 = coff[c1] + c1, n1 = coff[c1 + 1] - coff[c1];
+            const int b2 = coff[c2] + c2, n2 = coff[c2 + 1] - coff[c2];
+            const int l1lo = hp.z & 0xffff, l1hi = hp.z >> 16, l2lo = hp.w & 0xffff, l2hi = hp.w >> 16;
+            const double W = P[lo] - PC[b1 + l1lo] - PC[b2 + l2lo];
+            const double L = (P[Ho] - P[hi]) - (PC[b1 + n1] - PC[b1 + l1hi]) - (PC[b2 + n2] - PC[b2 + l2hi]);
+            const int cw = Pc[lo] - PCc[b1 + l1lo] - PCc[b2 + l2lo];
+            const int closs = (Pc[Ho] - Pc[hi]) - (PCc[b1 + n1] - PCc[b1 + l1hi]) - (PCc[b2 + n2] - PCc[b2 + l2hi]);
+            const double w = cw == 0 ? 0.0 : W, l = closs == 0 ? 0.0 : L;
+            v = static_cast<float>((w - l) * static_cast<double>(I.half_pot));
         }
         out[static_cast<size_t>(I.node) * hs + h] = v * sc;
     }
@@ -404,7 +614,7 @@ __global__ void k_fs_sigma(const float *__restrict__ R, const int *__restrict__ 
 }
 
 // one level of the read-out: every node's value for traverser t from its
-// children (terminals were written by k_fs_term): the traverser's decisions
+// children (terminals were written by k_fs_fold / k_fs_showdown): the traverser's decisions
 // weight by its last-pass strategy, the opponent's sum, chance nodes average
 // (flop_solve.cu:835-892 order: children in order, then the division)
 __global__ void k_fs_value_level(const FSNode *__restrict__ nodes, const int *__restrict__ children,
@@ -459,7 +669,6 @@ class Solve {
     cudaStream_t stream = nullptr;
     char *dbase = nullptr;
     float *dstate = nullptr;
-    unsigned *dstr = nullptr;
     int *diter = nullptr;
     float *dsnap = nullptr;
     float *dsig = nullptr, *dval = nullptr;   // read-out
@@ -469,6 +678,7 @@ class Solve {
     const CfvItem *cfv_items[2] = {};
     const FsTermItem *term_items[2] = {};
     const int *hand_cards = nullptr, *edge_first = nullptr, *edge_na = nullptr, *depth_nodes = nullptr;
+    FsTables tab{};
     FSNode *dnodes = nullptr;
     int *dchildren = nullptr;
     const int *dfirst_edge = nullptr;
@@ -478,7 +688,7 @@ class Solve {
     ~Solve() {
         if (gblock) cudaGraphExecDestroy(gblock);
         if (stream) {
-            for (void *p : {static_cast<void *>(dbase), static_cast<void *>(dstate), static_cast<void *>(dstr),
+            for (void *p : {static_cast<void *>(dbase), static_cast<void *>(dstate),
                             static_cast<void *>(diter), static_cast<void *>(dsnap), static_cast<void *>(dsig),
                             static_cast<void *>(dval), static_cast<void *>(dnodes), static_cast<void *>(dchildren)})
                 if (p) cudaFreeAsync(p, stream);
@@ -521,8 +731,10 @@ class Solve {
             ena[e] = td.nodes[P.edge_node[e]].num_children;
         }
         const size_t o_fro = b.add(P.fr_off), o_fri = b.add(P.fr_items), o_hc = b.add(P.hand_cards),
-                     o_sb = b.add(P.sboards), o_ef = b.add(ef), o_ena = b.add(ena), o_dn = b.add(P.depth_nodes),
-                     o_fe = b.add(P.first_edge);
+                     o_ef = b.add(ef), o_ena = b.add(ena), o_dn = b.add(P.depth_nodes), o_fe = b.add(P.first_edge),
+                     o_fco = b.add(P.f_coff), o_fcl = b.add(P.f_clist), o_sst = b.add(P.sd_str),
+                     o_sor = b.add(P.sd_ord), o_shp = b.add(P.sd_hpos), o_sco = b.add(P.sd_coff),
+                     o_scl = b.add(P.sd_clist);
         FCK(cudaMallocAsync(reinterpret_cast<void **>(&dbase), std::max<size_t>(b.host.size(), 256), stream));
         FCK(cudaMemcpyAsync(dbase, b.host.data(), b.host.size(), cudaMemcpyHostToDevice, stream));
         for (int p = 0; p < 2; ++p) {
@@ -531,6 +743,17 @@ class Solve {
             term_items[p] = reinterpret_cast<const FsTermItem *>(dbase + o_term[p]);
         }
         hand_cards = reinterpret_cast<const int *>(dbase + o_hc);
+        tab.hand_cards = hand_cards;
+        tab.f_coff = reinterpret_cast<const int *>(dbase + o_fco);
+        tab.f_clist = reinterpret_cast<const int *>(dbase + o_fcl);
+        tab.sd_str = reinterpret_cast<const unsigned *>(dbase + o_sst);
+        tab.sd_ord = reinterpret_cast<const int *>(dbase + o_sor);
+        tab.sd_hpos = reinterpret_cast<const int *>(dbase + o_shp);
+        tab.sd_coff = reinterpret_cast<const int *>(dbase + o_sco);
+        tab.sd_clist = reinterpret_cast<const int *>(dbase + o_scl);
+        tab.HS = P.HS;
+        tab.H0 = P.H[0];
+        tab.H1 = P.H[1];
         edge_first = reinterpret_cast<const int *>(dbase + o_ef);
         edge_na = reinterpret_cast<const int *>(dbase + o_ena);
         depth_nodes = reinterpret_cast<const int *>(dbase + o_dn);
@@ -552,15 +775,6 @@ class Solve {
         const int nrs = P.root_na * std::max(1, P.H[P.root_player]);
         FCK(cudaMallocAsync(reinterpret_cast<void **>(&dsnap), nrs * sizeof(float), stream));
         FCK(cudaMemsetAsync(dsnap, 0, nrs * sizeof(float), stream));
-        const int nsb = static_cast<int>(P.sboards.size() / 5);
-        FCK(cudaMallocAsync(reinterpret_cast<void **>(&dstr), std::max<size_t>(1, nsb * 2 * HS) * sizeof(unsigned),
-                            stream));
-        if (nsb > 0) {
-            const int n = nsb * 2 * P.HS;
-            k_fs_strengths<<<(n + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const int *>(dbase + o_sb), nsb,
-                                                                 hand_cards, P.HS, P.H[0], P.H[1], dstr);
-            FCK(cudaGetLastError());
-        }
         c.fr_off = reinterpret_cast<const int *>(dbase + o_fro);
         c.fr_items = reinterpret_cast<const int *>(dbase + o_fri);
         c.iter = diter;
@@ -583,10 +797,9 @@ class Solve {
     }
 
     cudaError_t terms(int t, float *out, int scaled) {
-        const int n = static_cast<int>(P.term[t].size());
-        if (n == 0) return cudaSuccess;
-        k_fs_term<<<n, kFsThreads, 0, stream>>>(term_items[t], t, c.reach, hand_cards, dstr, P.HS, P.H[0], P.H[1],
-                                                out, scaled);
+        const int nf = P.nfold[t], ns = static_cast<int>(P.term[t].size()) - nf;
+        if (nf > 0) k_fs_fold<<<nf, kFsThreads, 0, stream>>>(term_items[t], t, c.reach, tab, out, scaled);
+        if (ns > 0) k_fs_showdown<<<ns, kFsThreads, 0, stream>>>(term_items[t] + nf, t, c.reach, tab, out, scaled);
         return cudaGetLastError();
     }
 

@@ -43,9 +43,22 @@ struct FsPlan {
     std::vector<std::vector<CfvItem>> cfv_levels[2];
     std::vector<int> cfv_nlong[2];
     std::vector<int> fr_off, fr_items;
-    std::vector<FsTermItem> term[2];
+    std::vector<FsTermItem> term[2];   // per traverser: folds, then showdowns
+    int nfold[2] = {0, 0};
     std::vector<int> sboards;          // [nsb][5] river boards of the showdowns
     std::vector<int> hand_cards;       // [2][HS]: c0 | c1 << 8, -1 padding
+    std::vector<int> f_coff, f_clist;  // [2][53], [2][2 * HS]: each player's hands holding card c
+    // showdown tables per river board b and player p, [nsb][2][...]:
+    //   ord  [HS]   hand index at each position of ascending strength (board-
+    //               blocked hands, strength 0, first), -1 past the range
+    //   hpos [HS]   per hand (as traverser): int4 {lo | hi << 16, c1 | c2 << 8,
+    //               l1lo | l1hi << 16, l2lo | l2hi << 16} -- the opponent's
+    //               positions below its strength (lo) and up to it (hi), and the
+    //               same counts within the opponent's list of each of its cards
+    //   coff [53]   the opponent p's card lists: hands holding card c at
+    //   clist[2*HS] clist[coff[c] .. coff[c+1]), by position
+    std::vector<int> sd_ord, sd_hpos, sd_coff, sd_clist;
+    std::vector<unsigned> sd_str;      // [nsb][2][HS] strengths (0: blocked / padding)
     std::vector<int> depth_nodes;      // read-out: nodes by BFS depth, deepest level first
     std::vector<int> depth_off;        // [levels + 1]
 };
