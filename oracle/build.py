@@ -9,7 +9,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "lib", "liboracle.so")
-SRCS = ["ss_oracle.c", "ss_oracle_impl.h", "ss_oracle.h", "oracle_eval.h", "oracle_bench.c"]
+SRCS = ["ss_oracle.c", "ss_oracle_impl.h", "ss_oracle.h", "oracle_eval.h", "oracle_bench.c", "fs_oracle.c",
+        "fs_oracle_impl.h"]
 
 
 def build(force=False):

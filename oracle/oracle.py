@@ -478,3 +478,40 @@ class RefSolverC:
 
 def ref_solver_available():
     return os.path.exists(os.path.join(REF_DIR, "libref_solver.so"))
+
+
+class FlopOracle:
+    """The multi-street solve restated in C (fs_oracle.c, in liboracle.so):
+    the reference's flop_solve.cu loop in float (its arithmetic and order,
+    fused multiply-adds included) or double, on a tree from fs_build_tree."""
+
+    def __init__(self, path=None):
+        self.lib = ctypes.CDLL(path or _default_oracle_path())
+        for f in ("fso_solve_f32", "fso_solve_f64"):
+            getattr(self.lib, f).restype = ctypes.c_int
+
+    def solve(self, nodes, children, node_depth, max_depth, hands, weights, nh, iterations, precision="f32"):
+        """nodes [N, 13] int32 (FSNode fields), hands [2][200][2], weights
+        [2][200]; returns root_strategy, all_avg_strategies [N][6][max_h] and
+        all_cfv [N][max_h]."""
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        children = np.ascontiguousarray(children, np.int32)
+        nd = np.ascontiguousarray(node_depth, np.int32)
+        hands = np.ascontiguousarray(hands, np.int32)
+        weights = np.ascontiguousarray(weights, np.float32)
+        nh = np.ascontiguousarray(nh, np.int32)
+        N = nodes.shape[0]
+        mh = int(nh.max())
+        dt = np.float32 if precision == "f32" else np.float64
+        ptr = _f32p if precision == "f32" else _f64p
+        rp, na = int(nodes[0, 1]), int(nodes[0, 2])
+        rs = np.zeros(max(na * int(nh[rp]), 1), dt)
+        avg = np.zeros(N * 6 * mh, dt)
+        cfv = np.zeros(N * mh, dt)
+        fn = self.lib.fso_solve_f32 if precision == "f32" else self.lib.fso_solve_f64
+        rc = fn(_i32p(nodes), _i32p(children), N, _i32p(nd), int(max_depth), _i32p(hands), _f32p(weights),
+                _i32p(nh), int(iterations), ptr(rs), ptr(avg), ptr(cfv))
+        if rc != 0:
+            raise RuntimeError("fso_solve failed")
+        return {"root_strategy": rs[:na * int(nh[rp])].reshape(na, int(nh[rp])),
+                "all_avg_strategies": avg.reshape(N, 6, mh), "all_cfv": cfv.reshape(N, mh)}
