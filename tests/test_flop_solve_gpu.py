@@ -57,12 +57,34 @@ def test_root_strategy_against_reference(seed, flop, n, pot, stack, sizes, iters
 
 @pytest.mark.gpu
 def test_extract_all_against_reference():
-    a, b, dec = pair(4, [9, 21, 35], 16, 1000, 5000, [0.75], 5, True)
+    """Every decision node's average strategy and every node's value after 5
+    iterations.  On 16-hand ranges some hands' values tie exactly in one
+    summation order and not in another, and regret matching turns that into a
+    different strategy, so the element-wise bound is the envelope of
+    tests/test_parity_gpu.py: this solver may be no further from the FP64
+    restatement (oracle/fs_oracle.c) than ENVELOPE times the reference's own
+    FP32 distance from it, plus the 1e-4 tolerances."""
+    from oracle.oracle import FlopOracle
+    from test_parity_gpu import ENVELOPE
+    seed, flop, n, pot, stack, sizes, iters = 4, [9, 21, 35], 16, 1000, 5000, [0.75], 5
+    a, b, dec = pair(seed, flop, n, pot, stack, sizes, iters, True)
     assert np.array_equal(a["turn_root_indices"], b["turn_root_indices"])
     assert np.array_equal(a["turn_root_cards"], b["turn_root_cards"])
-    assert len(a["turn_root_indices"]) == 49 * 2 or len(a["turn_root_indices"]) > 0
-    mh = a["max_hands"]
-    assert np.abs(a["all_avg_strategies"][dec] - b["all_avg_strategies"][dec]).max() <= 1e-4
-    scale = max(np.abs(b["all_cfv"]).max(), 1e-30)
-    assert np.abs(a["all_cfv"] - b["all_cfv"]).max() / scale <= 1e-4
-    assert mh == b["max_hands"]
+    assert len(a["turn_root_indices"]) > 0 and a["max_hands"] == b["max_hands"]
+    lib = fsm.bind(ssg.load_library(200))
+    h, w = ranges(seed, flop, n)
+    sg = fsm.FlopSubgame(lib, flop, pot, stack, sizes, h, w)
+    nodes, ch, _, nd, _, _ = fsm.tree_arrays(sg.td)
+    H = np.zeros((2, 200, 2), np.int32)
+    W = np.zeros((2, 200), np.float32)
+    for p in range(2):
+        H[p, :n], W[p, :n] = h[p], w[p]
+    e = FlopOracle().solve(nodes, ch, nd, sg.td.max_depth, H, W, np.array([n, n], np.int32), iters, "f64")
+    sg.free()
+    da = np.abs(a["all_avg_strategies"][dec] - e["all_avg_strategies"][dec]).max()
+    db = np.abs(b["all_avg_strategies"][dec] - e["all_avg_strategies"][dec]).max()
+    assert da <= ENVELOPE * db + 1e-4, f"avg strategy: ours-f64 {da}, reference f32-f64 {db}"
+    scale = max(np.abs(e["all_cfv"]).max(), 1e-30)
+    va = np.abs(a["all_cfv"] - e["all_cfv"]).max() / scale
+    vb = np.abs(b["all_cfv"] - e["all_cfv"]).max() / scale
+    assert va <= ENVELOPE * vb + 1e-4, f"values: ours-f64 {va}, reference f32-f64 {vb}"
