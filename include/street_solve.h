@@ -320,7 +320,10 @@ int ss_rank7_checksum(unsigned long long *checksum, unsigned long long *category
  * like ss_solve_gpu's, and ss_free_output must not be called on them.  A
  * subgame whose state exceeds the array fails with SS_ERR_NOMEM and the size
  * it needs.  The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * (cudaGetSymbolAddress) and should come before any stream capture; the
+ * address is kept for the life of the process, so a caller that destroys the
+ * device's primary context (cudaDeviceReset) must not call this entry point
+ * on that device afterwards.  All calls
  * share the array and it keeps the previous call's data (each call rewrites
  * what it reads); calls that overlap on the same GPU race. */
 int ss_solve_gpu_noalloc(SSTreeData *tree_data, int max_iterations, SSOutput *output);

@@ -82,6 +82,29 @@ def test_noalloc_matches_solve_twice(name, nh, iters):
 
 
 @pytest.mark.gpu
+def test_noalloc_interleaved_subgames():
+    """A heads-up river, then a 3-player turn with other leaf values, then
+    the river again, all in the one shared array: each call must rewrite what
+    it reads, so every result equals its own ss_solve_gpu solve."""
+    river = wl.config("hu_river", seed=41, num_hands=90)
+    turn = wl.config("turn3", seed=42, num_hands=12, bet_sizes=[0.75], max_raises=2)
+    subs = []
+    for cfg, seed in ((river, 0), (turn, 777)):
+        sg = wl.AbiSubgame(cfg)
+        sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves, seed_offset=seed + 1000))
+        subs.append(sg)
+    refs = []
+    for sg in subs:
+        rc, ref = sg.solve(8)
+        assert rc == 0, ssg.last_error(sg.lib)
+        refs.append(ref)
+    for k in (0, 1, 0):
+        same(noalloc_solve(subs[k], 8), refs[k])
+    for sg in subs:
+        sg.free()
+
+
+@pytest.mark.gpu
 def test_noalloc_refuses_oversized_subgame():
     cfg = wl.config("turn3", seed=0)  # ~600 MB of device state
     sg = wl.AbiSubgame(cfg, max_hands=1326)
