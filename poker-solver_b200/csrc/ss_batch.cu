@@ -6,8 +6,9 @@
 // its subgame's context, item.sg); one launch advances every member's
 // iteration counter and one per pass snapshots the root strategies.  A block
 // of iterations is captured as one CUDA graph; members can be added or
-// retired between blocks (the graph is rebuilt), each keeps its own iteration
-// count, and arithmetic per subgame is identical to a solve alone.
+// retired between blocks, each keeps its own iteration count, and arithmetic
+// per subgame is identical to a solve alone (three-way showdown sweeps keep
+// each subgame's own run merge through a block map).
 //
 // Server: continuous batching on one GPU.  Requests are copied at submission
 // and admitted into the running batch while their estimated device footprint
@@ -171,6 +172,10 @@ class Batch {
         size_t off; // item offset in dlists
         int n;
         int H;      // largest hand count of the launch
+        // three-way showdowns: block -> (item, run group) map, blocks, largest merge
+        size_t map_off = 0;
+        int map_blocks = 0;
+        int map_lg = 0;
     };
     DevCtx *dctx = nullptr;
     char *dlists = nullptr;
@@ -188,6 +193,10 @@ class Batch {
             case L_BUMP: return launch_bump_many(dctx, reinterpret_cast<const int *>(dlists + L.off), L.n, stream);
             case L_SNAP: return launch_snapshot_many(dctx, reinterpret_cast<const int *>(dlists + L.off), L.n, stream);
             case L_TERM:
+                if (L.kind == TK_SD2)
+                    return launch_sd2_mapped(cmax, reinterpret_cast<const TermItem *>(dlists + L.off),
+                                             reinterpret_cast<const int2 *>(dlists + L.map_off), L.map_blocks,
+                                             L.map_lg, L.t, stream, dctx, false);
                 return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
                                     stream, dctx);
             case L_CFV:
@@ -202,6 +211,10 @@ class Batch {
                 return launch_br_reach_many(dctx, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H,
                                             L.t, stream);
             case L_BR_TERM:
+                if (L.kind == TK_SD2)
+                    return launch_sd2_mapped(cmax, reinterpret_cast<const TermItem *>(dlists + L.off),
+                                             reinterpret_cast<const int2 *>(dlists + L.map_off), L.map_blocks,
+                                             L.map_lg, L.t, stream, dctx, true);
                 return launch_terms_fp64(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
                                          stream, dctx);
             case L_BR_VALUE:
@@ -279,6 +292,23 @@ class Batch {
             if (bytes) std::memcpy(blob.data() + off, src, bytes);
             return off;
         };
+        // a terminal launch over merged items; three-way showdowns also get the
+        // block map that sweeps each subgame with its own run merge
+        auto term_launch = [&](int type, int k, int t, const std::vector<TermItem> &items) {
+            Launch L{type, k, t, put(items.data(), items.size() * sizeof(TermItem)), static_cast<int>(items.size()),
+                     0};
+            if (k == TK_SD2) {
+                std::vector<int2> bmap;
+                for (size_t i = 0; i < items.size(); ++i) {
+                    const int lg = items[i].kind_detail;
+                    L.map_lg = std::max(L.map_lg, lg);
+                    for (int g = 0; g < (kSd2Chunks >> lg); ++g) bmap.push_back(make_int2(static_cast<int>(i), g));
+                }
+                L.map_off = put(bmap.data(), bmap.size() * sizeof(int2));
+                L.map_blocks = static_cast<int>(bmap.size());
+            }
+            return L;
+        };
         std::vector<int> act;
         int maxnp = 0, maxh = 0;
         for (int i = 0; i < K; ++i) {
@@ -308,9 +338,7 @@ class Batch {
                     }
                     add_work(i, subs[i]->P.term[t][k].size());
                 }
-                if (!items.empty())
-                    seq.push_back({L_TERM, k, t, put(items.data(), items.size() * sizeof(TermItem)),
-                                   static_cast<int>(items.size()), 0});
+                if (!items.empty()) seq.push_back(term_launch(L_TERM, k, t, items));
             }
             size_t lv = 0;
             for (int i : act)
@@ -399,9 +427,7 @@ class Batch {
                         items.push_back(it);
                     }
                 }
-                if (!items.empty())
-                    br_seq.push_back({L_BR_TERM, k, t, put(items.data(), items.size() * sizeof(TermItem)),
-                                      static_cast<int>(items.size()), 0});
+                if (!items.empty()) br_seq.push_back(term_launch(L_BR_TERM, k, t, items));
             }
             size_t lv = 0;
             for (int i : act)
@@ -446,9 +472,7 @@ class Batch {
                         it.sg = i;
                         items.push_back(it);
                     }
-                if (!items.empty())
-                    br_seq.push_back({L_BR_TERM, k, 0, put(items.data(), items.size() * sizeof(TermItem)),
-                                      static_cast<int>(items.size()), 0});
+                if (!items.empty()) br_seq.push_back(term_launch(L_BR_TERM, k, 0, items));
             }
             for (int i : act)
                 roots.push_back({subs[i]->br_row, 1, i, 0, subs[i]->P.E, 1, i * kSlots + 2 * SS_MAX_PLAYERS});

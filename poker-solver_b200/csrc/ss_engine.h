@@ -117,6 +117,15 @@ constexpr int kSd2Slots = 148 * 4;
 // terminals in one launch (batches) need fewer, longer sweeps.
 constexpr int kSd2Merge = 5;
 static_assert(kSd2Chunks == 1 << (kSd2Merge - 1), "runs merge in powers of two");
+// a solve's launch of three-way showdowns merges runs (lg > 0) once it would
+// exceed this many sweep blocks; the choice belongs to the subgame (its
+// TermItem.kind_detail), so a batch sweeps each subgame as a solve alone does
+constexpr int kSd2BlocksTarget = 2 * 148 * 4;
+inline int sd2_merge_of(int n_terms) {
+    int lg = 0;
+    while (lg < kSd2Merge - 1 && n_terms * (kSd2Chunks >> lg) > kSd2BlocksTarget) ++lg;
+    return lg;
+}
 
 // Folds and leaves with three counted opponents use the conditioning closed
 // form (TK_CR3) once every counted range holds at least this many hands and
@@ -148,7 +157,7 @@ enum TermKind : int {
 constexpr int kTermGroupMax = 16;
 struct alignas(16) TermItem {
     int node;
-    int kind_detail;          // TK_ENUM: 0 fold, 1 leaf, 2 showdown
+    int kind_detail;          // TK_ENUM: 0 fold, 1 leaf, 2 showdown; TK_SD2: log2 of the runs per block
     int k;                    // number of counted opponents
     int leaf_off;
     float payoff;

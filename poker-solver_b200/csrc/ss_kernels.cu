@@ -1269,7 +1269,6 @@ __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevC
 // ---------------------------------------------------------------------------
 constexpr int SD2_S = 49;   // row stride of the sweep's card matrices (odd: conflict-free columns)
 constexpr int SD2_N = 48;   // cards a matrix covers (dense indices; a river deck has 47)
-constexpr int kSd2BlocksTarget = 2 * 148 * 4;   // sweep blocks per launch before runs merge
 static_assert(kTermThreads == 256, "the sweep's thread roles assume 256 threads");
 
 // the opponents' reach by rank position; after the sweep the same space holds
@@ -1589,15 +1588,26 @@ __device__ __forceinline__ void sd2_phase_mass(Sd2State st, const T *M1, const T
 }
 
 // One block per 2^lgm consecutive runs of a terminal's sweep (grid: items x
-// kSd2Chunks / 2^lgm).
+// kSd2Chunks / 2^lgm).  With bmap (batches), block b serves item bmap[b].x,
+// run group bmap[b].y, with that item's own lgm (its subgame's solo choice).
 template <class T>
 __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const DevCtx *__restrict__ ctxs,
-                                                              const TermItem *__restrict__ items, int trav, int lgm) {
+                                                              const TermItem *__restrict__ items, int trav, int lgm,
+                                                              const int2 *__restrict__ bmap) {
     extern __shared__ __align__(16) char smem[];
-    const int per = kSd2Chunks >> lgm;
-    const TermItem I = items[blockIdx.x / per];
+    int it_idx, grp;
+    if (bmap) {
+        const int2 m = bmap[blockIdx.x];
+        it_idx = m.x;
+        grp = m.y;
+        lgm = items[it_idx].kind_detail;
+    } else {
+        const int per = kSd2Chunks >> lgm;
+        it_idx = blockIdx.x / per;
+        grp = blockIdx.x % per;
+    }
+    const TermItem I = items[it_idx];
     if (retired(ctxs, I.sg)) return;
-    const int grp = blockIdx.x % per;
     const int o1 = I.opp_player[0], o2 = I.opp_player[1];
     const T *reach;
     T *val;
@@ -2465,12 +2475,11 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             break;
         case TK_SD2: {
             // runs per block: about two waves of four blocks per SM at most
-            int lgm = 0;
-            while (lgm < kSd2Merge - 1 && n * (kSd2Chunks >> lgm) > kSd2BlocksTarget) ++lgm;
+            const int lgm = sd2_merge_of(n);
             const size_t sm = sd2_smem<T>(c.sd_span[lgm], c.ncomb);
             e = cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
             if (e != cudaSuccess) return e;
-            k_term_sd2<T><<<n * (kSd2Chunks >> lgm), kTermThreads, sm, s>>>(c, ctxs, items, trav, lgm);
+            k_term_sd2<T><<<n * (kSd2Chunks >> lgm), kTermThreads, sm, s>>>(c, ctxs, items, trav, lgm, nullptr);
             break;
         }
         case TK_ENUM: {
@@ -2506,6 +2515,24 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s, const DevCtx *ctxs) {
     return launch_terms_t<float>(c, kind, items, n, trav, s, ctxs);
+}
+
+template <class T>
+cudaError_t launch_sd2_mapped_t(const DevCtx &c, const TermItem *items, const int2 *bmap, int nblocks, int lg_max,
+                                int trav, cudaStream_t s, const DevCtx *ctxs) {
+    if (nblocks <= 0) return cudaSuccess;
+    const size_t sm = sd2_smem<T>(c.sd_span[lg_max], c.ncomb);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
+    if (e != cudaSuccess) return e;
+    k_term_sd2<T><<<nblocks, kTermThreads, sm, s>>>(c, ctxs, items, trav, 0, bmap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sd2_mapped(const DevCtx &c, const TermItem *items, const int2 *bmap, int nblocks, int lg_max,
+                              int trav, cudaStream_t s, const DevCtx *ctxs, bool fp64) {
+    return fp64 ? launch_sd2_mapped_t<double>(c, items, bmap, nblocks, lg_max, trav, s, ctxs)
+                : launch_sd2_mapped_t<float>(c, items, bmap, nblocks, lg_max, trav, s, ctxs);
 }
 
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,

@@ -94,6 +94,12 @@ cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n
                          cudaStream_t s, const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                               cudaStream_t s, const DevCtx *ctxs = nullptr);
+// Three-way showdowns of many subgames (batches): block b sweeps run group
+// bmap[b].y of item bmap[b].x with that item's own merge (kind_detail), so
+// each subgame is swept exactly as in its own solve; lg_max sizes the shared
+// memory.  FP32 (CFR) or FP64 (best response).
+cudaError_t launch_sd2_mapped(const DevCtx &c, const TermItem *items, const int2 *bmap, int nblocks, int lg_max,
+                              int trav, cudaStream_t s, const DevCtx *ctxs, bool fp64);
 // batched best response: every item reads the context of its subgame (item.sg)
 cudaError_t launch_avg_many(const DevCtx *ctxs, const AvgItem *items, int n, int max_h, cudaStream_t s);
 cudaError_t launch_br_reach_many(const DevCtx *ctxs, const ReachItem *items, int n, int H, int player,

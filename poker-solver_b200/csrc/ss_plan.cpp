@@ -524,6 +524,11 @@ int build_plan(const Problem &pb, Plan *out) {
     double hsum = 0;
     for (int p = 0; p < np; ++p) hsum += P.H[p];
     P.node_hands = static_cast<double>(N) * hsum;
+    // three-way showdowns: the run merge of this subgame's own launch
+    for (int t = 0; t < np; ++t) {
+        const int lg = sd2_merge_of(static_cast<int>(P.term[t][TK_SD2].size()));
+        for (TermItem &it : P.term[t][TK_SD2]) it.kind_detail = lg;
+    }
     return SS_OK;
 }
 

@@ -1,10 +1,7 @@
 """Batched and served forms: every subgame's result must be the same whether
 it is solved alone or together with others (the batch merges launches, not
-arithmetic), and retirement at an exploitability target must hold.  One
-exception is stated and tested: a launch holding many three-way showdowns
-gives each sweep block several of a terminal's runs, so those FP64 masses
-round differently from a solo solve; results then agree within the parity
-tolerance."""
+arithmetic -- three-way showdown sweeps keep each subgame's own run merge),
+and retirement at an exploitability target must hold."""
 import numpy as np
 import pytest
 
@@ -62,11 +59,10 @@ def test_batch_equals_alone():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("count", [3, 15])
-def test_batch_merged_sweep_runs_agree_with_alone(count):
+def test_batch_many_sweeps_equal_alone(count):
     # full-range 3-player rivers, 40 three-way showdowns per traverser each:
-    # 3 of them (120 per launch) make the batch merge the sweep's runs
-    # pairwise, 15 (600 per launch) give each block all 16 runs, a whole
-    # sweep without directly computed states (a solo solve merges nothing)
+    # 3 or 15 of them in one launch (120 / 600 terminals) -- each sweep still
+    # uses its own subgame's run split, so results are identical to solos
     subs = []
     for seed in range(71, 71 + count):
         cfg = wl.config("river6", seed=seed, num_players=3)
@@ -77,10 +73,7 @@ def test_batch_merged_sweep_runs_agree_with_alone(count):
     for sg, r in zip(subs, together):
         rc, alone = sg.solve(37)
         assert rc == 0
-        for k in ("root_strategy", "avg_strategies"):
-            np.testing.assert_allclose(r[k], alone[k], rtol=0, atol=1e-4, err_msg=k)
-        np.testing.assert_allclose(r["root_ev"], alone["root_ev"], rtol=1e-4, atol=1e-3)
-        assert np.array_equal(r["avg_node_ids"], alone["avg_node_ids"])
+        identical(r, alone)
     for sg in subs:
         sg.free()
 
