@@ -998,9 +998,15 @@ def main():
     res = run_ours(args, world, rank, local)
     batched = served = None
     if rank == 0 and world == 1 and "batched" in forms:
-        batched = run_batched(args.batch_size, args.seed, local)
+        try:
+            batched = run_batched(args.batch_size, args.seed, local)
+        except Exception as e:  # the solver's line is printed whatever happens here
+            batched = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and "served" in forms:
-        served = run_served([float(r) for r in args.rates.split(",")], args.served_requests, args.seed, local)
+        try:
+            served = run_served([float(r) for r in args.rates.split(",")], args.served_requests, args.seed, local)
+        except Exception as e:  # the solver's line is printed whatever happens here
+            served = {"error": f"{type(e).__name__}: {e}"}
     hu = None
     if rank == 0 and world == 1 and "hu_river" in forms:
         try:
