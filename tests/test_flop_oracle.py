@@ -1,14 +1,12 @@
 """Pin the multi-street oracle (oracle/fs_oracle.c) to the reference: its
-float solve reproduces the reference's own GPU results
+float solve reproduces the root strategy of the reference's own GPU solve
 (tests/golden/flop_ref_*.npz, made by make_flop_golden.py with the
-reference's sm_100a build) -- root strategy, normalised average strategies
-and values at the sampled nodes.  The float restatement repeats the
-reference's operations in its order, fused multiply-adds included, so the
-bound is 1e-6 (strategies) and 1e-6 of the largest value.  The double solve
-follows the same algorithm; where two hands' values tie exactly in one
-precision and not the other, regret matching turns the difference into a
-different strategy, so only its root strategy is held (within 1e-4) on
-these small ranges."""
+reference's sm_100a build) after 1, 2, 3 and 5 iterations.  The float
+restatement repeats the reference's operations in its order, fused
+multiply-adds included, so the bound is 1e-6.  (The reference's extraction
+entry point overflows a host buffer on every full tree, so the root strategy
+is what the reference itself can give.)  The double solve must stay within
+1e-4 of it at the root."""
 import ctypes
 import glob
 import os
@@ -53,14 +51,12 @@ def test_oracle_matches_reference_gpu(oracle_flop, path):
     g = np.load(path)
     nodes, ch, nd, md = tree_of(g)
     H, W, nh = inputs(g)
-    ids = g["node_ids"]
-    r = oracle_flop.solve(nodes, ch, nd, md, H, W, nh, int(g["iterations"]), "f32")
-    assert np.abs(r["root_strategy"] - g["root_strategy"]).max() <= 1e-6
-    assert np.abs(r["all_avg_strategies"][ids] - g["avg"]).max() <= 1e-6
-    scale = max(np.abs(g["cfv"]).max(), 1e-30)
-    assert np.abs(r["all_cfv"][ids] - g["cfv"]).max() / scale <= 1e-6
-    r64 = oracle_flop.solve(nodes, ch, nd, md, H, W, nh, int(g["iterations"]), "f64")
-    assert np.abs(r64["root_strategy"] - g["root_strategy"]).max() <= 1e-4
+    for k in g["iterations"]:
+        want = g[f"root_strategy_{int(k)}"]
+        r = oracle_flop.solve(nodes, ch, nd, md, H, W, nh, int(k), "f32")
+        assert np.abs(r["root_strategy"] - want).max() <= 1e-6, f"{int(k)} iterations"
+        r64 = oracle_flop.solve(nodes, ch, nd, md, H, W, nh, int(k), "f64")
+        assert np.abs(r64["root_strategy"] - want).max() <= 1e-4, f"{int(k)} iterations (f64)"
 
 
 @pytest.fixture(scope="module")
