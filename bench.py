@@ -499,8 +499,8 @@ def pct(v, q):
 C4_STREETS = (1 / 3, 1 / 3, 1 / 3)     # flop, turn, river
 C5_STREETS = (0.05, 0.15, 0.80)
 C4_MIX = ("flop / turn / river equally, 2-6 players (flops 2-3, turns 2-4), target tree size log-uniform "
-          "in [50, 20000] nodes by bet-set / raise-cap search, 2-3 players on every combo, 4 players on "
-          "64-128 hands, 5 on 8, 6 on 6, U(0, 0.7) of each range zeroed")
+          "in [50, 20000] nodes by bet-set / raise-cap search (5-6 players: trees up to 3000 nodes), 2-3 "
+          "players on every combo, 4 players on 64-128 hands, 5 on 6, 6 on 4, U(0, 0.7) of each range zeroed")
 
 
 def mix_stats(subs):

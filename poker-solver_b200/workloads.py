@@ -355,19 +355,28 @@ def size_table(street, np_):
     if key not in _SIZE_TABLE:
         lib = ssg.load_library(ssg.SS_MAX_HANDS_WIDE)
         nb = {"flop": 3, "turn": 4, "river": 5}[street]
-        _SIZE_TABLE[key] = sorted((_tree_nodes(lib, nb, np_, b, r), b, r) for b in SIZE_BETS for r in SIZE_RAISES)
+        tab = sorted((_tree_nodes(lib, nb, np_, b, r), b, r) for b in SIZE_BETS for r in SIZE_RAISES)
+        if np_ >= 5:
+            tab = [e for e in tab if e[0] <= MULTIWAY_MAX_NODES] or tab[:1]
+        _SIZE_TABLE[key] = tab
     return _SIZE_TABLE[key]
+
+
+# 5-6 player trees: at most this many nodes, so that their terminals without
+# a closed form (4-5 counted opponents, enumerated) stay within the solver's
+# per-solve budget of tuple visits at the ranges below
+MULTIWAY_MAX_NODES = 3000
 
 
 def range_size(np_, rng):
     """Hands per player: every combo for 2-3 players; multiway ranges are
-    narrow (4 players 64-128 hands, 5 players 8, 6 players 6), which keeps the
+    narrow (4 players 64-128 hands, 5 players 6, 6 players 4), which keeps the
     terminals without a closed form (4-5 counted opponents) enumerable."""
     if np_ <= 3:
         return None
     if np_ == 4:
         return int(rng.integers(64, 129))
-    return 8 if np_ == 5 else 6
+    return 6 if np_ == 5 else 4
 
 
 def c4_config(rng, streets=(1 / 3, 1 / 3, 1 / 3), size=(50, 20000)):
