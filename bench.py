@@ -339,14 +339,32 @@ def run_ours(args, world, rank, local):
         if rc != 0:
             raise RuntimeError(f"{what} failed ({rc}): {ssg.last_error(lib)}")
 
-    # one profiled iteration (graph with event nodes between kernel classes)
+    class LaunchRec(ctypes.Structure):
+        _fields_ = [("cls", ctypes.c_int), ("items", ctypes.c_int), ("ms", ctypes.c_double),
+                    ("bytes", ctypes.c_double)]
+
+    # one profiled iteration (graph with event nodes between kernel classes),
+    # half-way through a solve, where reach rows and regrets look like the
+    # average timed iteration's (the first iteration's uniform strategies
+    # leave no zero reach)
     check(lib.ss_session_reset(sess), "reset")
+    check(lib.ss_session_run(sess, max(1, args.iterations // 2)), "run")
     prof = Prof()
     check(lib.ss_session_profile(sess, ctypes.byref(prof)), "profile")
-    classes = {}
+    classes, cls_names = {}, []
     for k in range(prof.num_classes):
         name = bytes(prof.name[k]).split(b"\0")[0].decode()
+        cls_names.append(name)
         classes[name] = {"launches": prof.launches[k], "ms": prof.ms[k], "bytes": prof.bytes[k]}
+    nrec = ctypes.c_int(0)
+    recs = (LaunchRec * 4096)()
+    lib.ss_session_profile_launches.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_int)]
+    check(lib.ss_session_profile_launches(sess, recs, 4096, ctypes.byref(nrec)), "profile launches")
+    # per launch in launch order: class, work items, device us, GB/s of the bytes it must move
+    launch_list = [[cls_names[r.cls], r.items, round(r.ms * 1e3, 1),
+                    round(r.bytes / (r.ms / 1e3) / 1e9, 1) if r.ms > 0 else 0.0]
+                   for r in recs[:min(nrec.value, 4096)] if r.items > 0]
     launches_per_iter = sum(v["launches"] for v in classes.values())
     reach_launches = classes["reach"]["launches"]
 
@@ -474,6 +492,7 @@ def run_ours(args, world, rank, local):
                         "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
                     for k, v in classes.items() if v["launches"]},
         "iteration_ms": prof.iteration_ms,
+        "profile_launches": launch_list,
         "exploitability_pct": exploit,
         "tree": tree_info,
         "roofline_iteration": roof_iter,
@@ -694,16 +713,57 @@ def run_leaf_producer(seed, calls=3):
                                        f"({bias_s:.2f} s), scaled"}}
 
 
-def run_four_player(seed, device, short=3, long=8):
+def session_iteration_profile(lib, td, device, reps=3, warm=2):
+    """Device time of one CFR iteration of a resident session (CUDA events
+    between kernel classes, ss_session_profile): `warm` plain iterations,
+    then `reps` profiled ones; returns the median iteration and, per kernel
+    class, its median time."""
+    import street_solver_gpu as ssg
+
+    class Prof(ctypes.Structure):
+        _fields_ = [("num_classes", ctypes.c_int), ("name", (ctypes.c_char * 16) * 8),
+                    ("launches", ctypes.c_int * 8), ("ms", ctypes.c_double * 8),
+                    ("bytes", ctypes.c_double * 8), ("iteration_ms", ctypes.c_double)]
+
+    lib.ss_session_destroy.argtypes = [ctypes.c_void_p]
+    lib.ss_session_run.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    opts = ssg.SSSolveOptions(device, 10, -1.0, 50, 0)
+    sess = ctypes.c_void_p()
+    rc = lib.ss_session_create(ctypes.byref(td), ctypes.byref(opts), ctypes.byref(sess))
+    if rc != 0:
+        raise RuntimeError(f"ss_session_create failed ({rc}): {ssg.last_error(lib)}")
+    try:
+        if warm:
+            rc = lib.ss_session_run(sess, warm)
+            if rc != 0:
+                raise RuntimeError(f"ss_session_run failed ({rc}): {ssg.last_error(lib)}")
+        its, cls = [], {}
+        for _ in range(reps):
+            prof = Prof()
+            rc = lib.ss_session_profile(sess, ctypes.byref(prof))
+            if rc != 0:
+                raise RuntimeError(f"ss_session_profile failed ({rc}): {ssg.last_error(lib)}")
+            its.append(prof.iteration_ms)
+            for k in range(prof.num_classes):
+                if prof.launches[k]:
+                    name = bytes(prof.name[k]).split(b"\0")[0].decode()
+                    cls.setdefault(name, []).append(prof.ms[k])
+    finally:
+        lib.ss_session_destroy(sess)
+    med = lambda v: sorted(v)[len(v) // 2]
+    return med(its), {k: round(med(v), 3) for k, v in cls.items()}
+
+
+def run_four_player(seed, device, reps=3):
     """4-player subgames with full ranges, whose terminals with three counted
     opponents take the closed forms (folds and leaves: k_term_cr3, four-way
     showdowns: k_term_sd3): a turn with continuation leaves (1128 combos per
     player, U(0,1) weights with 30% zeroed, pot 150, stacks 500, bets {1.0
     pot} + all-in, one raise, leaf values N(0, 0.3 pot); 5,681 nodes) and a
     river (1081 combos per player, U(0,1) weights, pot 300, stacks 1000, the
-    same bets; 125 nodes).  Time per iteration from solves of `short` and
-    `long` iterations through ss_solve_gpu_ex (their difference removes the
-    set-up and the output copy)."""
+    same bets; 125 nodes).  Device time per iteration: the median of `reps`
+    profiled iterations of a resident session (after two plain ones), with
+    the per-kernel-class split."""
     import workloads as wl
     out = {}
     for street, name in (("turn", "turn3"), ("river", "river6")):
@@ -713,21 +773,15 @@ def run_four_player(seed, device, short=3, long=8):
         sg = wl.AbiSubgame(cfg)
         try:
             sg.set_leaf_values(wl.leaf_values_for(cfg, sg.num_leaves))
-            walls = {}
-            for iters in (short, short, long):
-                t0 = time.perf_counter()
-                rc, _ = sg.solve(iters, device=device)
-                walls[iters] = time.perf_counter() - t0
-                if rc != 0:
-                    raise RuntimeError(f"ss_solve_gpu failed ({rc}): {wl.ssg.last_error(sg.lib)}")
+            it_ms, classes = session_iteration_profile(sg.lib, sg.td, device, reps=reps)
             nodes, nh = sg.td.num_nodes, [len(h) for h in cfg["hands"]]
         finally:
             sg.free()
-        per_it = (walls[long] - walls[short]) / (long - short)
-        out[street] = {"tree_nodes": nodes, "hands": nh[0], "ms_per_iteration": 1e3 * per_it,
+        per_it = it_ms / 1e3
+        out[street] = {"tree_nodes": nodes, "hands": nh[0], "ms_per_iteration": it_ms, "classes_ms": classes,
                        "node_hand_updates_per_s": nodes * sum(nh) / per_it if per_it > 0 else None,
                        "solve_1000_iterations_s_est": 1000 * per_it}
-    out["sample"] = f"solves of {short} and {long} iterations each"
+    out["sample"] = f"median of {reps} profiled iterations (CUDA events per kernel class) after 2 plain ones"
     return out
 
 
@@ -1063,6 +1117,7 @@ def main():
             "e2e": res["e2e"], "gpu_launches": res["gpu_launches"],
             "node_hand_updates_per_s": res["value"] * res["nhu_per_solve"],
             "iteration_ms": res["iteration_ms"], "profile": res["profile"],
+            "profile_launches": res["profile_launches"],
             "exploitability_pct_after_solve": res["exploitability_pct"],
             "batched": batched, "served": served, "hu_river": hu, "leaf_producer": leaf, "four_player": four,
             "anchor_same_config": anchor, "flop_solver": flop,

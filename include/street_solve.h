@@ -180,6 +180,17 @@ typedef struct {
     double iteration_ms;                 /* device time of the whole iteration */
 } SSKernelProfile;
 
+/* One launch of the profiled iteration (ss_session_profile_launches), in
+ * launch order: its class (index into SSKernelProfile.name), the work items
+ * it covers (decision nodes of one level, or terminals), device time and the
+ * bytes it must move. */
+typedef struct {
+    int cls;
+    int items;
+    double ms;
+    double bytes;
+} SSLaunchRecord;
+
 /* ── Host API ────────────────────────────────────────────────────────── */
 
 #ifdef __cplusplus
@@ -266,6 +277,11 @@ int ss_session_output(SSSession *session, SSOutput *output);
 /* EXTENSION: run one more iteration as a graph with event nodes between the
  * kernel classes and report their device times and minimum bytes. */
 int ss_session_profile(SSSession *session, SSKernelProfile *profile);
+
+/* EXTENSION: the launches of the iteration the last ss_session_profile call
+ * timed.  Writes at most max_records records and the launch count into
+ * *num_records (either pointer may be NULL when max_records is 0). */
+int ss_session_profile_launches(SSSession *session, SSLaunchRecord *records, int max_records, int *num_records);
 
 /* EXTENSION: the CUDA stream (cudaStream_t) the session's kernels run on, so a
  * caller can order its own work or time the session with CUDA events. */

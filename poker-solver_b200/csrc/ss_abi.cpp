@@ -305,6 +305,11 @@ int ss_session_profile(SSSession *s, SSKernelProfile *prof) {
     return ssb::session_profile(s->impl, prof);
 }
 
+int ss_session_profile_launches(SSSession *s, SSLaunchRecord *records, int max_records, int *num_records) {
+    if (!s || max_records < 0 || (max_records > 0 && !records)) return SS_ERR_INVALID;
+    return ssb::session_profile_launches(s->impl, records, max_records, num_records);
+}
+
 int ss_session_exploitability(SSSession *s, double *pct, double *nash, double *br, double *cur,
                               double *z) {
     if (!s) return SS_ERR_INVALID;

@@ -176,6 +176,8 @@ class Batch {
         size_t map_off = 0;
         int map_blocks = 0;
         int map_lg = 0;
+        int n_wide = 0;     // value/regret launches: very long items at the end
+        int cr2_form = -1;  // two-opponent terminals: 1 tensor-core form, 0 mma.sync form
     };
     DevCtx *dctx = nullptr;
     char *dlists = nullptr;
@@ -197,11 +199,20 @@ class Batch {
                     return launch_sd2_mapped(cmax, reinterpret_cast<const TermItem *>(dlists + L.off),
                                              reinterpret_cast<const int2 *>(dlists + L.map_off), L.map_blocks,
                                              L.map_lg, L.t, stream, dctx, false);
+                if (L.cr2_form >= 0) {
+                    // the launch context picks the form: a dense deck of 48 and no
+                    // repeated combo for the tensor-core one, no deck for the other
+                    DevCtx cl = cmax;
+                    cl.deck = L.cr2_form == 1 ? 48 : 0;
+                    for (int p = 0; p < SS_MAX_PLAYERS; ++p) cl.dup[p] = 0;
+                    return launch_terms(cl, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
+                                        stream, dctx);
+                }
                 return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
                                     stream, dctx);
             case L_CFV:
                 return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.kind, L.H, stream,
-                                  dctx, L.t);
+                                  dctx, L.t, L.n_wide);
             case L_REACH:
                 return launch_reach(cmax, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H, stream,
                                     dctx, L.t);
@@ -329,42 +340,58 @@ class Batch {
                 seq.push_back({L_SNAP, 0, t, put(snap.data(), snap.size() * sizeof(int)), static_cast<int>(snap.size()),
                                0});
             for (int k = 0; k < TK_COUNT; ++k) {
-                std::vector<TermItem> items;
-                for (int i : act) {
-                    if (subs[i]->P.np <= t) continue;
-                    for (TermItem it : subs[i]->P.term[t][k]) {
-                        it.sg = i;
-                        items.push_back(it);
+                // two-opponent terminals: one launch per product form, so each
+                // subgame's terminals take the form they take in a solo solve
+                for (int form = (k == TK_CR2 ? 1 : -1); form >= (k == TK_CR2 ? 0 : -1); --form) {
+                    std::vector<TermItem> items;
+                    for (int i : act) {
+                        if (subs[i]->P.np <= t) continue;
+                        if (form >= 0 && cr2_tensor_form(subs[i]->c) != (form == 1)) continue;
+                        for (TermItem it : subs[i]->P.term[t][k]) {
+                            it.sg = i;
+                            items.push_back(it);
+                        }
+                        add_work(i, subs[i]->P.term[t][k].size());
                     }
-                    add_work(i, subs[i]->P.term[t][k].size());
+                    if (items.empty()) continue;
+                    Launch L = term_launch(L_TERM, k, t, items);
+                    L.cr2_form = form;
+                    seq.push_back(L);
                 }
-                if (!items.empty()) seq.push_back(term_launch(L_TERM, k, t, items));
             }
             size_t lv = 0;
             for (int i : act)
                 if (subs[i]->P.np > t) lv = std::max(lv, subs[i]->P.cfv_levels[t].size());
             for (size_t l = 0; l < lv; ++l) {
-                // every subgame's short items, then every subgame's long ones
-                std::vector<CfvItem> items, longs;
+                // every subgame's short items, then every subgame's long
+                // ones, then every subgame's very long ones (each item keeps
+                // its own subgame's class, so it is summed as in a solo solve)
+                std::vector<CfvItem> items, longs, wides;
                 int H = 0;
                 for (int i : act) {
                     const Plan &P = subs[i]->P;
                     if (P.np <= t || l >= P.cfv_levels[t].size()) continue;
                     const auto &v = P.cfv_levels[t][l];
                     const size_t n_short = v.size() - static_cast<size_t>(P.cfv_nlong[t][l]);
+                    const size_t n_split = v.size() - static_cast<size_t>(P.cfv_nwide[t][l]);
                     for (size_t j = 0; j < v.size(); ++j) {
                         CfvItem it = v[j];
                         it.sg = i;
-                        (j < n_short ? items : longs).push_back(it);
+                        (j < n_short ? items : j < n_split ? longs : wides).push_back(it);
                     }
                     add_work(i, v.size());
                     H = std::max(H, P.H[t]);
                 }
-                const int n_long = static_cast<int>(longs.size());
+                const int n_wide = static_cast<int>(wides.size());
+                const int n_long = static_cast<int>(longs.size()) + n_wide;
                 items.insert(items.end(), longs.begin(), longs.end());
-                if (!items.empty())
-                    seq.push_back({L_CFV, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
-                                   static_cast<int>(items.size()), H});
+                items.insert(items.end(), wides.begin(), wides.end());
+                if (!items.empty()) {
+                    Launch L{L_CFV, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
+                             static_cast<int>(items.size()), H};
+                    L.n_wide = n_wide;
+                    seq.push_back(L);
+                }
             }
             lv = 0;
             for (int i : act)

@@ -236,6 +236,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     const size_t o_fr_items = b.add(P.fr_items);
     const size_t o_code = b.add(P.hand_code);
     const size_t o_pair = b.add(P.pair_idx);
+    const size_t o_cross = b.add(P.cross_idx);
     const size_t o_sdpos = b.add(P.sd_pos);
     const size_t o_str = b.add(P.strength);
     const size_t o_sdc = b.add(P.sd_combo);
@@ -303,6 +304,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.fr_items = reinterpret_cast<const int *>(dbase + o_fr_items);
     c.hand_code = reinterpret_cast<const int *>(dbase + o_code);
     c.pair_idx = reinterpret_cast<const int *>(dbase + o_pair);
+    c.cross_idx = reinterpret_cast<const int *>(dbase + o_cross);
     c.sd_pos = reinterpret_cast<const int *>(dbase + o_sdpos);
     c.strength = reinterpret_cast<const unsigned *>(dbase + o_str);
     c.sd_combo = reinterpret_cast<const SdCombo *>(dbase + o_sdc);
@@ -402,12 +404,18 @@ int Session::output(SSOutput *out) {
                             cudaMemcpyDeviceToHost, stream);
     cudaFreeAsync(davg, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) {
+    unsigned fault = 0;
+    if (e == cudaSuccess) e = read_device_fault(&fault, stream);
+    if (e != cudaSuccess || fault) {
         std::free(h_rs);
         std::free(h_rev);
         host_block_give(h_avg);
         std::free(h_ids);
-        set_error(std::string("CUDA: ") + cudaGetErrorString(e));
+        if (e != cudaSuccess)
+            set_error(std::string("CUDA: ") + cudaGetErrorString(e));
+        else
+            set_error("a kernel recorded a device fault (code " + std::to_string(fault) +
+                      "): the tensor-core product's completion wait ran out or it got a subgame it does not serve");
         return SS_ERR_CUDA;
     }
     for (int i = 0; i < P.num_dec; ++i) h_ids[i] = P.dec_nodes[i];
@@ -441,12 +449,14 @@ int Session::profile(SSKernelProfile *prof) {
         prof->num_classes = SS_PROFILE_CLASSES;
         for (int k = 0; k < SS_PROFILE_CLASSES; ++k)
             std::strncpy(prof->name[k], kClassName[k], sizeof(prof->name[k]) - 1);
+        last_launches.clear();
         for (size_t i = 0; i < ms.size() && e == cudaSuccess; ++i) {
             float t = 0.f;
             e = cudaEventElapsedTime(&t, ms[i].ev, i + 1 < ms.size() ? ms[i + 1].ev : end);
             prof->ms[ms[i].cls] += t;
             prof->bytes[ms[i].cls] += ms[i].bytes;
             prof->launches[ms[i].cls] += 1;
+            last_launches.push_back(SSLaunchRecord{ms[i].cls, ms[i].items, static_cast<double>(t), ms[i].bytes});
         }
         float tot = 0.f;
         if (e == cudaSuccess && !ms.empty()) e = cudaEventElapsedTime(&tot, ms.front().ev, end);
@@ -456,6 +466,14 @@ int Session::profile(SSKernelProfile *prof) {
     if (end) cudaEventDestroy(end);
     if (g) cudaGraphExecDestroy(g);
     CK(e);
+    return SS_OK;
+}
+
+int Session::profile_launches(SSLaunchRecord *rec, int max_records, int *num_records) const {
+    const int n = static_cast<int>(last_launches.size());
+    if (num_records) *num_records = n;
+    if (rec)
+        for (int i = 0; i < n && i < max_records; ++i) rec[i] = last_launches[i];
     return SS_OK;
 }
 
@@ -611,6 +629,9 @@ int session_reset(Session *s) { return s->reset(); }
 int session_iterations(const Session *s) { return s->iterations; }
 int session_output(Session *s, SSOutput *out) { return s->output(out); }
 int session_profile(Session *s, SSKernelProfile *p) { return s->profile(p); }
+int session_profile_launches(const Session *s, SSLaunchRecord *rec, int max_records, int *num_records) {
+    return s->profile_launches(rec, max_records, num_records);
+}
 int session_exploitability(Session *s, const float *host_avg, double *pct, double *nash, double *br,
                            double *cur, double *z) {
     return s->exploitability(host_avg, pct, nash, br, cur, z);

@@ -8,9 +8,11 @@
 
 #include "street_solve.h"
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace ssb {
@@ -98,8 +100,19 @@ struct alignas(16) CfvItem {
 };
 
 // A value/regret item whose edges' frontiers hold at least this many rows in
-// total is long: several warps share each of its hand chunks.
+// total is long: several warps share each of its hand chunks (more warps from
+// the second bound on).
 constexpr int kCfvLongFrontier = 48;
+constexpr int kCfvWideFrontier = 96;
+
+// Order one level's value/regret items short, long, very long (stable within
+// each class); returns {long and very long, very long} counts.
+template <class Item, class FrontierRows>
+inline std::pair<int, int> order_cfv_level(std::vector<Item> &v, FrontierRows rows) {
+    auto mid = std::stable_partition(v.begin(), v.end(), [&](const Item &it) { return rows(it) < kCfvLongFrontier; });
+    auto wide = std::stable_partition(mid, v.end(), [&](const Item &it) { return rows(it) < kCfvWideFrontier; });
+    return {static_cast<int>(v.end() - mid), static_cast<int>(v.end() - wide)};
+}
 
 // A three-way showdown's rank-order sweep is cut into at most this many runs
 // of tie groups, each swept by its own block from a directly computed state.
@@ -199,9 +212,11 @@ struct Plan {
     // per player: reach levels (top-down)
     std::vector<std::vector<ReachItem>> reach_levels[SS_MAX_PLAYERS];
     // per traverser: cfv levels (bottom-up order); within a level the items
-    // with long frontiers come last, cfv_nlong of them
+    // with long frontiers come last, cfv_nlong of them, and of those the
+    // items with very long frontiers, cfv_nwide of them
     std::vector<std::vector<CfvItem>> cfv_levels[SS_MAX_PLAYERS];
     std::vector<int> cfv_nlong[SS_MAX_PLAYERS];
+    std::vector<int> cfv_nwide[SS_MAX_PLAYERS];
     std::vector<int> fr_off;           // [E + 1]
     std::vector<int> fr_items;         // val rows (= node ids)
     std::vector<int> root_fr[SS_MAX_PLAYERS];
@@ -213,6 +228,7 @@ struct Plan {
     std::vector<int> hand_code;
     int deck = 0;                      // number of non-board cards
     std::vector<int> pair_idx;         // [np][52][52] range index of each dense-card pair, HS if none
+    std::vector<int> cross_idx;        // [np][np][HS] index in o's range of t's hand h, HS if none
     // showdown tables (river only)
     int ncomb = 0;
     std::vector<SdCombo> sd_combo;     // [ncomb]
@@ -269,6 +285,7 @@ int session_reset(Session *s);
 int session_iterations(const Session *s);
 int session_output(Session *s, SSOutput *out);
 int session_profile(Session *s, SSKernelProfile *prof);
+int session_profile_launches(const Session *s, SSLaunchRecord *rec, int max_records, int *num_records);
 void session_destroy(Session *s);
 void *session_stream(Session *s);
 int session_exploitability(Session *s, const float *host_avg, double *pct, double *nash, double *br,

@@ -13,11 +13,21 @@
 // opponents).  The reference enumerates opponent tuples per traverser hand
 // instead (street_solve.cu:704-1130), which is O(H^k).
 #include "ss_kernels.h"
+
+#include <cstdlib>
 #include "ss_cr3.cuh"
 
 namespace ssb {
 
+// Device fault word: a kernel that gives up a bounded wait on the tensor
+// cores, or gets a block it was not built for, records it here instead of
+// trapping; the host reads and clears it after a solve (read_device_fault).
+__device__ unsigned g_ss_fault = 0;
+
 namespace {
+
+constexpr unsigned kFaultTcInput = 1u;   // k_term_cr2_tc: a subgame outside its path
+constexpr unsigned kFaultTcWait = 2u;    // k_term_cr2_tc: the MMA completion wait ran out
 
 constexpr int MS = 52;  // shared-memory row stride of a 52x52 combo matrix (16-byte rows)
 
@@ -121,10 +131,12 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
 // (street_solve.cu:1155-1175): v = sum_a sigma_a ev_a; r_a = (r_a + (ev_a - v))
 // * t/(t+1); s_a += t * sigma_a; ev_a = sum of val over frontier(edge a).
 // Each lane owns 2 hands, each warp 64 consecutive hands.  S == 1: the four
-// warps of a block take four hand chunks and walk whole frontiers, eight row
-// loads in flight.  S > 1 (items with long frontiers, which are few): the S
-// warps of a block share one hand chunk and each sums every S-th frontier
-// row; warp 0 adds the S partial sums in a fixed order and updates.
+// warps of a block take four hand chunks and walk whole frontiers.  S > 1
+// (items with long frontiers, which are few): the S warps of a block share
+// one hand chunk and each sums every S-th frontier row; warp 0 adds the S
+// partial sums in a fixed order and updates.  Frontier row indices are read
+// 32 at a time (one per lane, handed out by shuffles), row values 8 at a
+// time, so a walk costs one dependent round trip per 8 rows.
 // --------------------------------------------------------------------------
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
@@ -150,10 +162,13 @@ __device__ __forceinline__ CfvView cfv_view(const DevCtx &c, int H) {
     return CfvView{c.R, c.S, c.val, c.fr_off, c.fr_items, c.iter, c.HS, H};
 }
 
+// threads per block of the value/regret kernel with S warps per hand chunk
+constexpr int cfv_threads(int S) { return S <= kCfvThreads / 32 ? kCfvThreads : 32 * S; }
+
 template <int S>
-__global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
-                                                     const CfvItem *__restrict__ items, int nchunk, int Hl,
-                                                     int trav) {
+__global__ void __launch_bounds__(cfv_threads(S), S > kCfvThreads / 32 ? 2 : 8)
+    k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs, const CfvItem *__restrict__ items, int nchunk, int Hl,
+          int trav) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const CfvItem I = items[it];
@@ -162,9 +177,10 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int h0 = (S == 1 ? ch * (kCfvThreads / 32) + warp : ch) * 64 + lane * 2;
     const bool act = h0 < V.H;
-    if (S == 1 && !act) return;
+    // whole warps past the hands leave; lanes past them stay for the shuffles
+    if (S == 1 && __all_sync(0xffffffffu, !act)) return;
     const size_t HS = static_cast<size_t>(V.HS);
-    const float *val = V.val + h0;
+    const float *val = V.val + (act ? h0 : 0);
     const int *__restrict__ fr = V.fr_items;
     // the regret and strategy-sum rows are needed after the frontier sums:
     // start bringing them into L1 now (no registers held)
@@ -191,47 +207,55 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
 #pragma unroll
         for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
         const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
-        for (int k = k0; k < kend; k += 8) {
-            float2 x[8];
+        for (int kb = k0; kb < kend; kb += 32) {
+            const int idx = kb + lane < kend ? __ldg(fr + kb + lane) : 0;
+            const int nrow = min(32, kend - kb);
+            for (int j = 0; j < nrow; j += 8) {
+                float2 x[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-                x[i] = k + i < kend ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS) : make_float2(0.f, 0.f);
+                for (int i = 0; i < 8; ++i) {
+                    const int r = __shfl_sync(0xffffffffu, idx, j + i);
+                    x[i] = (j + i < nrow && act) ? ld2(val + static_cast<size_t>(r) * HS) : make_float2(0.f, 0.f);
+                }
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (k + i < kend) {
-                    int e = 0;
+                for (int i = 0; i < 8; ++i) {
+                    const int k = kb + j + i;
+                    if (j + i < nrow) {
+                        int e = 0;
 #pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
+                        for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k >= bnd[a] ? 1 : 0;
 #pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
-                        if (e == a) add2(ev[a], x[i]);
+                        for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+                            if (e == a) add2(ev[a], x[i]);
+                    }
                 }
             }
         }
     } else {
 #pragma unroll
         for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-            if (a < I.na && act) {
+            if (a < I.na) {
+                // this warp's rows of edge a: k0, k0 + S, ... below k1, in
+                // windows of 32 (row indices one per lane)
                 float2 e = make_float2(0.f, 0.f);
-                int k = V.fr_off[I.first_edge + a] + warp;
+                const int k0 = V.fr_off[I.first_edge + a] + warp;
                 const int k1 = V.fr_off[I.first_edge + a + 1];
-                for (; k + 7 * S < k1; k += 8 * S) {
-                    float2 x[8];
+                for (int kb = k0; kb < k1; kb += 32 * S) {
+                    const int kl = kb + lane * S;
+                    const int idx = kl < k1 ? __ldg(fr + kl) : 0;
+                    const int nrow = min(32, (k1 - kb + S - 1) / S);
+                    for (int j = 0; j < nrow; j += 8) {
+                        // rows past the end add +0, so the sum is the row-order sum
+                        float2 x[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) x[i] = ld2(val + static_cast<size_t>(__ldg(fr + k + i * S)) * HS);
+                        for (int i = 0; i < 8; ++i) {
+                            const int r = __shfl_sync(0xffffffffu, idx, j + i);
+                            x[i] = (j + i < nrow && act) ? ld2(val + static_cast<size_t>(r) * HS)
+                                                         : make_float2(0.f, 0.f);
+                        }
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) add2(e, x[i]);
-                }
-                if (k < k1) {
-                    // the last (< 8) rows of this warp, loaded together; the
-                    // missing ones add +0, so the sum is the row-order sum
-                    float2 x[8];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                        x[i] = k + i * S < k1 ? ld2(val + static_cast<size_t>(__ldg(fr + k + i * S)) * HS)
-                                              : make_float2(0.f, 0.f);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) add2(e, x[i]);
+                        for (int i = 0; i < 8; ++i) add2(e, x[i]);
+                    }
                 }
                 ev[a] = e;
             }
@@ -243,7 +267,7 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
         for (int a = 0; a < SS_MAX_ACTIONS; ++a)
             if (a < I.na) part[warp][a][lane] = ev[a];
         __syncthreads();
-        if (warp != 0 || !act) return;
+        if (warp != 0) return;
 #pragma unroll
         for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
             if (a < I.na) {
@@ -254,6 +278,7 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
             }
         }
     }
+    if (!act) return;
     // the regrets are read three times (sum, value, update) instead of being
     // held in registers; the rereads hit L1
     const float *Rh = V.R + static_cast<size_t>(I.first_edge) * HS + h0;
@@ -589,6 +614,7 @@ struct Cr2View {
     T *val;
     const int *code_t, *code0, *code1;   // hand codes of the traverser and the two opponents
     const int *tab0, *tab1;              // dense-pair tables of the two opponents
+    const int *x0, *x1;                  // each traverser hand's index in the two opponents' ranges
     const float *leaf;
     int HS, deck, Ht, H0, H1;
     bool dup;
@@ -603,6 +629,8 @@ __device__ __forceinline__ Cr2View<T> cr2_view(const DevCtx &c, int trav, int o0
     v.code1 = c.hand_code + static_cast<size_t>(o1) * c.HS;
     v.tab0 = c.pair_idx + static_cast<size_t>(o0) * 52 * 52;
     v.tab1 = c.pair_idx + static_cast<size_t>(o1) * 52 * 52;
+    v.x0 = c.cross_idx + (static_cast<size_t>(trav) * c.np + o0) * c.HS;
+    v.x1 = c.cross_idx + (static_cast<size_t>(trav) * c.np + o1) * c.HS;
     v.leaf = c.leaf_values;
     v.HS = c.HS;
     v.deck = c.deck;
@@ -974,6 +1002,8 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     }
 }
 
+#include "ss_cr2_tc.cuh"
+
 template <class T>
 constexpr size_t cr1_gather_smem(int HS) {
     return (static_cast<size_t>(HS) + 4) * sizeof(T) + static_cast<size_t>(HS) * 4 + 64 * 8 + 64 * 4 +
@@ -1078,8 +1108,7 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevC
         if (h < Ht) {
             const int hc = __ldg(tc + h);
             const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
-            const bool on = (a < kCr2Off) && (b < kCr2Off);
-            const T f = on ? r[__ldg(V.tab0 + a * 52 + b)] : T(0);
+            const T f = r[__ldg(V.x0 + h)];   // 0 for a hand touching the board (index HS)
             const int live = N - nz[a] - nz[b] + (f > T(0) ? 1 : 0);
             if (live > 0) v = F - u[a] - u[b] + static_cast<double>(f);
         }
@@ -2403,7 +2432,37 @@ __global__ void __launch_bounds__(128) k_avg_strategy(DevCtx c, const int *__res
 
 inline int chunks(int H) { return (H + kHandsPerBlock - 1) / kHandsPerBlock; }
 
+// The tensor-core form of the two-opponent terminals serves dense decks of
+// at most 48 cards (turn and river boards) without repeated combos; c is the
+// launch's context (for a batch: the largest deck and the OR of every
+// member's repeated-combo flags).  SSB_CR2_TENSOR=0 in the environment keeps
+// the mma.sync form (for comparisons).
+bool tensor_product_serves(const DevCtx &c) {
+    static const bool off = [] {
+        const char *v = std::getenv("SSB_CR2_TENSOR");
+        return v && v[0] == '0';
+    }();
+    if (off || c.deck <= 0 || c.deck > kTcRows) return false;
+    for (int p = 0; p < SS_MAX_PLAYERS; ++p)
+        if (c.dup[p]) return false;
+    return true;
+}
+
 }  // namespace
+
+bool cr2_tensor_form(const DevCtx &c) { return tensor_product_serves(c); }
+
+cudaError_t read_device_fault(unsigned *code, cudaStream_t s) {
+    *code = 0;
+    cudaError_t e = cudaMemcpyFromSymbolAsync(code, g_ss_fault, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && *code) {
+        static const unsigned zero = 0;
+        e = cudaMemcpyToSymbolAsync(g_ss_fault, &zero, sizeof(unsigned), 0, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    return e;
+}
 
 cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
                          const DevCtx *ctxs, int player) {
@@ -2414,19 +2473,21 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
 }
 
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
-                       const DevCtx *ctxs, int trav) {
+                       const DevCtx *ctxs, int trav, int n_wide) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     n_long = n_long < 0 ? 0 : n_long > n ? n : n_long;
-    const int n_short = n - n_long;
+    n_wide = n_wide < 0 ? 0 : n_wide > n_long ? n_long : n_wide;
+    const int n_short = n - n_long, n_split = n_long - n_wide;
     if (n_short > 0) {
         const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
-        k_cfv<1><<<n_short * nc, kCfvThreads, 0, s>>>(c, ctxs, items, nc, H, trav);
+        k_cfv<1><<<n_short * nc, cfv_threads(1), 0, s>>>(c, ctxs, items, nc, H, trav);
     }
-    if (n_long > 0) {
-        const int nc = (H + 63) / 64;
-        static_assert(32 * kCfvSplit == kCfvThreads, "the split form fills one block of kCfvThreads");
-        k_cfv<kCfvSplit><<<n_long * nc, kCfvThreads, 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
-    }
+    const int nc = (H + 63) / 64;
+    if (n_split > 0)
+        k_cfv<kCfvSplit><<<n_split * nc, cfv_threads(kCfvSplit), 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
+    if (n_wide > 0)
+        k_cfv<kCfvSplitWide><<<n_wide * nc, cfv_threads(kCfvSplitWide), 0, s>>>(c, ctxs, items + n_short + n_split,
+                                                                              nc, H, trav);
     return cudaGetLastError();
 }
 
@@ -2458,6 +2519,15 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             // c.HS: the row stride (the largest of a batch); the staging of two
             // reach rows in the product's space needs HS <= kMaxHS
             if (c.HS > kMaxHS) return cudaErrorInvalidValue;
+            if constexpr (sizeof(T) == 4) {
+                if (tensor_product_serves(c)) {
+                    e = cudaFuncSetAttribute(k_term_cr2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(cr2_tc_smem(kMaxHS)));
+                    if (e != cudaSuccess) return e;
+                    k_term_cr2_tc<<<n, kTermThreads, cr2_tc_smem(c.HS), s>>>(c, ctxs, items, trav);
+                    break;
+                }
+            }
             const size_t sm = cr2_smem<T>(c.HS);
             if (sm > 48 * 1024)
                 e = cudaFuncSetAttribute(k_term_cr2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

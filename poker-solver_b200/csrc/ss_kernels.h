@@ -19,6 +19,7 @@ struct DevCtx {
     const int *fr_items;
     const int *hand_code;  // [np][HS]
     const int *pair_idx;   // [np][52][52] range index of each dense-card pair, HS if none
+    const int *cross_idx;  // [np][np][HS] index in opponent o's range of traverser t's hand h, HS if none
     const int *sd_pos;     // [np][HS]
     const unsigned *strength;    // [np][HS]
     const SdCombo *sd_combo;     // [ncomb]
@@ -76,8 +77,10 @@ constexpr int kHandThreads = 64;
 constexpr int kHandsPerBlock = kHandThreads * 4;
 // threads per block of the value/regret kernel (2 hands each)
 constexpr int kCfvThreads = 128;
-// warps that share one hand chunk of a value/regret item with a long frontier
+// warps that share one hand chunk of a value/regret item with a long frontier,
+// and with a very long one
 constexpr int kCfvSplit = 4;
+constexpr int kCfvSplitWide = 16;
 // threads per block of the per-terminal kernels
 constexpr int kTermThreads = 256;
 
@@ -87,9 +90,10 @@ constexpr int kTermThreads = 256;
 // count of the launch).
 cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
                          const DevCtx *ctxs = nullptr, int player = -1);
-// The last n_long items (long frontiers) run with kCfvSplit warps per hand chunk.
+// The last n_long items (long frontiers) run with kCfvSplit warps per hand
+// chunk, the last n_wide of those (very long frontiers) with kCfvSplitWide.
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
-                       const DevCtx *ctxs = nullptr, int trav = -1);
+                       const DevCtx *ctxs = nullptr, int trav = -1, int n_wide = 0);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s, const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
@@ -107,6 +111,12 @@ cudaError_t launch_br_reach_many(const DevCtx *ctxs, const ReachItem *items, int
 cudaError_t launch_br_value_many(const DevCtx *ctxs, const CfvItem *items, int n, int H, int trav, int mode,
                                  cudaStream_t s);
 cudaError_t launch_br_root_many(const DevCtx *ctxs, const RootItem *items, int n, double *out, cudaStream_t s);
+// Whether two-opponent terminals of a subgame with context c take the
+// tensor-core form (tcgen05) rather than the mma.sync form.
+bool cr2_tensor_form(const DevCtx &c);
+// The device fault word (a bounded tensor-core wait that ran out, or a block
+// a kernel was not built for): copied into *code and cleared; synchronizes s.
+cudaError_t read_device_fault(unsigned *code, cudaStream_t s);
 cudaError_t launch_bump(int *iter, cudaStream_t s);
 cudaError_t launch_bump_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s);
 cudaError_t launch_snapshot_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s);

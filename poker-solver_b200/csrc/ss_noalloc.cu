@@ -172,6 +172,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     const size_t o_fr_items = up(P.fr_items.data(), P.fr_items.size() * sizeof(int));
     const size_t o_code = up(P.hand_code.data(), P.hand_code.size() * sizeof(int));
     const size_t o_pair = up(P.pair_idx.data(), P.pair_idx.size() * sizeof(int));
+    const size_t o_cross = up(P.cross_idx.data(), P.cross_idx.size() * sizeof(int));
     const size_t o_sdpos = up(P.sd_pos.data(), P.sd_pos.size() * sizeof(int));
     const size_t o_str = up(P.strength.data(), P.strength.size() * sizeof(uint32_t));
     const size_t o_sdc = up(P.sd_combo.data(), P.sd_combo.size() * sizeof(SdCombo));
@@ -215,6 +216,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     c.fr_items = reinterpret_cast<const int *>(base + o_fr_items);
     c.hand_code = reinterpret_cast<const int *>(base + o_code);
     c.pair_idx = reinterpret_cast<const int *>(base + o_pair);
+    c.cross_idx = reinterpret_cast<const int *>(base + o_cross);
     c.sd_pos = reinterpret_cast<const int *>(base + o_sdpos);
     c.strength = reinterpret_cast<const unsigned *>(base + o_str);
     c.sd_combo = reinterpret_cast<const SdCombo *>(base + o_sdc);
@@ -261,7 +263,8 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
                                    static_cast<int>(P.term[t][k].size()), t, s0));
             for (size_t l = 0; l < cfv_lv[t].size(); ++l)
                 NA_CK(launch_cfv(c, reinterpret_cast<const CfvItem *>(base + o_cfv[t]) + cfv_lv[t][l].first,
-                                 cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t], s0));
+                                 cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t], s0, nullptr, -1,
+                                 P.cfv_nwide[t][l]));
             NA_CK(reach(t));
         }
     }

@@ -243,13 +243,13 @@ int build_plan(const Problem &pb, Plan *out) {
             P.cfv_levels[t][h].push_back(it);
         }
         P.cfv_nlong[t].assign(P.cfv_levels[t].size(), 0);
+        P.cfv_nwide[t].assign(P.cfv_levels[t].size(), 0);
         for (size_t l = 0; l < P.cfv_levels[t].size(); ++l) {
-            auto &v = P.cfv_levels[t][l];
-            auto is_short = [&](const CfvItem &it) {
-                return P.fr_off[it.first_edge + it.na] - P.fr_off[it.first_edge] < kCfvLongFrontier;
-            };
-            auto mid = std::stable_partition(v.begin(), v.end(), is_short);
-            P.cfv_nlong[t][l] = static_cast<int>(v.end() - mid);
+            const auto n = order_cfv_level(P.cfv_levels[t][l], [&](const CfvItem &it) {
+                return P.fr_off[it.first_edge + it.na] - P.fr_off[it.first_edge];
+            });
+            P.cfv_nlong[t][l] = n.first;
+            P.cfv_nwide[t][l] = n.second;
         }
     }
 
@@ -520,6 +520,21 @@ int build_plan(const Problem &pb, Plan *out) {
             P.pair_idx[(static_cast<size_t>(p) * 52 + a) * 52 + b] = h;
             P.pair_idx[(static_cast<size_t>(p) * 52 + b) * 52 + a] = h;
         }
+
+    // per (traverser t, opponent o): the range index in o's range of each of
+    // t's hands (the same two cards), HS where o has no such hand or the hand
+    // touches the board -- the terminal kernels read an opponent's reach at the
+    // traverser's own combo through it with one coalesced load per hand
+    P.cross_idx.assign(static_cast<size_t>(np) * np * HS, P.HS);
+    for (int t = 0; t < np; ++t)
+        for (int o = 0; o < np; ++o)
+            for (int h = 0; h < P.H[t]; ++h) {
+                const int hc = P.hand_code[t * HS + h];
+                if (hc & 0x10000) continue;
+                const int a = (hc >> 20) & 63, b = (hc >> 26) & 63;
+                P.cross_idx[(static_cast<size_t>(t) * np + o) * HS + h] =
+                    P.pair_idx[(static_cast<size_t>(o) * 52 + a) * 52 + b];
+            }
 
     double hsum = 0;
     for (int p = 0; p < np; ++p) hsum += P.H[p];

@@ -79,9 +79,11 @@ class Session {
     struct Mark {
         int cls;
         double bytes;
+        int items;
         cudaEvent_t ev;
     };
     std::vector<Mark> *marks = nullptr;
+    std::vector<SSLaunchRecord> last_launches;   // per launch of the last profiled iteration
 
     // terminal kinds of one pass write disjoint value rows and only read
     // reach: in the captured iteration all but one run on side streams
@@ -112,9 +114,9 @@ class Session {
         }
     }
 
-    cudaError_t mark(int cls, double bytes) {
+    cudaError_t mark(int cls, double bytes, int items = 0) {
         if (!marks) return cudaSuccess;
-        Mark m{cls, bytes, nullptr};
+        Mark m{cls, bytes, items, nullptr};
         cudaError_t e = cudaEventCreate(&m.ev);
         if (e != cudaSuccess) return e;
         marks->push_back(m);
@@ -124,7 +126,7 @@ class Session {
 
     cudaError_t reach(int p) {
         for (size_t l = 0; l < reach_lv[p].size(); ++l) {
-            cudaError_t e = mark(PC_REACH, reach_bytes[p][l]);
+            cudaError_t e = mark(PC_REACH, reach_bytes[p][l], reach_lv[p][l].second);
             if (e == cudaSuccess)
                 e = launch_reach(c, reach_items[p] + reach_lv[p][l].first, reach_lv[p][l].second,
                                  P.H[p], stream);
@@ -153,7 +155,7 @@ class Session {
             // one kind after the other (the profile times each class)
             for (int i = 0; i < nk; ++i) {
                 const int k = kinds[i];
-                e = mark(term_class(k), term_bytes[t][k]);
+                e = mark(term_class(k), term_bytes[t][k], static_cast<int>(P.term[t][k].size()));
                 if (e == cudaSuccess)
                     e = launch_terms(c, k, term_items[t][k], static_cast<int>(P.term[t][k].size()), t, stream);
                 if (e != cudaSuccess) return e;
@@ -176,10 +178,10 @@ class Session {
             if (e != cudaSuccess) return e;
         }
         for (size_t l = 0; l < cfv_lv[t].size(); ++l) {
-            e = mark(PC_CFV, cfv_bytes[t][l]);
+            e = mark(PC_CFV, cfv_bytes[t][l], cfv_lv[t][l].second);
             if (e == cudaSuccess)
                 e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.cfv_nlong[t][l],
-                               P.H[t], stream);
+                               P.H[t], stream, nullptr, -1, P.cfv_nwide[t][l]);
             if (e != cudaSuccess) return e;
         }
         return reach(t);
@@ -219,6 +221,7 @@ class Session {
     int run(int iters);
     int output(SSOutput *out);
     int profile(SSKernelProfile *prof);
+    int profile_launches(SSLaunchRecord *rec, int max_records, int *num_records) const;
 };
 
 }  // namespace ssb
