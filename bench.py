@@ -540,12 +540,19 @@ def run_batched(n, seed, device):
     sg0 = subs[0]
     rc, _ = sg0.solve(CHECK, target=TARGET, check_every=CHECK)  # warm the library / pool
     t0 = time.perf_counter()
-    plain = []
+    plain, by_kind = [], {}
     for sg in subs:
+        t1 = time.perf_counter()
         rc, r = sg.solve(MAX_ITERS, target=TARGET, check_every=CHECK, device=device)
         if rc != 0:
             raise RuntimeError(f"plain solve failed ({rc}): {wl.ssg.last_error(sg.lib)}")
         plain.append(r["stats"])
+        k = by_kind.setdefault(sg.cfg["name"], {"n": 0, "s": 0.0, "iterations": 0, "max_ms": 0.0})
+        dt = time.perf_counter() - t1
+        k["n"] += 1
+        k["s"] += dt
+        k["iterations"] += r["stats"]["iterations_run"]
+        k["max_ms"] = max(k["max_ms"], dt * 1e3)
     t_plain = time.perf_counter() - t0
     # warm the batched path (its kernels load on first use) as the plain
     # leg was warmed above: one short batch over the first requests
@@ -574,6 +581,10 @@ def run_batched(n, seed, device):
            "iterations_p50": pct(its, 50), "iterations_max": max(its),
            "exploitability_max_pct": max(expl),
            "plain_iterations_p50": pct([p["iterations_run"] for p in plain], 50),
+           # where the plain form's time goes: per request kind, requests,
+           # summed solve seconds, iterations run, slowest solve
+           "plain_by_kind": {k: {"n": v["n"], "s": round(v["s"], 3), "iterations": v["iterations"],
+                                 "max_ms": round(v["max_ms"], 1)} for k, v in sorted(by_kind.items())},
            "mix": C4_MIX}
     out.update(mix)
     return out

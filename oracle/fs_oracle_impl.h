@@ -8,12 +8,17 @@
  * may be NULL): root_strategy [na_root][nh_root] (the last regret-matched
  * strategy at node 0), avg [N][6][max_h] (normalised strategy sums at
  * decision nodes, 0 elsewhere), cfv [N][max_h] (the last traverser's
- * values).  Returns 0, or -1 on bad input.
+ * values); snap_root [n_snap][na_root][nh_root]: the root strategy after
+ * iteration snap_iters[j] (the same read-out as root_strategy, taken on the
+ * way).  Loops over the nodes of one level (and over all nodes where each
+ * writes only its own rows) run on OpenMP threads: no sums cross threads, so
+ * the results do not depend on the thread count.  Returns 0, or -1 on bad
+ * input.
  */
 
 int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int *node_depth, int max_depth,
                     const int *hands, const float *weights, const int *nh, int iterations, REAL *root_strategy,
-                    REAL *avg, REAL *cfv_out)
+                    REAL *avg, REAL *cfv_out, int n_snap, const int *snap_iters, REAL *snap_root)
 {
     const int max_h = nh[0] > nh[1] ? nh[0] : nh[1];
     if (max_h <= 0 || N <= 0) return -1;
@@ -35,6 +40,7 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
     }
     /* strengths per (showdown node, player, hand), :366-399 */
     uint32_t *str = (uint32_t *)calloc((size_t)N * 2 * H, sizeof(uint32_t));
+#pragma omp parallel for schedule(dynamic, 256)
     for (int x = 0; x < N; x++) {
         if (nodes[x].type != 2) continue;
         for (int p = 0; p < 2; p++)
@@ -57,6 +63,7 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
         for (int trav = 0; trav < 2; trav++) {
             const int opp = 1 - trav;
             /* regret matching, :652-684 */
+#pragma omp parallel for schedule(dynamic, 1024)
             for (int x = 0; x < N; x++) {
                 const FsoNode *n = &nodes[x];
                 if (n->type != 0) continue;
@@ -78,6 +85,7 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
             memset(reach, 0, (size_t)N * H * sizeof(REAL));
             for (int h = 0; h < nh[opp]; h++) reach[h] = (REAL)weights[opp * FSO_MAX_HANDS + h];
             for (int d = 0; d <= max_depth; d++)
+#pragma omp parallel for schedule(dynamic, 256)
                 for (int k = lev_off[d]; k < lev_off[d + 1]; k++) {
                     const int x = lev[k];
                     const FsoNode *n = &nodes[x];
@@ -93,6 +101,7 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
                 }
             /* terminal values, :731-833 */
             memset(cfv, 0, (size_t)N * H * sizeof(REAL));
+#pragma omp parallel for schedule(dynamic, 256)
             for (int x = 0; x < N; x++) {
                 const FsoNode *n = &nodes[x];
                 if (n->type != 1 && n->type != 2) continue;
@@ -135,6 +144,7 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
             /* values bottom-up, regrets and strategy sums, :835-892 */
             const REAL disc = (REAL)it / ((REAL)it + FLIT(1.0));
             for (int d = max_depth; d >= 0; d--)
+#pragma omp parallel for schedule(dynamic, 256)
                 for (int k = lev_off[d]; k < lev_off[d + 1]; k++) {
                     const int x = lev[k];
                     const FsoNode *n = &nodes[x];
@@ -159,6 +169,13 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
                     }
                 }
         }
+        for (int j = 0; j < n_snap; j++)
+            if (snap_iters[j] == it) {
+                const int rp = nodes[0].player, na = nodes[0].num_children;
+                REAL *dst = snap_root + (size_t)j * na * nh[rp];
+                for (int a = 0; a < na; a++)
+                    for (int h = 0; h < nh[rp]; h++) dst[(size_t)a * nh[rp] + h] = ST(strategy, 0, a, h);
+            }
     }
     if (root_strategy) {
         const int rp = nodes[0].player, na = nodes[0].num_children;
@@ -168,6 +185,7 @@ int FSUF(fso_solve)(const FsoNode *nodes, const int *children, int N, const int 
     if (avg) {
         /* :1516-1540 */
         memset(avg, 0, (size_t)N * A * H * sizeof(REAL));
+#pragma omp parallel for schedule(dynamic, 1024)
         for (int x = 0; x < N; x++) {
             const FsoNode *n = &nodes[x];
             if (n->type != 0) continue;

@@ -490,10 +490,12 @@ class FlopOracle:
         for f in ("fso_solve_f32", "fso_solve_f64"):
             getattr(self.lib, f).restype = ctypes.c_int
 
-    def solve(self, nodes, children, node_depth, max_depth, hands, weights, nh, iterations, precision="f32"):
+    def solve(self, nodes, children, node_depth, max_depth, hands, weights, nh, iterations, precision="f32",
+              snapshots=(), full=True):
         """nodes [N, 13] int32 (FSNode fields), hands [2][200][2], weights
         [2][200]; returns root_strategy, all_avg_strategies [N][6][max_h] and
-        all_cfv [N][max_h]."""
+        all_cfv [N][max_h] (None without `full`), and root_snapshots {k: the
+        root strategy after iteration k} for each k in `snapshots`."""
         nodes = np.ascontiguousarray(nodes, np.int32)
         children = np.ascontiguousarray(children, np.int32)
         nd = np.ascontiguousarray(node_depth, np.int32)
@@ -506,12 +508,19 @@ class FlopOracle:
         ptr = _f32p if precision == "f32" else _f64p
         rp, na = int(nodes[0, 1]), int(nodes[0, 2])
         rs = np.zeros(max(na * int(nh[rp]), 1), dt)
-        avg = np.zeros(N * 6 * mh, dt)
-        cfv = np.zeros(N * mh, dt)
+        avg = np.zeros(N * 6 * mh, dt) if full else None
+        cfv = np.zeros(N * mh, dt) if full else None
+        snaps = np.ascontiguousarray([int(k) for k in snapshots] or [0], np.int32)
+        sr = np.zeros(max(len(snapshots), 1) * max(na * int(nh[rp]), 1), dt)
         fn = self.lib.fso_solve_f32 if precision == "f32" else self.lib.fso_solve_f64
         rc = fn(_i32p(nodes), _i32p(children), N, _i32p(nd), int(max_depth), _i32p(hands), _f32p(weights),
-                _i32p(nh), int(iterations), ptr(rs), ptr(avg), ptr(cfv))
+                _i32p(nh), int(iterations), ptr(rs), ptr(avg) if full else None, ptr(cfv) if full else None,
+                len(snapshots), _i32p(snaps), ptr(sr))
         if rc != 0:
             raise RuntimeError("fso_solve failed")
-        return {"root_strategy": rs[:na * int(nh[rp])].reshape(na, int(nh[rp])),
-                "all_avg_strategies": avg.reshape(N, 6, mh), "all_cfv": cfv.reshape(N, mh)}
+        k = na * int(nh[rp])
+        return {"root_strategy": rs[:k].reshape(na, int(nh[rp])),
+                "all_avg_strategies": avg.reshape(N, 6, mh) if full else None,
+                "all_cfv": cfv.reshape(N, mh) if full else None,
+                "root_snapshots": {int(s_): sr[j * k:(j + 1) * k].reshape(na, int(nh[rp]))
+                                   for j, s_ in enumerate(snapshots)}}
