@@ -121,6 +121,32 @@ SSB_CR3_HD void phase_product(int tid, int nt, const Tables &t) {
     }
 }
 
+// phase 3, tiled: the same P and PT, 4 x 4 cells per item (13 x 13 items):
+// A is symmetric, so row c of A is its column c, and each cell still sums
+// over c = 0 .. kS-1 in order (the same value as phase_product), with a
+// quarter of the table reads
+SSB_CR3_HD void phase_product_tiled(int tid, int nt, const Tables &t) {
+    constexpr int kT = kS / 4;
+    for (int q = tid; q < kT * kT; q += nt) {
+        const int e0 = (q / kT) * 4, f0 = (q % kT) * 4;
+        double acc[4][4] = {};
+        for (int c = 0; c < kS; ++c) {
+            double xs[4], ys[4];
+            for (int i = 0; i < 4; ++i) {
+                xs[i] = t.A[c * kS + e0 + i];
+                ys[i] = t.B[c * kS + f0 + i];
+            }
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j) acc[i][j] += xs[i] * ys[j];
+        }
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                t.P[(e0 + i) * kS + f0 + j] = acc[i][j];
+                t.PT[(f0 + j) * kS + e0 + i] = acc[i][j];
+            }
+    }
+}
+
 // phase 4: per card w and d, and on item kS the third opponent's compacted
 // list (in hand order) -- done by one item, so its order is fixed
 template <class T>
@@ -157,6 +183,26 @@ SSB_CR3_HD void phase_vectors(int tid, int nt, const Opp3<T> &in, const Tables &
     }
 }
 
+// the third opponent's compacted positive-reach list in hand order (the
+// kS item of phase_vectors, on its own)
+template <class T>
+SSB_CR3_HD void compact_third_list(const Opp3<T> &in, const Tables &t) {
+    long long n = 0;
+    double f3 = 0.0;
+    for (int h = 0; h < in.H3; ++h) {
+        const int code = in.code3[h];
+        if (code & 0x10000) continue;   // touches the board
+        const T r = in.r3[h];
+        if (!(r > T(0))) continue;
+        t.r3[n] = static_cast<double>(r);
+        f3 += t.r3[n];
+        t.xy[n] = static_cast<unsigned short>(((code >> 20) & 63) | (((code >> 26) & 63) << 8));
+        ++n;
+    }
+    t.isc[4] = n;
+    t.sc[4] = f3;
+}
+
 // phase 5 (one item): the scalars
 SSB_CR3_HD void phase_scalars(int tid, const Tables &t) {
     if (tid != 0) return;
@@ -181,6 +227,111 @@ SSB_CR3_HD void phase_scalars(int tid, const Tables &t) {
     t.isc[2] = iq;
     t.isc[3] = ie / 2;
 }
+
+#if defined(__CUDACC__)
+// Device form of phases 2-5 for a block of 256 threads, in two barrier-
+// separated steps after the gather (3 barriers per table build instead of 5):
+//   step 1: per card u, masks and counts, four lanes per card (13 cells each,
+//           partial sums combined by shuffles in a fixed order), beside the
+//           tiled product;
+//   step 2: per card w, d and their counts, four lanes per card, and the
+//           block scalars by the last warp (one lane per card pair of slots,
+//           shuffle sums in a fixed order).
+// The integer parts are exact; the FP64 sums differ from the one-item phases
+// only in summation order.
+__device__ __forceinline__ double quad_sum(double v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v + __shfl_xor_sync(0xffffffffu, v, 2);
+}
+__device__ __forceinline__ void build_step1(int tid, const Tables &t) {
+    if (tid < 224) {   // warps 0-6: cards tid / 4 < kS (lanes of cards 52-55 add zeros)
+        const int c = tid >> 2, part = tid & 3;
+        double sa = 0.0, sb = 0.0;
+        unsigned long long ma = 0ull, mb = 0ull;
+        if (c < kS)
+            for (int e = part * 13; e < part * 13 + 13; ++e) {
+                const double a = t.A[c * kS + e], b = t.B[c * kS + e];
+                sa += a;
+                sb += b;
+                if (a > 0.0) ma |= 1ull << e;
+                if (b > 0.0) mb |= 1ull << e;
+            }
+        sa = quad_sum(sa);
+        sb = quad_sum(sb);
+        ma |= __shfl_xor_sync(0xffffffffu, ma, 1);
+        ma |= __shfl_xor_sync(0xffffffffu, ma, 2);
+        mb |= __shfl_xor_sync(0xffffffffu, mb, 1);
+        mb |= __shfl_xor_sync(0xffffffffu, mb, 2);
+        if (part == 0 && c < kS) {
+            t.uA[c] = sa;
+            t.uB[c] = sb;
+            t.mA[c] = ma;
+            t.mB[c] = mb;
+            t.iuA[c] = __popcll(ma);
+            t.iuB[c] = __popcll(mb);
+        }
+    }
+    phase_product_tiled(tid, 256, t);
+}
+__device__ __forceinline__ void build_step2(int tid, const Tables &t) {
+    if (tid < 224) {
+        const int c = tid >> 2, part = tid & 3;
+        double w = 0.0;
+        int iw = 0;
+        if (c < kS) {
+            const unsigned long long mAc = t.mA[c], mBc = t.mB[c];
+            for (int f = part * 13; f < part * 13 + 13; ++f) {
+                w += t.A[c * kS + f] * t.uB[f] + t.B[c * kS + f] * t.uA[f];
+                iw += ((mAc >> f) & 1ull ? t.iuB[f] : 0) + ((mBc >> f) & 1ull ? t.iuA[f] : 0);
+            }
+        }
+        w = quad_sum(w);
+        iw += __shfl_xor_sync(0xffffffffu, iw, 1);
+        iw += __shfl_xor_sync(0xffffffffu, iw, 2);
+        if (part == 0 && c < kS) {
+            t.w[c] = w;
+            t.iw[c] = iw;
+            t.d[c] = t.P[c * kS + c];
+            t.id[c] = __popcll(t.mA[c] & t.mB[c]);
+        }
+    } else {
+        // the scalars from step 1's vectors and P's diagonal
+        const int lane = tid & 31;
+        double fa = 0.0, fb = 0.0, q = 0.0, e = 0.0;
+        long long ifa = 0, ifb = 0, iq = 0, ie = 0;
+        for (int c = lane; c < kS; c += 32) {
+            fa += t.uA[c];
+            fb += t.uB[c];
+            q += t.uA[c] * t.uB[c];
+            e += t.P[c * kS + c];
+            ifa += t.iuA[c];
+            ifb += t.iuB[c];
+            iq += static_cast<long long>(t.iuA[c]) * t.iuB[c];
+            ie += __popcll(t.mA[c] & t.mB[c]);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            fa += __shfl_xor_sync(0xffffffffu, fa, o);
+            fb += __shfl_xor_sync(0xffffffffu, fb, o);
+            q += __shfl_xor_sync(0xffffffffu, q, o);
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            ifa += __shfl_xor_sync(0xffffffffu, ifa, o);
+            ifb += __shfl_xor_sync(0xffffffffu, ifb, o);
+            iq += __shfl_xor_sync(0xffffffffu, iq, o);
+            ie += __shfl_xor_sync(0xffffffffu, ie, o);
+        }
+        if (lane == 0) {
+            t.sc[0] = 0.5 * fa;
+            t.sc[1] = 0.5 * fb;
+            t.sc[2] = q;
+            t.sc[3] = 0.5 * e;
+            t.isc[0] = ifa / 2;
+            t.isc[1] = ifb / 2;
+            t.isc[2] = iq;
+            t.isc[3] = ie / 2;
+        }
+    }
+}
+#endif
 
 // The traverser's part of every sum in D2(S), S = {a, b} + {x, y}: computed
 // once per hand, reused for every third-opponent hand (x, y).

@@ -243,6 +243,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     const size_t o_sdl = b.add(P.sd_card_list);
     const size_t o_sdp = b.add(P.sd_card_partner);
     const size_t o_ph = b.add(P.pos_hand);
+    const size_t o_pp = b.add(P.pos_prefix);
     const size_t o_seg = b.add(P.sd_seg);
     const size_t o_chunk = b.add(P.sd_chunk);
     std::vector<int> dfe, dna, dpl;
@@ -311,6 +312,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     c.sd_card_list = reinterpret_cast<const short *>(dbase + o_sdl);
     c.sd_card_partner = reinterpret_cast<const short *>(dbase + o_sdp);
     c.pos_hand = reinterpret_cast<const int *>(dbase + o_ph);
+    c.pos_prefix = reinterpret_cast<const int *>(dbase + o_pp);
     c.sd_seg = reinterpret_cast<const int *>(dbase + o_seg);
     c.sd_chunk = reinterpret_cast<const int *>(dbase + o_chunk);
     for (int p = 0; p <= SS_MAX_PLAYERS; ++p) c.sd_seg_off[p] = P.sd_seg_off[p];

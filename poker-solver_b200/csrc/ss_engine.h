@@ -236,6 +236,7 @@ struct Plan {
     std::vector<short> sd_card_partner;// [52][52] the other card of each of those combos
     std::vector<int> sd_pos;           // [np][HS], -1 if blocked / padding
     std::vector<int> pos_hand;         // [np][ncomb] hand index at each rank position, -1 if none
+    std::vector<int> pos_prefix;       // [np][ncomb + 1] hands of the player below each rank position
     // per player, the rank axis cut into segments for the three-way showdown
     // sweep: {lo, hi, holds a hand of the player, 0}; a segment is one tie
     // group holding some of the player's hands, or a run of groups holding

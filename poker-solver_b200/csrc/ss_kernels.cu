@@ -1970,15 +1970,13 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     in.HS = HS;
     in.deck = c.deck;
     const int tid = threadIdx.x;
+    static_assert(kTermThreads == 256, "the device build steps assume 256 threads");
     cr3::phase_gather(tid, kTermThreads, in, t);
     __syncthreads();
-    cr3::phase_rows(tid, kTermThreads, t);
+    cr3::build_step1(tid, t);
+    if (tid == kTermThreads - 1) cr3::compact_third_list(in, t);
     __syncthreads();
-    cr3::phase_product(tid, kTermThreads, t);
-    __syncthreads();
-    cr3::phase_vectors(tid, kTermThreads, in, t);
-    __syncthreads();
-    cr3::phase_scalars(tid, t);
+    cr3::build_step2(tid, t);
     __syncthreads();
     const int h = h0 + tid;
     if (h >= HS) return;
@@ -2077,6 +2075,8 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     in.deck = c.deck;
     const int *posA = c.sd_pos + static_cast<size_t>(o1) * hs;
     const int *posB = c.sd_pos + static_cast<size_t>(o2) * hs;
+    const int *pre1 = c.pos_prefix + static_cast<size_t>(o1) * (nc + 1);
+    const int *pre2 = c.pos_prefix + static_cast<size_t>(o2) * (nc + 1);
     // this thread's rank position and the traverser's hand there
     cr3::Sd3Thread st;
     cr3::sd3_thread_init(q0 + tid, qend, c.pos_hand + static_cast<size_t>(trav) * nc,
@@ -2088,13 +2088,9 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     auto build = [&](int lo1, int hi1, int lo2, int hi2) {
         cr3::phase_gather_cls(tid, kTermThreads, in, t, posA, lo1, hi1, posB, lo2, hi2);
         __syncthreads();
-        cr3::phase_rows(tid, kTermThreads, t);
+        cr3::build_step1(tid, t);
         __syncthreads();
-        cr3::phase_product(tid, kTermThreads, t);
-        __syncthreads();
-        cr3::phase_vectors(tid, kTermThreads, in, t, false);
-        __syncthreads();
-        cr3::phase_scalars(tid, t);
+        cr3::build_step2(tid, t);
         __syncthreads();
     };
     cr3::compact_third(tid, in, t, c.sd_pos + static_cast<size_t>(o3) * hs, p3);
@@ -2141,6 +2137,13 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
             for (int pr = 0; pr < 4; ++pr) {
                 int lo1, hi1, lo2, hi2;
                 cr3::sd3_pair_bounds(pr, lo, hi, &lo1, &hi1, &lo2, &hi2);
+                // an opponent without a hand in its part of the pair: no
+                // tuple, both class masses exactly 0 (what the tables and the
+                // exact count would give), no tables to build
+                if (pre1[hi1] == pre1[lo1] || pre2[hi2] == pre2[lo2]) {
+                    if (mine) st.m[pr][0] = st.m[pr][1] = 0.0;
+                    continue;
+                }
                 build(lo1, hi1, lo2, hi2);
                 const double zb = cr3::zero_bound(t);
                 bool near_zero = false;

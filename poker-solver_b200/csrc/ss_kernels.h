@@ -26,6 +26,7 @@ struct DevCtx {
     const short *sd_card_list;   // [52][52]
     const short *sd_card_partner;// [52][52]
     const int *pos_hand;         // [np][ncomb] hand index at each rank position, -1 if none
+    const int *pos_prefix;       // [np][ncomb + 1] hands of the player below each rank position
     const int *sd_seg;           // three-way showdown sweep segments, 4 ints each
     const int *sd_chunk;         // [np][kSd2Chunks + 1] runs of segments
     int sd_seg_off[SS_MAX_PLAYERS + 1];

@@ -179,6 +179,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     const size_t o_sdl = up(P.sd_card_list.data(), P.sd_card_list.size() * sizeof(short));
     const size_t o_sdp = up(P.sd_card_partner.data(), P.sd_card_partner.size() * sizeof(short));
     const size_t o_ph = up(P.pos_hand.data(), P.pos_hand.size() * sizeof(int));
+    const size_t o_pp = up(P.pos_prefix.data(), P.pos_prefix.size() * sizeof(int));
     const size_t o_seg = up(P.sd_seg.data(), P.sd_seg.size() * sizeof(int));
     const size_t o_chunk = up(P.sd_chunk.data(), P.sd_chunk.size() * sizeof(int));
     const size_t o_dfe = up(dfe.data(), dfe.size() * sizeof(int));
@@ -223,6 +224,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     c.sd_card_list = reinterpret_cast<const short *>(base + o_sdl);
     c.sd_card_partner = reinterpret_cast<const short *>(base + o_sdp);
     c.pos_hand = reinterpret_cast<const int *>(base + o_ph);
+    c.pos_prefix = reinterpret_cast<const int *>(base + o_pp);
     c.sd_seg = reinterpret_cast<const int *>(base + o_seg);
     c.sd_chunk = reinterpret_cast<const int *>(base + o_chunk);
     for (int p = 0; p <= SS_MAX_PLAYERS; ++p) c.sd_seg_off[p] = P.sd_seg_off[p];

@@ -452,6 +452,13 @@ int build_plan(const Problem &pb, Plan *out) {
         for (int p = 0; p < np; ++p)
             for (int h = 0; h < P.H[p]; ++h)
                 if (P.sd_pos[p * HS + h] >= 0) P.pos_hand[static_cast<size_t>(p) * nc + P.sd_pos[p * HS + h]] = h;
+        // per player: how many of its hands sit below each rank position
+        P.pos_prefix.assign(static_cast<size_t>(np) * (nc + 1), 0);
+        for (int p = 0; p < np; ++p)
+            for (int q = 0; q < nc; ++q)
+                P.pos_prefix[static_cast<size_t>(p) * (nc + 1) + q + 1] =
+                    P.pos_prefix[static_cast<size_t>(p) * (nc + 1) + q] +
+                    (P.pos_hand[static_cast<size_t>(p) * nc + q] >= 0 ? 1 : 0);
         P.sd_seg.clear();
         for (int p = 0; p < np; ++p) {
             P.sd_seg_off[p] = static_cast<int>(P.sd_seg.size() / 4);

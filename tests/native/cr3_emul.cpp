@@ -77,7 +77,7 @@ int main(int argc, char **argv) {
     const int nt = 256;
     for (int tid = 0; tid < nt; ++tid) phase_gather(tid, nt, in, t);
     for (int tid = 0; tid < nt; ++tid) phase_rows(tid, nt, t);
-    for (int tid = 0; tid < nt; ++tid) phase_product(tid, nt, t);
+    for (int tid = 0; tid < nt; ++tid) phase_product_tiled(tid, nt, t);
     for (int tid = 0; tid < nt; ++tid) phase_vectors(tid, nt, in, t);
     for (int tid = 0; tid < nt; ++tid) phase_scalars(tid, t);
     const double zb = zero_bound(t);

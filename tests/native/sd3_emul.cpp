@@ -78,7 +78,7 @@ int main(int argc, char **argv) {
     auto build = [&](int lo1, int hi1, int lo2, int hi2) {
         for (int tid = 0; tid < nt; ++tid) phase_gather_cls(tid, nt, in, t, pos[0].data(), lo1, hi1, pos[1].data(), lo2, hi2);
         for (int tid = 0; tid < nt; ++tid) phase_rows(tid, nt, t);
-        for (int tid = 0; tid < nt; ++tid) phase_product(tid, nt, t);
+        for (int tid = 0; tid < nt; ++tid) phase_product_tiled(tid, nt, t);
         for (int tid = 0; tid < nt; ++tid) phase_vectors(tid, nt, in, t, false);
         for (int tid = 0; tid < nt; ++tid) phase_scalars(tid, t);
     };
