@@ -619,12 +619,13 @@ def run_served(rates, n, seed, device):
 
         th = threading.Thread(target=feeder)
         th.start()
-        lat, its, nhu = [], [], []
+        lat, queue, its, nhu = [], [], [], []
         for i, sg in enumerate(subs):
             while ids[i] is None:
                 time.sleep(0.0005)
             r = srv.wait(ids[i], sg.nh)
             lat.append(r["latency_ms"])
+            queue.append(r["stats"]["queue_ms"])
             its.append(r["stats"]["iterations_run"])
             nhu.append(float(sg.td.num_nodes) * float(sum(sg.nh)) * r["stats"]["iterations_run"])
         th.join()
@@ -633,6 +634,12 @@ def run_served(rates, n, seed, device):
         per_rate.append({"rate_per_s": rate, "requests": n, "arrivals_s": float(gaps.sum()),
                          "solves_per_s": n / wall, "node_hand_updates_per_s": sum(nhu) / wall,
                          "latency_p50_ms": pct(lat, 50), "latency_p99_ms": pct(lat, 99),
+                         # latency = queueing (submission until the request joins
+                         # the running batch) + time in the batch
+                         "queue_p50_ms": pct(queue, 50), "queue_p99_ms": pct(queue, 99),
+                         "in_batch_p50_ms": pct([a - b for a, b in zip(lat, queue)], 50),
+                         "in_batch_p99_ms": pct([a - b for a, b in zip(lat, queue)], 99),
+                         "offered_over_served": rate / (n / wall),
                          "iterations_p50": pct(its, 50)})
     service = []
     for sg in subs[:min(n, 64)]:

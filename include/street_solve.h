@@ -151,6 +151,8 @@ typedef struct {
     double nashconv;              /* sum over players of best-response gain per unit of deal mass */
     double solve_ms;              /* device time of the CFR iterations */
     double node_hand_updates;     /* num_nodes x sum of hand counts x iterations */
+    double queue_ms;              /* served form: submission until the request joined the running batch
+                                     (admission and session build included); 0 for the other forms */
 } SSSolveStats;
 
 /* Served form: continuous batching of solve requests on one GPU. */

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstddef>
 #include <condition_variable>
 #include <deque>
@@ -687,7 +688,7 @@ struct Request {
     std::vector<int> frozen;
     Problem pb;
     size_t bytes = 0;
-    std::chrono::steady_clock::time_point t_submit, t_done;
+    std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
     int slot = -1;
     int iters_done = 0;  // iterations run so far (updated after each block)
     int state = 0;  // 0 pending, 1 running, 2 done, <0 failed with that code
@@ -852,6 +853,13 @@ class Server {
     }
 
   private:
+    // whether the device context still works after a failed call (a sticky
+    // error, such as an illegal address, ends every request)
+    static bool context_usable() {
+        cudaGetLastError();   // clears a non-sticky error of the last call
+        return cudaDeviceSynchronize() == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    }
+
     void fail(Request *r, int rc, const std::string &msg) {
         r->state = rc;
         r->error = msg;
@@ -935,12 +943,33 @@ class Server {
                 }
                 r->slot = slot;
                 r->state = 1;
+                r->t_admit = std::chrono::steady_clock::now();
                 if (static_cast<int>(slot_req.size()) <= slot) slot_req.resize(slot + 1, nullptr);
                 slot_req[slot] = r;
             }
             if (batch.num_active() == 0) continue;
             int rc = batch.run(block);
             if (rc == SS_OK) rc = batch.check(pct, nash);
+            if (rc != SS_OK && !add.empty() && context_usable()) {
+                // a failure that left the context usable (an allocation or a
+                // graph build for the members added this round): those members
+                // leave with the error, the rest of the batch carries on
+                const std::string msg = last_error();
+                for (auto &rs : add) {
+                    Request *r = rs.first;
+                    if (r->slot < 0 || r->state != 1) continue;
+                    batch.retire(r->slot);
+                    batch.release(r->slot);
+                    std::lock_guard<std::mutex> lk(mu);
+                    used -= r->bytes;
+                    slot_req[r->slot] = nullptr;
+                    fail(r, rc, msg);
+                }
+                std::lock_guard<std::mutex> lk(mu);
+                cv_done.notify_all();
+                cv_admit.notify_all();
+                continue;
+            }
             if (rc != SS_OK) {
                 std::lock_guard<std::mutex> lk(mu);
                 fatal = rc;
@@ -960,6 +989,22 @@ class Server {
                 if (!batch.active[i]) continue;
                 Request *r = slot_req[i];
                 const bool cap = batch.iters_run[i] >= opt.max_iterations;
+                if (!std::isfinite(pct[i])) {
+                    // non-finite values (a caller's NaN or infinite leaf value
+                    // spreads through the regrets): this request fails, the
+                    // others never read its rows
+                    batch.retire(static_cast<int>(i));
+                    batch.release(static_cast<int>(i));
+                    std::lock_guard<std::mutex> lk(mu);
+                    used -= r->bytes;
+                    fail(r, SS_ERR_INVALID,
+                         "non-finite exploitability after " + std::to_string(batch.iters_run[i]) +
+                             " iterations: the subgame's inputs (leaf values, weights) hold NaN or infinity");
+                    slot_req[i] = nullptr;
+                    cv_done.notify_all();
+                    cv_admit.notify_all();
+                    continue;
+                }
                 if (!(cap || pct[i] <= opt.target_exploitability)) continue;
                 rc = batch.retire(static_cast<int>(i));
                 SSOutput o{};
@@ -977,6 +1022,7 @@ class Server {
                     r->stats.exploitability_pct = pct[i];
                     r->stats.nashconv = nash[i];
                     r->stats.node_hand_updates = nhu;
+                    r->stats.queue_ms = std::chrono::duration<double, std::milli>(r->t_admit - r->t_submit).count();
                     r->t_done = std::chrono::steady_clock::now();
                     r->state = 2;
                 }

@@ -92,7 +92,7 @@ class SSSolveOptions(ctypes.Structure):
 class SSSolveStats(ctypes.Structure):
     _fields_ = [("iterations_run", ctypes.c_int), ("exploitability_pct", ctypes.c_double),
                 ("nashconv", ctypes.c_double), ("solve_ms", ctypes.c_double),
-                ("node_hand_updates", ctypes.c_double)]
+                ("node_hand_updates", ctypes.c_double), ("queue_ms", ctypes.c_double)]
 
 
 def tree_struct(max_hands=SS_MAX_HANDS):

@@ -162,3 +162,36 @@ def test_server_memory_budget_queues_requests():
     assert all(r["stats"]["iterations_run"] > 0 for r in res)
     for sg in subs:
         sg.free()
+
+
+@pytest.mark.gpu
+def test_server_failure_retires_only_that_request():
+    """A request whose leaf values hold NaN fails with its own error (its
+    exploitability is not finite) while the requests batched with it finish
+    with their solo results."""
+    subs = mixed_subgames()
+    good = [subs[2], subs[6]]
+    lib = good[0].lib
+    cfg = wl.config("turn3", seed=48, num_hands=12, bet_sizes=[0.75], max_raises=2)
+    bad = wl.AbiSubgame(cfg, max_hands=200)
+    lv = wl.leaf_values_for(cfg, bad.num_leaves)
+    lv[:, :, 3] = np.nan
+    bad.set_leaf_values(lv)
+    kw = dict(block_iterations=25, target_exploitability=2.0, max_iterations=300)
+    alone = []
+    for sg in good:
+        srv = wl.Server(lib, **kw)
+        alone.append(srv.wait(srv.submit(sg), sg.nh))
+        srv.close()
+    srv = wl.Server(lib, **kw)
+    ids = [srv.submit(good[0]), srv.submit(bad), srv.submit(good[1])]
+    first = srv.wait(ids[0], good[0].nh)
+    with pytest.raises(RuntimeError, match="non-finite"):
+        srv.wait(ids[1], bad.nh)
+    last = srv.wait(ids[2], good[1].nh)
+    srv.close()
+    for a, m in zip(alone, (first, last)):
+        identical(a, m)
+        assert a["stats"]["iterations_run"] == m["stats"]["iterations_run"]
+    for sg in subs + [bad]:
+        sg.free()
