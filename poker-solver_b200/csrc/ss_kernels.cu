@@ -14,6 +14,7 @@
 // instead (street_solve.cu:704-1130), which is O(H^k).
 #include "ss_kernels.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include "ss_cr3.cuh"
 
@@ -134,9 +135,9 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
 // warps of a block take four hand chunks and walk whole frontiers.  S > 1
 // (items with long frontiers, which are few): the S warps of a block share
 // one hand chunk and each sums every S-th frontier row; warp 0 adds the S
-// partial sums in a fixed order and updates.  Frontier row indices are read
-// 32 at a time (one per lane, handed out by shuffles), row values 8 at a
-// time, so a walk costs one dependent round trip per 8 rows.
+// partial sums in a fixed order and updates.  In the split form frontier row
+// indices are read 32 at a time (one per lane, handed out by shuffles), row
+// values 8 at a time, so a walk costs one dependent round trip per 8 rows.
 // --------------------------------------------------------------------------
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
@@ -164,6 +165,64 @@ __device__ __forceinline__ CfvView cfv_view(const DevCtx &c, int H) {
 
 // threads per block of the value/regret kernel with S warps per hand chunk
 constexpr int cfv_threads(int S) { return S <= kCfvThreads / 32 ? kCfvThreads : 32 * S; }
+
+// Value, regret and strategy-sum update of one traverser node for the two
+// hands h0, h0 + 1 of this lane, from its edges' values ev (the frontier
+// sums): regret matching from R, v = sum_a sigma_a ev_a,
+// r_a = (r_a + ev_a - v) * t / (t + 1), s_a += t sigma_a, val[node] = v * scale.
+__device__ __forceinline__ void cfv_update(const CfvView &V, const CfvItem &I, int h0,
+                                           const float2 (&ev)[SS_MAX_ACTIONS]) {
+    const size_t HS = static_cast<size_t>(V.HS);
+    // the regrets are read three times (sum, value, update) instead of being
+    // held in registers; the rereads hit L1
+    const float *Rh = V.R + static_cast<size_t>(I.first_edge) * HS + h0;
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+        if (a < I.na) {
+            const float2 r = ld2_l1(Rh + a * HS);
+            s0 += r.x > 0.f ? r.x : 0.f;
+            s1 += r.y > 0.f ? r.y : 0.f;
+        }
+    }
+    const float uni = 1.0f / static_cast<float>(I.na);
+    const float inv0 = s0 > 0.f ? 1.0f / s0 : 0.f, inv1 = s1 > 0.f ? 1.0f / s1 : 0.f;
+    // strategy of action a (regret matching, A3 freeze)
+    auto sigma = [&](int a, float ra, float sum, float inv) {
+        if (I.frozen >= 0) return a == I.frozen ? 1.0f : 0.0f;
+        return sum > 0.f ? (ra > 0.f ? ra : 0.f) * inv : uni;
+    };
+    float v0 = 0.f, v1 = 0.f;
+#pragma unroll
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+        if (a < I.na) {
+            const float2 r = ld2_l1(Rh + a * HS);
+            v0 += sigma(a, r.x, s0, inv0) * ev[a].x;
+            v1 += sigma(a, r.y, s1, inv1) * ev[a].y;
+        }
+    }
+    const int t = *V.iter;
+    const float d = static_cast<float>(t) / (static_cast<float>(t) + 1.0f);
+    const float w = static_cast<float>(t);
+#pragma unroll
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+        if (a < I.na) {
+            const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
+            const float2 r = ld2_l1(Rh + a * HS);
+            const float2 sm = ld2(V.S + off);
+            float2 nr, ns;
+            nr.x = (r.x + (ev[a].x - v0)) * d;
+            nr.y = (r.y + (ev[a].y - v1)) * d;
+            ns.x = sm.x + w * sigma(a, r.x, s0, inv0);
+            ns.y = sm.y + w * sigma(a, r.y, s1, inv1);
+            st2(V.R + off, nr);
+            st2(V.S + off, ns);
+        }
+    }
+    // scale 1 on a single street (exact: the row equals v); below chance
+    // nodes the row carries their 1 / cards weights for the parent's frontier
+    st2(V.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0 * I.scale, v1 * I.scale));
+}
 
 template <int S>
 __global__ void __launch_bounds__(cfv_threads(S), S > kCfvThreads / 32 ? 2 : 8)
@@ -207,27 +266,21 @@ __global__ void __launch_bounds__(cfv_threads(S), S > kCfvThreads / 32 ? 2 : 8)
 #pragma unroll
         for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
         const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
-        for (int kb = k0; kb < kend; kb += 32) {
-            const int idx = kb + lane < kend ? __ldg(fr + kb + lane) : 0;
-            const int nrow = min(32, kend - kb);
-            for (int j = 0; j < nrow; j += 8) {
-                float2 x[8];
+        for (int k = k0; k < kend; k += 8) {
+            float2 x[8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int r = __shfl_sync(0xffffffffu, idx, j + i);
-                    x[i] = (j + i < nrow && act) ? ld2(val + static_cast<size_t>(r) * HS) : make_float2(0.f, 0.f);
-                }
+            for (int i = 0; i < 8; ++i)
+                x[i] = (k + i < kend && act) ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS)
+                                             : make_float2(0.f, 0.f);
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int k = kb + j + i;
-                    if (j + i < nrow) {
-                        int e = 0;
+            for (int i = 0; i < 8; ++i) {
+                if (k + i < kend) {
+                    int e = 0;
 #pragma unroll
-                        for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k >= bnd[a] ? 1 : 0;
+                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
 #pragma unroll
-                        for (int a = 0; a < SS_MAX_ACTIONS; ++a)
-                            if (e == a) add2(ev[a], x[i]);
-                    }
+                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+                        if (e == a) add2(ev[a], x[i]);
                 }
             }
         }
@@ -279,55 +332,119 @@ __global__ void __launch_bounds__(cfv_threads(S), S > kCfvThreads / 32 ? 2 : 8)
         }
     }
     if (!act) return;
-    // the regrets are read three times (sum, value, update) instead of being
-    // held in registers; the rereads hit L1
-    const float *Rh = V.R + static_cast<size_t>(I.first_edge) * HS + h0;
-    float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-        if (a < I.na) {
-            const float2 r = ld2_l1(Rh + a * HS);
-            s0 += r.x > 0.f ? r.x : 0.f;
-            s1 += r.y > 0.f ? r.y : 0.f;
-        }
+    cfv_update(V, I, h0, ev);
+}
+
+// One value/regret level in one launch (single street).  Block kinds:
+//  0 -- four warps on four 64-hand chunks of a short item, each walking the
+//       item's whole frontier (at most two rounds of eight row loads) and
+//       updating the node;
+//  1 -- four warps on four chunks of one slice of a long item: at most eight
+//       rows of one edge in one round, the sum stored as the slice's partial
+//       row, then a count on the (item, chunk) counter; the warp that brings
+//       the count to the item's slice total adds the partials edge by edge in
+//       slice order (a fixed order whichever warp is last), updates the node
+//       and clears the counter for the next launch.  Nothing waits on another
+//       warp: the last one to arrive does the rest.
+__global__ void __launch_bounds__(kCfvThreads, 6)
+    k_cfv_level(DevCtx c0, const DevCtx *__restrict__ ctxs, const CfvBlock *__restrict__ blocks,
+                const CfvItem *__restrict__ shorts, const CfvLongItem *__restrict__ longs,
+                const CfvSlice *__restrict__ slices, int trav) {
+    const CfvBlock B = blocks[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chunk = B.chunk + warp;
+    const CfvLongItem *L = nullptr;
+    CfvSlice Sl{};
+    CfvItem I;
+    if (B.kind == 0) {
+        I = shorts[B.index];
+    } else {
+        Sl = slices[B.index];
+        L = longs + Sl.item;
+        I = L->it;
     }
-    const float uni = 1.0f / static_cast<float>(I.na);
-    const float inv0 = s0 > 0.f ? 1.0f / s0 : 0.f, inv1 = s1 > 0.f ? 1.0f / s1 : 0.f;
-    // strategy of action a (regret matching, A3 freeze)
-    auto sigma = [&](int a, float ra, float sum, float inv) {
-        if (I.frozen >= 0) return a == I.frozen ? 1.0f : 0.0f;
-        return sum > 0.f ? (ra > 0.f ? ra : 0.f) * inv : uni;
-    };
-    float v0 = 0.f, v1 = 0.f;
+    if (retired(ctxs, I.sg)) return;
+    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
+    const CfvView V = cfv_view(c, c.H[trav]);
+    const int h0 = chunk * 64 + lane * 2;
+    const bool act = h0 < V.H;
+    if (__all_sync(0xffffffffu, !act)) return;   // a chunk past the hands (never counted)
+    const size_t HS = static_cast<size_t>(V.HS);
+    float2 ev[SS_MAX_ACTIONS];
 #pragma unroll
-    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-        if (a < I.na) {
-            const float2 r = ld2_l1(Rh + a * HS);
-            v0 += sigma(a, r.x, s0, inv0) * ev[a].x;
-            v1 += sigma(a, r.y, s1, inv1) * ev[a].y;
-        }
-    }
-    const int t = *V.iter;
-    const float d = static_cast<float>(t) / (static_cast<float>(t) + 1.0f);
-    const float w = static_cast<float>(t);
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) ev[a] = make_float2(0.f, 0.f);
+    if (B.kind == 0) {
+        if (act) {
 #pragma unroll
-    for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-        if (a < I.na) {
-            const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
-            const float2 r = ld2_l1(Rh + a * HS);
-            const float2 sm = ld2(V.S + off);
-            float2 nr, ns;
-            nr.x = (r.x + (ev[a].x - v0)) * d;
-            nr.y = (r.y + (ev[a].y - v1)) * d;
-            ns.x = sm.x + w * sigma(a, r.x, s0, inv0);
-            ns.y = sm.y + w * sigma(a, r.y, s1, inv1);
-            st2(V.R + off, nr);
-            st2(V.S + off, ns);
+            for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+                if (a < I.na) {
+                    const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(V.R + off));
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(V.S + off));
+                }
+            }
         }
+        const float *val = V.val + (act ? h0 : 0);
+        const int fe = I.first_edge;
+        int bnd[SS_MAX_ACTIONS];
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
+        const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
+        for (int k = k0; k < kend; k += 8) {
+            float2 x[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                x[i] = (k + i < kend && act) ? ld2(val + static_cast<size_t>(__ldg(V.fr_items + k + i)) * HS)
+                                             : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (k + i < kend) {
+                    int e = 0;
+#pragma unroll
+                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
+#pragma unroll
+                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+                        if (e == a) add2(ev[a], x[i]);
+                }
+            }
+        }
+    } else {
+        const int nrow = Sl.k1 - Sl.k0;   // 1 .. kCfvSliceRows
+        const int idx = lane < nrow ? __ldg(V.fr_items + Sl.k0 + lane) : 0;
+        float2 e = make_float2(0.f, 0.f);
+        {
+            float2 x[kCfvSliceRows];
+#pragma unroll
+            for (int i = 0; i < kCfvSliceRows; ++i) {
+                const int r = __shfl_sync(0xffffffffu, idx, i);
+                x[i] = (i < nrow && act) ? ld2(V.val + static_cast<size_t>(r) * HS + h0) : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int i = 0; i < kCfvSliceRows; ++i) add2(e, x[i]);
+        }
+        const float *part = c.cfv_part + (act ? h0 : 0);
+        if (act) st2(const_cast<float *>(part) + static_cast<size_t>(L->part_base + Sl.slot) * HS, e);
+        __threadfence();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(c.cfv_cnt + L->cnt_base + chunk, 1) == L->n_slices - 1 ? 1 : 0;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (!last) return;
+        __threadfence();
+        if (act) {
+#pragma unroll
+            for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+                if (a < I.na) {
+                    float2 s = make_float2(0.f, 0.f);
+                    for (int q = L->slot_off[a]; q < L->slot_off[a + 1]; ++q)
+                        add2(s, __ldcg(reinterpret_cast<const float2 *>(part + static_cast<size_t>(L->part_base + q) *
+                                                                                    HS)));
+                    ev[a] = s;
+                }
+            }
+        }
+        if (lane == 0) c.cfv_cnt[L->cnt_base + chunk] = 0;
     }
-    // scale 1 on a single street (exact: the row equals v); below chance
-    // nodes the row carries their 1 / cards weights for the parent's frontier
-    st2(V.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0 * I.scale, v1 * I.scale));
+    if (act) cfv_update(V, I, h0, ev);
 }
 
 // --------------------------------------------------------------------------
@@ -1813,94 +1930,123 @@ __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const D
     }
 }
 
-// Exact enumeration of opponent hand tuples for one (terminal, traverser hand)
-// per thread, with the reference validity rules and payoffs
-// (street_solve.cu:771-823 fold, :936-1002 showdown, :1079-1127 leaf).  Cost
-// is the product of the opponents' range sizes; the planner only routes small
-// cases here.
+// Exact enumeration of opponent hand tuples, with the reference validity
+// rules and payoffs (street_solve.cu:771-823 fold, :936-1002 showdown,
+// :1079-1127 leaf).  One warp per (terminal, traverser hand): the tuple space
+// (the opponents' hands in odometer order, the last opponent fastest) is cut
+// into 32 contiguous runs, one per lane; each lane walks its run with an
+// odometer and adds the positive products in FP64, and the lanes' sums are
+// combined in a fixed order.  A block of 4 warps serves 4 hands; the blocks
+// of a terminal stride over the subgame's hands.  Cost is the product of the
+// opponents' range sizes; the planner only routes small cases here.
+constexpr int kEnumWarps = 4;
 template <class T>
-__global__ void __launch_bounds__(128) k_term_enum(DevCtx c0, const DevCtx *__restrict__ ctxs,
-                                                   const TermItem *__restrict__ items, int nchunk, int trav) {
+__global__ void __launch_bounds__(32 * kEnumWarps) k_term_enum(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                               const TermItem *__restrict__ items, int nchunk,
+                                                               int trav) {
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
-    const int h = ch * blockDim.x + threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const TermItem I = items[it];
     if (retired(ctxs, I.sg)) return;
     const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
-    if (h >= c.HS) return;
     T *out = val_rows<T>(c) + static_cast<size_t>(I.node) * c.HS;
     const T *reach = reach_rows<T>(c);
-    const int Ht = c.H[trav];
-    if (h >= Ht) {
-        out[h] = T(0);
-        return;
-    }
-    const size_t HS = static_cast<size_t>(c.HS);
-    const int hc = c.hand_code[trav * HS + h];
-    const int t0 = hc & 0xff, t1 = (hc >> 8) & 0xff;
+    const int Ht = c.H[trav], HSs = c.HS;
+    const size_t HS = static_cast<size_t>(HSs);
     const int k = I.k;
     const bool sd = I.kind_detail == 2;
-    unsigned hs = 0;
-    if (sd) {
-        hs = c.strength[trav * HS + h];
-        if (hs == 0) {
-            out[h] = T(0);
-            return;
-        }
+    int radix[SS_MAX_PLAYERS - 1] = {1, 1, 1, 1, 1};
+    long long ntup = 1;
+    for (int i = 0; i < k; ++i) {
+        radix[i] = c.H[I.opp_player[i]];
+        ntup *= radix[i];
     }
-    int idx[SS_MAX_PLAYERS - 1] = {0, 0, 0, 0, 0};
-    T total = T(0);
-    const T pot = I.pot, tb = I.bet;
-    for (;;) {
-        int cards[SS_MAX_PLAYERS - 1][2];
-        unsigned os[SS_MAX_PLAYERS - 1];
-        T prod = T(1);
-        bool ok = true;
-        for (int i = 0; i < k && ok; ++i) {
-            const int p = I.opp_player[i], o = idx[i];
-            const int code = c.hand_code[p * HS + o];
-            const int a0 = code & 0xff, a1 = (code >> 8) & 0xff;
-            cards[i][0] = a0;
-            cards[i][1] = a1;
-            if (t0 == a0 || t0 == a1 || t1 == a0 || t1 == a1) { ok = false; break; }
-            if (sd) {
-                os[i] = c.strength[p * HS + o];
-                if (os[i] == 0) { ok = false; break; }
-            } else if (code & 0x10000) {
-                ok = false;
-                break;
+    const long long per = (ntup + 31) / 32;
+    const double tb = static_cast<double>(static_cast<T>(I.bet));
+    for (int hb = ch; hb * kEnumWarps < HSs; hb += nchunk) {
+        const int h = hb * kEnumWarps + warp;
+        if (h >= HSs) break;
+        if (h >= Ht) {
+            if (lane == 0) out[h] = T(0);
+            continue;
+        }
+        const int hc = c.hand_code[trav * HS + h];
+        const int t0 = hc & 0xff, t1 = (hc >> 8) & 0xff;
+        unsigned hs = 0;
+        if (sd) {
+            hs = c.strength[trav * HS + h];
+            if (hs == 0) {
+                if (lane == 0) out[h] = T(0);
+                continue;
             }
-            prod *= reach[static_cast<size_t>(I.opp_row[i]) * HS + o];
-            for (int j = 0; j < i; ++j)
-                if (a0 == cards[j][0] || a0 == cards[j][1] || a1 == cards[j][0] || a1 == cards[j][1]) {
+        }
+        // this lane's run of tuples [q0, q1), its first tuple's digits (an
+        // opponent without hands leaves no tuple at all)
+        const long long q0 = lane * per, q1 = q0 + per < ntup ? q0 + per : ntup;
+        int idx[SS_MAX_PLAYERS - 1] = {0, 0, 0, 0, 0};
+        if (q0 < q1) {
+            long long q = q0;
+            for (int i = k - 1; i >= 0; --i) {
+                idx[i] = static_cast<int>(q % radix[i]);
+                q /= radix[i];
+            }
+        }
+        double total = 0.0;
+        for (long long q = q0; q < q1; ++q) {
+            int cards[SS_MAX_PLAYERS - 1][2];
+            unsigned os[SS_MAX_PLAYERS - 1];
+            T prod = T(1);
+            bool ok = true;
+            for (int i = 0; i < k && ok; ++i) {
+                const int p = I.opp_player[i], o = idx[i];
+                const int code = c.hand_code[p * HS + o];
+                const int a0 = code & 0xff, a1 = (code >> 8) & 0xff;
+                cards[i][0] = a0;
+                cards[i][1] = a1;
+                if (t0 == a0 || t0 == a1 || t1 == a0 || t1 == a1) { ok = false; break; }
+                if (sd) {
+                    os[i] = c.strength[p * HS + o];
+                    if (os[i] == 0) { ok = false; break; }
+                } else if (code & 0x10000) {
                     ok = false;
                     break;
                 }
-        }
-        if (ok && prod > T(0)) {
-            if (!sd) {
-                total += prod;
-            } else {
-                unsigned best = hs;
-                for (int i = 0; i < k; ++i) best = os[i] > best ? os[i] : best;
-                if (hs < best) {
-                    total += prod * (-tb);
+                prod *= reach[static_cast<size_t>(I.opp_row[i]) * HS + o];
+                for (int j = 0; j < i; ++j)
+                    if (a0 == cards[j][0] || a0 == cards[j][1] || a1 == cards[j][0] || a1 == cards[j][1]) {
+                        ok = false;
+                        break;
+                    }
+            }
+            if (ok && prod > T(0)) {
+                if (!sd) {
+                    total += static_cast<double>(prod);
                 } else {
-                    int wins = 1;
-                    for (int i = 0; i < k; ++i) wins += os[i] == best ? 1 : 0;
-                    total += prod * (pot / static_cast<T>(wins) - tb);
+                    unsigned best = hs;
+                    for (int i = 0; i < k; ++i) best = os[i] > best ? os[i] : best;
+                    if (hs < best) {
+                        total += static_cast<double>(prod) * (-tb);
+                    } else {
+                        int wins = 1;
+                        for (int i = 0; i < k; ++i) wins += os[i] == best ? 1 : 0;
+                        // the reference's float payoff pot / winners - bet
+                        const double pay = static_cast<double>(static_cast<T>(I.pot) / static_cast<T>(wins) -
+                                                               static_cast<T>(I.bet));
+                        total += static_cast<double>(prod) * pay;
+                    }
                 }
             }
+            for (int j = k - 1; j >= 0; --j) {
+                if (++idx[j] < radix[j]) break;
+                idx[j] = 0;
+            }
         }
-        int j = k - 1;
-        while (j >= 0) {
-            if (++idx[j] < c.H[I.opp_player[j]]) break;
-            idx[j] = 0;
-            --j;
-        }
-        if (j < 0) break;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+        if (lane == 0)
+            out[h] = sd ? static_cast<T>(total) : static_cast<T>(static_cast<double>(term_factor(c, I, h)) * total);
     }
-    out[h] = sd ? total : static_cast<T>(term_factor(c, I, h)) * total;
 }
 
 // Folds and leaves with three counted opponents (4+ player subgames): the
@@ -2438,14 +2584,17 @@ inline int chunks(int H) { return (H + kHandsPerBlock - 1) / kHandsPerBlock; }
 // The tensor-core form of the two-opponent terminals serves dense decks of
 // at most 48 cards (turn and river boards) without repeated combos; c is the
 // launch's context (for a batch: the largest deck and the OR of every
-// member's repeated-combo flags).  SSB_CR2_TENSOR=0 in the environment keeps
-// the mma.sync form (for comparisons).
+// member's repeated-combo flags).  It is taken only with SSB_CR2_TENSOR=1 in
+// the environment: measured on the 3-player turn it is slower than the
+// mma.sync form (0.70 vs 0.55 ms of two-opponent terminals per iteration) --
+// its operand space (55 KB per block) leaves four blocks per SM instead of
+// five, and a block's time is set by its serial phases, not the product.
 bool tensor_product_serves(const DevCtx &c) {
-    static const bool off = [] {
+    static const bool on = [] {
         const char *v = std::getenv("SSB_CR2_TENSOR");
-        return v && v[0] == '0';
+        return v && v[0] == '1';
     }();
-    if (off || c.deck <= 0 || c.deck > kTcRows) return false;
+    if (!on || c.deck <= 0 || c.deck > kTcRows) return false;
     for (int p = 0; p < SS_MAX_PLAYERS; ++p)
         if (c.dup[p]) return false;
     return true;
@@ -2472,6 +2621,14 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = chunks(H);
     k_reach<<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, H, player);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cfv_level(const DevCtx &c, const CfvBlock *blocks, int nblocks, const CfvItem *shorts,
+                             const CfvLongItem *longs, const CfvSlice *slices, int trav, cudaStream_t s,
+                             const DevCtx *ctxs) {
+    if (nblocks <= 0) return cudaSuccess;
+    k_cfv_level<<<nblocks, kCfvThreads, 0, s>>>(c, ctxs, blocks, shorts, longs, slices, trav);
     return cudaGetLastError();
 }
 
@@ -2556,8 +2713,10 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             break;
         }
         case TK_ENUM: {
-            const int nc = (c.HS + 127) / 128;
-            k_term_enum<T><<<n * nc, 128, 0, s>>>(c, ctxs, items, nc, trav);
+            // blocks per terminal: one per 4 hands, at most 16 (they stride
+            // over a larger range; a batch's c.HS is its largest row stride)
+            const int nc = std::min((c.HS + kEnumWarps - 1) / kEnumWarps, 16);
+            k_term_enum<T><<<n * nc, 32 * kEnumWarps, 0, s>>>(c, ctxs, items, nc, trav);
             break;
         }
         case TK_SD3: {
