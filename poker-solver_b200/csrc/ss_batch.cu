@@ -177,10 +177,8 @@ class Batch {
         size_t map_off = 0;
         int map_blocks = 0;
         int map_lg = 0;
+        int n_wide = 0;     // value/regret launches: very long items at the end
         int cr2_form = -1;  // two-opponent terminals: 1 tensor-core form, 0 mma.sync form
-        // value/regret level launches: off holds the blocks, these the short
-        // items, sliced items and slices
-        size_t off_short = 0, off_long = 0, off_slice = 0;
     };
     DevCtx *dctx = nullptr;
     char *dlists = nullptr;
@@ -214,10 +212,8 @@ class Batch {
                 return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
                                     stream, dctx);
             case L_CFV:
-                return launch_cfv_level(cmax, reinterpret_cast<const CfvBlock *>(dlists + L.off), L.n,
-                                        reinterpret_cast<const CfvItem *>(dlists + L.off_short),
-                                        reinterpret_cast<const CfvLongItem *>(dlists + L.off_long),
-                                        reinterpret_cast<const CfvSlice *>(dlists + L.off_slice), L.t, stream, dctx);
+                return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.kind, L.H, stream,
+                                  dctx, L.t, L.n_wide);
             case L_REACH:
                 return launch_reach(cmax, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H, stream,
                                     dctx, L.t);
@@ -368,43 +364,35 @@ class Batch {
             for (int i : act)
                 if (subs[i]->P.np > t) lv = std::max(lv, subs[i]->P.cfv_levels[t].size());
             for (size_t l = 0; l < lv; ++l) {
-                // one level launch over every member's short items, sliced
-                // items and slices (each item keeps its own subgame's form,
-                // so it is summed as in a solo solve; indices are rebased
-                // into the merged lists)
-                std::vector<CfvItem> sh;
-                std::vector<CfvLongItem> lg;
-                std::vector<CfvSlice> sl;
-                std::vector<CfvBlock> bl;
+                // every subgame's short items, then every subgame's long
+                // ones, then every subgame's very long ones (each item keeps
+                // its own subgame's class, so it is summed as in a solo solve)
+                std::vector<CfvItem> items, longs, wides;
+                int H = 0;
                 for (int i : act) {
                     const Plan &P = subs[i]->P;
-                    if (P.np <= t || l >= P.cfv_short[t].size()) continue;
-                    const int bs = static_cast<int>(sh.size()), bg = static_cast<int>(lg.size()),
-                              bsl = static_cast<int>(sl.size());
-                    for (CfvItem it : P.cfv_short[t][l]) {
+                    if (P.np <= t || l >= P.cfv_levels[t].size()) continue;
+                    const auto &v = P.cfv_levels[t][l];
+                    const size_t n_short = v.size() - static_cast<size_t>(P.cfv_nlong[t][l]);
+                    const size_t n_split = v.size() - static_cast<size_t>(P.cfv_nwide[t][l]);
+                    for (size_t j = 0; j < v.size(); ++j) {
+                        CfvItem it = v[j];
                         it.sg = i;
-                        sh.push_back(it);
+                        (j < n_short ? items : j < n_split ? longs : wides).push_back(it);
                     }
-                    for (CfvLongItem L : P.cfv_long[t][l]) {
-                        L.it.sg = i;
-                        lg.push_back(L);
-                    }
-                    for (CfvSlice x : P.cfv_slices[t][l]) {
-                        x.item += bg;
-                        sl.push_back(x);
-                    }
-                    for (CfvBlock B : P.cfv_blocks[t][l]) {
-                        B.index += B.kind == 0 ? bs : bsl;
-                        bl.push_back(B);
-                    }
-                    add_work(i, P.cfv_levels[t][l].size());
+                    add_work(i, v.size());
+                    H = std::max(H, P.H[t]);
                 }
-                if (bl.empty()) continue;
-                Launch L{L_CFV, 0, t, put(bl.data(), bl.size() * sizeof(CfvBlock)), static_cast<int>(bl.size()), 0};
-                L.off_short = put(sh.data(), sh.size() * sizeof(CfvItem));
-                L.off_long = put(lg.data(), lg.size() * sizeof(CfvLongItem));
-                L.off_slice = put(sl.data(), sl.size() * sizeof(CfvSlice));
-                seq.push_back(L);
+                const int n_wide = static_cast<int>(wides.size());
+                const int n_long = static_cast<int>(longs.size()) + n_wide;
+                items.insert(items.end(), longs.begin(), longs.end());
+                items.insert(items.end(), wides.begin(), wides.end());
+                if (!items.empty()) {
+                    Launch L{L_CFV, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
+                             static_cast<int>(items.size()), H};
+                    L.n_wide = n_wide;
+                    seq.push_back(L);
+                }
             }
             lv = 0;
             for (int i : act)

@@ -231,9 +231,10 @@ SSB_CR3_HD void phase_scalars(int tid, const Tables &t) {
 #if defined(__CUDACC__)
 // Device form of phases 2-5 for a block of 256 threads, in two barrier-
 // separated steps after the gather (3 barriers per table build instead of 5):
-//   step 1: per card u, masks and counts, four lanes per card (13 cells each,
+//   step 1: per card u and counts, four lanes per card (13 cells each,
 //           partial sums combined by shuffles in a fixed order), beside the
-//           tiled product;
+//           tiled product, which skips the card indices whose cells of the
+//           tile are zero (sparse ranges; the masks come from the gather);
 //   step 2: per card w, d and their counts, four lanes per card, and the
 //           block scalars by the last warp (one lane per card pair of slots,
 //           shuffle sums in a fixed order).
@@ -243,35 +244,89 @@ __device__ __forceinline__ double quad_sum(double v) {
     v += __shfl_xor_sync(0xffffffffu, v, 1);
     return v + __shfl_xor_sync(0xffffffffu, v, 2);
 }
+// Device gather (phase 1 with or without rank-position bounds): each warp
+// fills whole rows c of A and B (columns 0-31, then 32-51) and takes each
+// row's positive-cell masks from two ballots, so the masks exist before the
+// product.  Cells outside rows / columns 0 .. deck-1 are 0.
+template <class T>
+__device__ __forceinline__ void gather_dev(int tid, const Opp3<T> &in, const Tables &t, const int *pos1, int lo1,
+                                           int hi1, const int *pos2, int lo2, int hi2) {
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int c = warp; c < kS; c += 8) {
+        unsigned long long ma = 0ull, mb = 0ull;
+        for (int half = 0; half < 2; ++half) {
+            const int e = half * 32 + lane;
+            double a = 0.0, b = 0.0;
+            if (e < kS && c < in.deck && e < in.deck) {
+                const int j1 = in.pair1[c * 52 + e], j2 = in.pair2[c * 52 + e];
+                if (j1 < in.HS && (!pos1 || (pos1[j1] >= lo1 && pos1[j1] < hi1))) a = static_cast<double>(in.r1[j1]);
+                if (j2 < in.HS && (!pos2 || (pos2[j2] >= lo2 && pos2[j2] < hi2))) b = static_cast<double>(in.r2[j2]);
+            }
+            if (e < kS) {
+                t.A[c * kS + e] = a;
+                t.B[c * kS + e] = b;
+            }
+            ma |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, a > 0.0)) << (32 * half);
+            mb |= static_cast<unsigned long long>(__ballot_sync(0xffffffffu, b > 0.0)) << (32 * half);
+        }
+        if (lane == 0) {
+            t.mA[c] = ma;
+            t.mB[c] = mb;
+        }
+    }
+}
+
+// the tiled product skipping card indices c whose four A cells (rows e0..,
+// column c: A is symmetric) or four B cells are all zero: their terms are
+// exact +0, so every cell keeps phase_product's value
+__device__ __forceinline__ void product_masked(int tid, const Tables &t) {
+    constexpr int kT = kS / 4;
+    if (tid >= kT * kT) return;
+    const int e0 = (tid / kT) * 4, f0 = (tid % kT) * 4;
+    double acc[4][4] = {};
+    for (int c = 0; c < kS; ++c) {
+        if (!((t.mA[c] >> e0) & 0xfull) || !((t.mB[c] >> f0) & 0xfull)) continue;
+        double xs[4], ys[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            xs[i] = t.A[c * kS + e0 + i];
+            ys[i] = t.B[c * kS + f0 + i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += xs[i] * ys[j];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            t.P[(e0 + i) * kS + f0 + j] = acc[i][j];
+            t.PT[(f0 + j) * kS + e0 + i] = acc[i][j];
+        }
+}
+
+// step 1 after gather_dev: per card u and counts (masks from the gather)
+// beside the masked product
 __device__ __forceinline__ void build_step1(int tid, const Tables &t) {
     if (tid < 224) {   // warps 0-6: cards tid / 4 < kS (lanes of cards 52-55 add zeros)
         const int c = tid >> 2, part = tid & 3;
         double sa = 0.0, sb = 0.0;
-        unsigned long long ma = 0ull, mb = 0ull;
         if (c < kS)
             for (int e = part * 13; e < part * 13 + 13; ++e) {
-                const double a = t.A[c * kS + e], b = t.B[c * kS + e];
-                sa += a;
-                sb += b;
-                if (a > 0.0) ma |= 1ull << e;
-                if (b > 0.0) mb |= 1ull << e;
+                sa += t.A[c * kS + e];
+                sb += t.B[c * kS + e];
             }
         sa = quad_sum(sa);
         sb = quad_sum(sb);
-        ma |= __shfl_xor_sync(0xffffffffu, ma, 1);
-        ma |= __shfl_xor_sync(0xffffffffu, ma, 2);
-        mb |= __shfl_xor_sync(0xffffffffu, mb, 1);
-        mb |= __shfl_xor_sync(0xffffffffu, mb, 2);
         if (part == 0 && c < kS) {
             t.uA[c] = sa;
             t.uB[c] = sb;
-            t.mA[c] = ma;
-            t.mB[c] = mb;
-            t.iuA[c] = __popcll(ma);
-            t.iuB[c] = __popcll(mb);
+            t.iuA[c] = __popcll(t.mA[c]);
+            t.iuB[c] = __popcll(t.mB[c]);
         }
     }
-    phase_product_tiled(tid, 256, t);
+    product_masked(tid, t);
 }
 __device__ __forceinline__ void build_step2(int tid, const Tables &t) {
     if (tid < 224) {

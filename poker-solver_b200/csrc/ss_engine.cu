@@ -196,7 +196,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     // ---- static tables and the minimum bytes of every launch ------------
     Blob b;
     size_t o_reach[SS_MAX_PLAYERS], o_cfv[SS_MAX_PLAYERS], o_term[SS_MAX_PLAYERS][TK_COUNT],
-        o_rootfr[SS_MAX_PLAYERS], o_cfvl[SS_MAX_PLAYERS][4];
+        o_rootfr[SS_MAX_PLAYERS];
     for (int p = 0; p < np; ++p) {
         std::vector<ReachItem> all;
         for (auto &lv : P.reach_levels[p]) {
@@ -219,25 +219,6 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
             call.insert(call.end(), lv.begin(), lv.end());
         }
         o_cfv[p] = b.add(call);
-        {
-            std::vector<CfvItem> sh;
-            std::vector<CfvLongItem> lg;
-            std::vector<CfvSlice> sl;
-            std::vector<CfvBlock> bl;
-            for (size_t l = 0; l < P.cfv_short[p].size(); ++l) {
-                cfvl_off[p].push_back({static_cast<int>(sh.size()), static_cast<int>(lg.size()),
-                                       static_cast<int>(sl.size()), static_cast<int>(bl.size()),
-                                       static_cast<int>(P.cfv_blocks[p][l].size())});
-                sh.insert(sh.end(), P.cfv_short[p][l].begin(), P.cfv_short[p][l].end());
-                lg.insert(lg.end(), P.cfv_long[p][l].begin(), P.cfv_long[p][l].end());
-                sl.insert(sl.end(), P.cfv_slices[p][l].begin(), P.cfv_slices[p][l].end());
-                bl.insert(bl.end(), P.cfv_blocks[p][l].begin(), P.cfv_blocks[p][l].end());
-            }
-            o_cfvl[p][0] = b.add(sh);
-            o_cfvl[p][1] = b.add(lg);
-            o_cfvl[p][2] = b.add(sl);
-            o_cfvl[p][3] = b.add(bl);
-        }
         for (int k = 0; k < TK_COUNT; ++k) {
             double by = 0;
             for (auto &it : P.term[p][k]) {
@@ -279,10 +260,6 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     for (int p = 0; p < np; ++p) {
         reach_items[p] = reinterpret_cast<const ReachItem *>(dbase + o_reach[p]);
         cfv_items[p] = reinterpret_cast<const CfvItem *>(dbase + o_cfv[p]);
-        cfvl_short[p] = reinterpret_cast<const CfvItem *>(dbase + o_cfvl[p][0]);
-        cfvl_long[p] = reinterpret_cast<const CfvLongItem *>(dbase + o_cfvl[p][1]);
-        cfvl_slice[p] = reinterpret_cast<const CfvSlice *>(dbase + o_cfvl[p][2]);
-        cfvl_block[p] = reinterpret_cast<const CfvBlock *>(dbase + o_cfvl[p][3]);
         for (int k = 0; k < TK_COUNT; ++k)
             term_items[p][k] = reinterpret_cast<const TermItem *>(dbase + o_term[p][k]);
         root_fr[p] = reinterpret_cast<const int *>(dbase + o_rootfr[p]);
@@ -319,15 +296,6 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     }
     n_rs = static_cast<size_t>(P.root_na) * P.H[P.root_player];
     CK(cudaMallocAsync(reinterpret_cast<void **>(&dsmall), (n_rs + HS) * sizeof(float), stream));
-    {
-        // partial rows of the sliced value/regret items, then their counters (zero)
-        const size_t part = static_cast<size_t>(P.cfv_part_rows) * HS * sizeof(float);
-        const size_t cnt = static_cast<size_t>(P.cfv_counters) * sizeof(int);
-        CK(cudaMallocAsync(reinterpret_cast<void **>(&dcfv), std::max<size_t>(part + cnt, 256), stream));
-        CK(cudaMemsetAsync(dcfv + part, 0, cnt, stream));
-        c.cfv_part = reinterpret_cast<float *>(dcfv);
-        c.cfv_cnt = reinterpret_cast<int *>(dcfv + part);
-    }
 
     c.R = R;
     c.S = S;

@@ -101,46 +101,10 @@ struct alignas(16) CfvItem {
 
 // A value/regret item whose edges' frontiers hold at least this many rows in
 // total is long: several warps share each of its hand chunks (more warps from
-// the second bound on).  (The grouping of the multi-street solver; the
-// single-street levels use the sliced form below.)
+// the second bound on).
 constexpr int kCfvLongFrontier = 48;
 constexpr int kCfvWideFrontier = 96;
 
-// Single-street value/regret levels run as one launch each (k_cfv_level):
-// an item whose frontier holds at most kCfvShortRows rows is walked by one
-// warp per 64-hand chunk (two dependent rounds of eight row loads at most);
-// a longer one is cut into slices of at most kCfvSliceRows rows of one edge,
-// one warp per (slice, chunk), whose partial sums the last warp of the chunk
-// to finish adds in slice order before it updates the node.  The upper
-// levels hold few items with long frontiers, so their cost is the chain of
-// dependent loads, which the slices keep at one round.
-constexpr int kCfvShortRows = 16;
-constexpr int kCfvSliceRows = 8;
-
-// a sliced item: its node, its slices' partial rows and chunk counters
-struct alignas(16) CfvLongItem {
-    CfvItem it;
-    int part_base;                        // first partial row (rows of HS) in the subgame's partial buffer
-    int cnt_base;                         // first 64-hand-chunk counter in the subgame's counter buffer
-    int n_slices;
-    int pad_ = 0;
-    int slot_off[SS_MAX_ACTIONS + 4];     // slices of edge a: [slot_off[a], slot_off[a + 1])
-};
-// one slice: frontier rows [k0, k1) of one edge of long item `item` (an
-// index into the launch's long-item list), its partial row part_base + slot
-struct alignas(16) CfvSlice {
-    int item;
-    int slot;
-    int k0, k1;
-};
-// one 128-thread block of a level launch: four warps on the 64-hand chunks
-// chunk .. chunk + 3 of a short item (kind 0) or of a slice (kind 1)
-struct alignas(16) CfvBlock {
-    int kind;
-    int index;
-    int chunk;
-    int pad_ = 0;
-};
 
 // Order one level's value/regret items short, long, very long (stable within
 // each class); returns {long and very long, very long} counts.
@@ -254,14 +218,6 @@ struct Plan {
     std::vector<std::vector<CfvItem>> cfv_levels[SS_MAX_PLAYERS];
     std::vector<int> cfv_nlong[SS_MAX_PLAYERS];
     std::vector<int> cfv_nwide[SS_MAX_PLAYERS];
-    // the same levels in the one-launch form: per traverser and level the
-    // short items, the sliced items, their slices and the blocks
-    std::vector<std::vector<CfvItem>> cfv_short[SS_MAX_PLAYERS];
-    std::vector<std::vector<CfvLongItem>> cfv_long[SS_MAX_PLAYERS];
-    std::vector<std::vector<CfvSlice>> cfv_slices[SS_MAX_PLAYERS];
-    std::vector<std::vector<CfvBlock>> cfv_blocks[SS_MAX_PLAYERS];
-    int cfv_part_rows = 0;             // partial rows of all sliced items
-    int cfv_counters = 0;              // chunk counters of all sliced items
     std::vector<int> fr_off;           // [E + 1]
     std::vector<int> fr_items;         // val rows (= node ids)
     std::vector<int> root_fr[SS_MAX_PLAYERS];

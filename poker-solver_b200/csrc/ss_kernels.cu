@@ -335,118 +335,6 @@ __global__ void __launch_bounds__(cfv_threads(S), S > kCfvThreads / 32 ? 2 : 8)
     cfv_update(V, I, h0, ev);
 }
 
-// One value/regret level in one launch (single street).  Block kinds:
-//  0 -- four warps on four 64-hand chunks of a short item, each walking the
-//       item's whole frontier (at most two rounds of eight row loads) and
-//       updating the node;
-//  1 -- four warps on four chunks of one slice of a long item: at most eight
-//       rows of one edge in one round, the sum stored as the slice's partial
-//       row, then a count on the (item, chunk) counter; the warp that brings
-//       the count to the item's slice total adds the partials edge by edge in
-//       slice order (a fixed order whichever warp is last), updates the node
-//       and clears the counter for the next launch.  Nothing waits on another
-//       warp: the last one to arrive does the rest.
-__global__ void __launch_bounds__(kCfvThreads, 6)
-    k_cfv_level(DevCtx c0, const DevCtx *__restrict__ ctxs, const CfvBlock *__restrict__ blocks,
-                const CfvItem *__restrict__ shorts, const CfvLongItem *__restrict__ longs,
-                const CfvSlice *__restrict__ slices, int trav) {
-    const CfvBlock B = blocks[blockIdx.x];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int chunk = B.chunk + warp;
-    const CfvLongItem *L = nullptr;
-    CfvSlice Sl{};
-    CfvItem I;
-    if (B.kind == 0) {
-        I = shorts[B.index];
-    } else {
-        Sl = slices[B.index];
-        L = longs + Sl.item;
-        I = L->it;
-    }
-    if (retired(ctxs, I.sg)) return;
-    const DevCtx &c = ctxs ? ctxs[I.sg] : c0;
-    const CfvView V = cfv_view(c, c.H[trav]);
-    const int h0 = chunk * 64 + lane * 2;
-    const bool act = h0 < V.H;
-    if (__all_sync(0xffffffffu, !act)) return;   // a chunk past the hands (never counted)
-    const size_t HS = static_cast<size_t>(V.HS);
-    float2 ev[SS_MAX_ACTIONS];
-#pragma unroll
-    for (int a = 0; a < SS_MAX_ACTIONS; ++a) ev[a] = make_float2(0.f, 0.f);
-    if (B.kind == 0) {
-        if (act) {
-#pragma unroll
-            for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-                if (a < I.na) {
-                    const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(V.R + off));
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(V.S + off));
-                }
-            }
-        }
-        const float *val = V.val + (act ? h0 : 0);
-        const int fe = I.first_edge;
-        int bnd[SS_MAX_ACTIONS];
-#pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
-        const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
-        for (int k = k0; k < kend; k += 8) {
-            float2 x[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                x[i] = (k + i < kend && act) ? ld2(val + static_cast<size_t>(__ldg(V.fr_items + k + i)) * HS)
-                                             : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (k + i < kend) {
-                    int e = 0;
-#pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
-#pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
-                        if (e == a) add2(ev[a], x[i]);
-                }
-            }
-        }
-    } else {
-        const int nrow = Sl.k1 - Sl.k0;   // 1 .. kCfvSliceRows
-        const int idx = lane < nrow ? __ldg(V.fr_items + Sl.k0 + lane) : 0;
-        float2 e = make_float2(0.f, 0.f);
-        {
-            float2 x[kCfvSliceRows];
-#pragma unroll
-            for (int i = 0; i < kCfvSliceRows; ++i) {
-                const int r = __shfl_sync(0xffffffffu, idx, i);
-                x[i] = (i < nrow && act) ? ld2(V.val + static_cast<size_t>(r) * HS + h0) : make_float2(0.f, 0.f);
-            }
-#pragma unroll
-            for (int i = 0; i < kCfvSliceRows; ++i) add2(e, x[i]);
-        }
-        const float *part = c.cfv_part + (act ? h0 : 0);
-        if (act) st2(const_cast<float *>(part) + static_cast<size_t>(L->part_base + Sl.slot) * HS, e);
-        __threadfence();
-        int last = 0;
-        if (lane == 0) last = atomicAdd(c.cfv_cnt + L->cnt_base + chunk, 1) == L->n_slices - 1 ? 1 : 0;
-        last = __shfl_sync(0xffffffffu, last, 0);
-        if (!last) return;
-        __threadfence();
-        if (act) {
-#pragma unroll
-            for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-                if (a < I.na) {
-                    float2 s = make_float2(0.f, 0.f);
-                    for (int q = L->slot_off[a]; q < L->slot_off[a + 1]; ++q)
-                        add2(s, __ldcg(reinterpret_cast<const float2 *>(part + static_cast<size_t>(L->part_base + q) *
-                                                                                    HS)));
-                    ev[a] = s;
-                }
-            }
-        }
-        if (lane == 0) c.cfv_cnt[L->cnt_base + chunk] = 0;
-    }
-    if (act) cfv_update(V, I, h0, ev);
-}
-
 // --------------------------------------------------------------------------
 // terminals
 // --------------------------------------------------------------------------
@@ -2117,7 +2005,7 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
     in.deck = c.deck;
     const int tid = threadIdx.x;
     static_assert(kTermThreads == 256, "the device build steps assume 256 threads");
-    cr3::phase_gather(tid, kTermThreads, in, t);
+    cr3::gather_dev(tid, in, t, nullptr, 0, 0, nullptr, 0, 0);
     __syncthreads();
     cr3::build_step1(tid, t);
     if (tid == kTermThreads - 1) cr3::compact_third_list(in, t);
@@ -2232,7 +2120,7 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     ghas[tid] = st.h >= 0;
     constexpr int kAll = 1 << 30;
     auto build = [&](int lo1, int hi1, int lo2, int hi2) {
-        cr3::phase_gather_cls(tid, kTermThreads, in, t, posA, lo1, hi1, posB, lo2, hi2);
+        cr3::gather_dev(tid, in, t, posA, lo1, hi1, posB, lo2, hi2);
         __syncthreads();
         cr3::build_step1(tid, t);
         __syncthreads();
@@ -2621,14 +2509,6 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = chunks(H);
     k_reach<<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, H, player);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_cfv_level(const DevCtx &c, const CfvBlock *blocks, int nblocks, const CfvItem *shorts,
-                             const CfvLongItem *longs, const CfvSlice *slices, int trav, cudaStream_t s,
-                             const DevCtx *ctxs) {
-    if (nblocks <= 0) return cudaSuccess;
-    k_cfv_level<<<nblocks, kCfvThreads, 0, s>>>(c, ctxs, blocks, shorts, longs, slices, trav);
     return cudaGetLastError();
 }
 

@@ -52,10 +52,6 @@ struct DevCtx {
     const int *dec_na;
     const int *dec_pl;
     int max_h;
-    // sliced value/regret items: partial rows [cfv_part_rows][HS] and one
-    // counter per (sliced item, 64-hand chunk), zero between launches
-    float *cfv_part;
-    int *cfv_cnt;
 };
 
 // Batched best response: the root sums of one subgame, one block each.
@@ -99,11 +95,6 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
 // chunk, the last n_wide of those (very long frontiers) with kCfvSplitWide.
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
                        const DevCtx *ctxs = nullptr, int trav = -1, int n_wide = 0);
-// One value/regret level in one launch (single street; see CfvBlock): nblocks
-// blocks of kCfvThreads over short items, sliced items and their slices.
-cudaError_t launch_cfv_level(const DevCtx &c, const CfvBlock *blocks, int nblocks, const CfvItem *shorts,
-                             const CfvLongItem *longs, const CfvSlice *slices, int trav, cudaStream_t s,
-                             const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s, const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,

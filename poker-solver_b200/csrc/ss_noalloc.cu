@@ -120,27 +120,16 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     // ---- host images of the tables (same content as a session's) --------
     std::vector<ReachItem> reach_all[SS_MAX_PLAYERS];
     std::vector<std::pair<int, int>> reach_lv[SS_MAX_PLAYERS];
-    // value/regret levels in their one-launch form (as a session runs them)
-    std::vector<CfvItem> cfvl_sh[SS_MAX_PLAYERS];
-    std::vector<CfvLongItem> cfvl_lg[SS_MAX_PLAYERS];
-    std::vector<CfvSlice> cfvl_sl[SS_MAX_PLAYERS];
-    std::vector<CfvBlock> cfvl_bl[SS_MAX_PLAYERS];
-    struct LevelOff {
-        size_t shorts, longs, slices, blocks, nblocks;
-    };
-    std::vector<LevelOff> cfvl_off[SS_MAX_PLAYERS];
+    std::vector<CfvItem> cfv_all[SS_MAX_PLAYERS];
+    std::vector<std::pair<int, int>> cfv_lv[SS_MAX_PLAYERS];
     for (int p = 0; p < np; ++p) {
         for (auto &lv : P.reach_levels[p]) {
             reach_lv[p].push_back({static_cast<int>(reach_all[p].size()), static_cast<int>(lv.size())});
             reach_all[p].insert(reach_all[p].end(), lv.begin(), lv.end());
         }
-        for (size_t l = 0; l < P.cfv_short[p].size(); ++l) {
-            cfvl_off[p].push_back({cfvl_sh[p].size(), cfvl_lg[p].size(), cfvl_sl[p].size(), cfvl_bl[p].size(),
-                                   P.cfv_blocks[p][l].size()});
-            cfvl_sh[p].insert(cfvl_sh[p].end(), P.cfv_short[p][l].begin(), P.cfv_short[p][l].end());
-            cfvl_lg[p].insert(cfvl_lg[p].end(), P.cfv_long[p][l].begin(), P.cfv_long[p][l].end());
-            cfvl_sl[p].insert(cfvl_sl[p].end(), P.cfv_slices[p][l].begin(), P.cfv_slices[p][l].end());
-            cfvl_bl[p].insert(cfvl_bl[p].end(), P.cfv_blocks[p][l].begin(), P.cfv_blocks[p][l].end());
+        for (auto &lv : P.cfv_levels[p]) {
+            cfv_lv[p].push_back({static_cast<int>(cfv_all[p].size()), static_cast<int>(lv.size())});
+            cfv_all[p].insert(cfv_all[p].end(), lv.begin(), lv.end());
         }
     }
     std::vector<int> dfe, dna, dpl;
@@ -170,14 +159,11 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
         uploads.push_back({off, src, bytes});
         return off;
     };
-    size_t o_reach[SS_MAX_PLAYERS], o_cfvl[SS_MAX_PLAYERS][4], o_term[SS_MAX_PLAYERS][TK_COUNT],
+    size_t o_reach[SS_MAX_PLAYERS], o_cfv[SS_MAX_PLAYERS], o_term[SS_MAX_PLAYERS][TK_COUNT],
         o_rootfr[SS_MAX_PLAYERS];
     for (int p = 0; p < np; ++p) {
         o_reach[p] = up(reach_all[p].data(), reach_all[p].size() * sizeof(ReachItem));
-        o_cfvl[p][0] = up(cfvl_sh[p].data(), cfvl_sh[p].size() * sizeof(CfvItem));
-        o_cfvl[p][1] = up(cfvl_lg[p].data(), cfvl_lg[p].size() * sizeof(CfvLongItem));
-        o_cfvl[p][2] = up(cfvl_sl[p].data(), cfvl_sl[p].size() * sizeof(CfvSlice));
-        o_cfvl[p][3] = up(cfvl_bl[p].data(), cfvl_bl[p].size() * sizeof(CfvBlock));
+        o_cfv[p] = up(cfv_all[p].data(), cfv_all[p].size() * sizeof(CfvItem));
         for (int k = 0; k < TK_COUNT; ++k)
             o_term[p][k] = up(P.term[p][k].data(), P.term[p][k].size() * sizeof(TermItem));
         o_rootfr[p] = up(P.root_fr[p].data(), P.root_fr[p].size() * sizeof(int));
@@ -204,8 +190,6 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     const size_t o_state = L.take((2 * nR + nReach + nVal) * sizeof(float));
     const size_t o_weights = o_state + (2 * nR + E * HS) * sizeof(float);  // last np reach rows
     const size_t o_iter = L.take(sizeof(int));
-    const size_t o_cfvpart = L.take(static_cast<size_t>(P.cfv_part_rows) * HS * sizeof(float));
-    const size_t o_cfvcnt = L.take(static_cast<size_t>(P.cfv_counters) * sizeof(int));
     const size_t o_rs = L.take((n_rs + HS) * sizeof(float));
     const size_t o_avg = L.take(n_avg * sizeof(float));
     if (L.used > kArenaBytes) {
@@ -221,7 +205,6 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     NA_CK(cudaMemcpy(base + o_weights, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
     NA_CK(cudaMemset(base + o_weights + np * HS * sizeof(float), 0, nVal * sizeof(float)));
     NA_CK(cudaMemset(base + o_iter, 0, sizeof(int)));
-    NA_CK(cudaMemset(base + o_cfvcnt, 0, static_cast<size_t>(P.cfv_counters) * sizeof(int)));
     NA_CK(cudaMemset(base + o_rs, 0, (n_rs + HS) * sizeof(float)));
 
     DevCtx c{};
@@ -230,8 +213,6 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
     c.S = state + nR;
     c.reach = state + 2 * nR;
     c.val = state + 2 * nR + nReach;
-    c.cfv_part = reinterpret_cast<float *>(base + o_cfvpart);
-    c.cfv_cnt = reinterpret_cast<int *>(base + o_cfvcnt);
     c.fr_off = reinterpret_cast<const int *>(base + o_fr_off);
     c.fr_items = reinterpret_cast<const int *>(base + o_fr_items);
     c.hand_code = reinterpret_cast<const int *>(base + o_code);
@@ -282,12 +263,10 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
             for (int k = 0; k < TK_COUNT; ++k)
                 NA_CK(launch_terms(c, k, reinterpret_cast<const TermItem *>(base + o_term[t][k]),
                                    static_cast<int>(P.term[t][k].size()), t, s0));
-            for (const LevelOff &o : cfvl_off[t])
-                NA_CK(launch_cfv_level(c, reinterpret_cast<const CfvBlock *>(base + o_cfvl[t][3]) + o.blocks,
-                                       static_cast<int>(o.nblocks),
-                                       reinterpret_cast<const CfvItem *>(base + o_cfvl[t][0]) + o.shorts,
-                                       reinterpret_cast<const CfvLongItem *>(base + o_cfvl[t][1]) + o.longs,
-                                       reinterpret_cast<const CfvSlice *>(base + o_cfvl[t][2]) + o.slices, t, s0));
+            for (size_t l = 0; l < cfv_lv[t].size(); ++l)
+                NA_CK(launch_cfv(c, reinterpret_cast<const CfvItem *>(base + o_cfv[t]) + cfv_lv[t][l].first,
+                                 cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t], s0, nullptr, -1,
+                                 P.cfv_nwide[t][l]));
             NA_CK(reach(t));
         }
     }

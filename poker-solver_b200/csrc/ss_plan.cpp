@@ -252,51 +252,6 @@ int build_plan(const Problem &pb, Plan *out) {
             P.cfv_nwide[t][l] = n.second;
         }
     }
-    // the one-launch form of every level (k_cfv_level): short items walked
-    // whole, longer ones cut into slices of one edge's rows; blocks of four
-    // 64-hand chunks of this traverser's hands
-    P.cfv_part_rows = 0;
-    P.cfv_counters = 0;
-    for (int t = 0; t < np; ++t) {
-        const size_t nl = P.cfv_levels[t].size();
-        P.cfv_short[t].assign(nl, {});
-        P.cfv_long[t].assign(nl, {});
-        P.cfv_slices[t].assign(nl, {});
-        P.cfv_blocks[t].assign(nl, {});
-        const int nchunk = (P.H[t] + 63) / 64;
-        for (size_t l = 0; l < nl; ++l) {
-            for (const CfvItem &it : P.cfv_levels[t][l]) {
-                const int fe = it.first_edge;
-                if (P.fr_off[fe + it.na] - P.fr_off[fe] <= kCfvShortRows) {
-                    P.cfv_short[t][l].push_back(it);
-                    continue;
-                }
-                CfvLongItem L{};
-                L.it = it;
-                L.part_base = P.cfv_part_rows;
-                L.cnt_base = P.cfv_counters;
-                const int li = static_cast<int>(P.cfv_long[t][l].size());
-                int slot = 0;
-                for (int a = 0; a < it.na; ++a) {
-                    L.slot_off[a] = slot;
-                    for (int k = P.fr_off[fe + a]; k < P.fr_off[fe + a + 1]; k += kCfvSliceRows)
-                        P.cfv_slices[t][l].push_back(
-                            CfvSlice{li, slot++, k, std::min(k + kCfvSliceRows, P.fr_off[fe + a + 1])});
-                }
-                L.slot_off[it.na] = slot;
-                L.n_slices = slot;
-                P.cfv_part_rows += slot;
-                P.cfv_counters += nchunk;
-                P.cfv_long[t][l].push_back(L);
-            }
-            for (size_t i = 0; i < P.cfv_slices[t][l].size(); ++i)
-                for (int ch = 0; ch < nchunk; ch += 4)
-                    P.cfv_blocks[t][l].push_back(CfvBlock{1, static_cast<int>(i), ch});
-            for (size_t i = 0; i < P.cfv_short[t][l].size(); ++i)
-                for (int ch = 0; ch < nchunk; ch += 4)
-                    P.cfv_blocks[t][l].push_back(CfvBlock{0, static_cast<int>(i), ch});
-        }
-    }
 
     // board and hand tables
     const int nb = nd[0].num_board;

@@ -55,17 +55,6 @@ class Session {
     std::vector<std::pair<int, int>> reach_lv[SS_MAX_PLAYERS];
     const CfvItem *cfv_items[SS_MAX_PLAYERS] = {};
     std::vector<std::pair<int, int>> cfv_lv[SS_MAX_PLAYERS];
-    // the levels' one-launch form: per traverser the concatenated short items,
-    // sliced items, slices and blocks, and per level where each begins
-    struct CfvLevelOff {
-        int shorts, longs, slices, blocks, nblocks;
-    };
-    const CfvItem *cfvl_short[SS_MAX_PLAYERS] = {};
-    const CfvLongItem *cfvl_long[SS_MAX_PLAYERS] = {};
-    const CfvSlice *cfvl_slice[SS_MAX_PLAYERS] = {};
-    const CfvBlock *cfvl_block[SS_MAX_PLAYERS] = {};
-    std::vector<CfvLevelOff> cfvl_off[SS_MAX_PLAYERS];
-    char *dcfv = nullptr;               // partial rows and chunk counters of the sliced items
     const TermItem *term_items[SS_MAX_PLAYERS][TK_COUNT] = {};
     const int *root_fr[SS_MAX_PLAYERS] = {};
     const int *dec_fe = nullptr, *dec_na = nullptr, *dec_pl = nullptr;
@@ -119,7 +108,6 @@ class Session {
             if (diter) cudaFreeAsync(diter, stream);
             if (dbr) cudaFreeAsync(dbr, stream);
             if (dbr_tab) cudaFreeAsync(dbr_tab, stream);
-            if (dcfv) cudaFreeAsync(dcfv, stream);
             if (davg_br) cudaFreeAsync(davg_br, stream);
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
@@ -189,12 +177,11 @@ class Session {
                 if (kinds[i] != main_k) e = cudaStreamWaitEvent(stream, ev_join[kinds[i]], 0);
             if (e != cudaSuccess) return e;
         }
-        for (size_t l = 0; l < cfvl_off[t].size(); ++l) {
-            const CfvLevelOff &o = cfvl_off[t][l];
+        for (size_t l = 0; l < cfv_lv[t].size(); ++l) {
             e = mark(PC_CFV, cfv_bytes[t][l], cfv_lv[t][l].second);
             if (e == cudaSuccess)
-                e = launch_cfv_level(c, cfvl_block[t] + o.blocks, o.nblocks, cfvl_short[t] + o.shorts,
-                                     cfvl_long[t] + o.longs, cfvl_slice[t] + o.slices, t, stream);
+                e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.cfv_nlong[t][l],
+                               P.H[t], stream, nullptr, -1, P.cfv_nwide[t][l]);
             if (e != cudaSuccess) return e;
         }
         return reach(t);

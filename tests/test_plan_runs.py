@@ -8,11 +8,7 @@ tree builder into small drivers (tests/native/):
 * plan_kinds: the terminal routing -- each terminal goes to the closed form
   for its number of counted opponents (folds count every other player,
   showdowns and leaves the live ones), the scatter form for ranges that
-  repeat a combo, and exact enumeration for the rest;
-* plan_levels: the one-launch form of the value/regret levels -- every item
-  once, short or sliced by its frontier length, slices tiling each edge's
-  frontier rows in order, disjoint partial rows and chunk counters, and
-  blocks covering each short item and slice once per four hand chunks."""
+  repeat a combo, and exact enumeration for the rest."""
 import json
 import os
 import shutil
@@ -191,19 +187,3 @@ def check_groups(d):
                     assert nxt[2:] != lead[2:], "a full group ends where its rows end"
                 i += n
 
-
-@pytest.fixture(scope="module")
-def levels_driver(tmp_path_factory):
-    return _compile(tmp_path_factory, "plan_levels")
-
-
-@pytest.mark.parametrize("players,hands,raises", [(3, 1128, 3), (2, 200, 2), (3, 60, 1), (4, 40, 1)])
-def test_value_levels_one_launch_form(levels_driver, players, hands, raises):
-    board = [str(card_to_int(c)) for c in ["2c", "7d", "9h", "Js"]]
-    r = subprocess.run([levels_driver, str(players), str(hands), str(raises)] + board, check=True,
-                       capture_output=True, text=True)
-    out = json.loads(r.stdout)
-    assert out["ok"], out.get("why")
-    assert out["blocks"] > 0
-    if players == 3 and hands == 1128:
-        assert out["long"] > 0 and out["slices"] > out["long"]
