@@ -213,13 +213,10 @@ int build_plan(const FSTreeData &td, FsPlan *out) {
             P.cfv_levels[t][h].push_back(it);
         }
         P.cfv_nlong[t].assign(P.cfv_levels[t].size(), 0);
-        P.cfv_nwide[t].assign(P.cfv_levels[t].size(), 0);
         for (size_t l = 0; l < P.cfv_levels[t].size(); ++l) {
-            const auto n = order_cfv_level(P.cfv_levels[t][l], [&](const CfvItem &it) {
+            P.cfv_nlong[t][l] = order_cfv_level(P.cfv_levels[t][l], [&](const CfvItem &it) {
                 return P.fr_off[it.first_edge + it.na] - P.fr_off[it.first_edge];
             });
-            P.cfv_nlong[t][l] = n.first;
-            P.cfv_nwide[t][l] = n.second;
         }
     }
     // river boards of the showdowns, and the terminal items
@@ -820,7 +817,7 @@ class Solve {
             if (e == cudaSuccess) e = terms(t, c.val, 1);
             for (size_t l = 0; l < cfv_lv[t].size() && e == cudaSuccess; ++l)
                 e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t],
-                               stream, nullptr, -1, P.cfv_nwide[t][l]);
+                               stream);
             if (e == cudaSuccess) e = reach(t);
         }
         return e;

@@ -42,7 +42,6 @@ struct FsPlan {
     std::vector<std::vector<ReachItem>> reach_levels[2];
     std::vector<std::vector<CfvItem>> cfv_levels[2];
     std::vector<int> cfv_nlong[2];
-    std::vector<int> cfv_nwide[2];
     std::vector<int> fr_off, fr_items;
     std::vector<FsTermItem> term[2];   // per traverser: folds, then showdowns
     int nfold[2] = {0, 0};

@@ -177,7 +177,6 @@ class Batch {
         size_t map_off = 0;
         int map_blocks = 0;
         int map_lg = 0;
-        int n_wide = 0;     // value/regret launches: very long items at the end
         int cr2_form = -1;  // two-opponent terminals: 1 tensor-core form, 0 mma.sync form
     };
     DevCtx *dctx = nullptr;
@@ -213,7 +212,7 @@ class Batch {
                                     stream, dctx);
             case L_CFV:
                 return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.kind, L.H, stream,
-                                  dctx, L.t, L.n_wide);
+                                  dctx, L.t);
             case L_REACH:
                 return launch_reach(cmax, reinterpret_cast<const ReachItem *>(dlists + L.off), L.n, L.H, stream,
                                     dctx, L.t);
@@ -364,35 +363,29 @@ class Batch {
             for (int i : act)
                 if (subs[i]->P.np > t) lv = std::max(lv, subs[i]->P.cfv_levels[t].size());
             for (size_t l = 0; l < lv; ++l) {
-                // every subgame's short items, then every subgame's long
-                // ones, then every subgame's very long ones (each item keeps
-                // its own subgame's class, so it is summed as in a solo solve)
-                std::vector<CfvItem> items, longs, wides;
+                // every subgame's short items, then every subgame's long ones
+                // (each item keeps its own subgame's class, so it is summed as
+                // in a solo solve)
+                std::vector<CfvItem> items, longs;
                 int H = 0;
                 for (int i : act) {
                     const Plan &P = subs[i]->P;
                     if (P.np <= t || l >= P.cfv_levels[t].size()) continue;
                     const auto &v = P.cfv_levels[t][l];
                     const size_t n_short = v.size() - static_cast<size_t>(P.cfv_nlong[t][l]);
-                    const size_t n_split = v.size() - static_cast<size_t>(P.cfv_nwide[t][l]);
                     for (size_t j = 0; j < v.size(); ++j) {
                         CfvItem it = v[j];
                         it.sg = i;
-                        (j < n_short ? items : j < n_split ? longs : wides).push_back(it);
+                        (j < n_short ? items : longs).push_back(it);
                     }
                     add_work(i, v.size());
                     H = std::max(H, P.H[t]);
                 }
-                const int n_wide = static_cast<int>(wides.size());
-                const int n_long = static_cast<int>(longs.size()) + n_wide;
+                const int n_long = static_cast<int>(longs.size());
                 items.insert(items.end(), longs.begin(), longs.end());
-                items.insert(items.end(), wides.begin(), wides.end());
-                if (!items.empty()) {
-                    Launch L{L_CFV, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
-                             static_cast<int>(items.size()), H};
-                    L.n_wide = n_wide;
-                    seq.push_back(L);
-                }
+                if (!items.empty())
+                    seq.push_back({L_CFV, n_long, t, put(items.data(), items.size() * sizeof(CfvItem)),
+                                   static_cast<int>(items.size()), H});
             }
             lv = 0;
             for (int i : act)

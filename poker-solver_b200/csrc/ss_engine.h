@@ -100,19 +100,15 @@ struct alignas(16) CfvItem {
 };
 
 // A value/regret item whose edges' frontiers hold at least this many rows in
-// total is long: several warps share each of its hand chunks (more warps from
-// the second bound on).
+// total is long: several warps share each of its hand chunks.
 constexpr int kCfvLongFrontier = 48;
-constexpr int kCfvWideFrontier = 96;
 
-
-// Order one level's value/regret items short, long, very long (stable within
-// each class); returns {long and very long, very long} counts.
+// Order one level's value/regret items short, then long (stable within each
+// class); returns the number of long items.
 template <class Item, class FrontierRows>
-inline std::pair<int, int> order_cfv_level(std::vector<Item> &v, FrontierRows rows) {
+inline int order_cfv_level(std::vector<Item> &v, FrontierRows rows) {
     auto mid = std::stable_partition(v.begin(), v.end(), [&](const Item &it) { return rows(it) < kCfvLongFrontier; });
-    auto wide = std::stable_partition(mid, v.end(), [&](const Item &it) { return rows(it) < kCfvWideFrontier; });
-    return {static_cast<int>(v.end() - mid), static_cast<int>(v.end() - wide)};
+    return static_cast<int>(v.end() - mid);
 }
 
 // A three-way showdown's rank-order sweep is cut into at most this many runs
@@ -213,11 +209,9 @@ struct Plan {
     // per player: reach levels (top-down)
     std::vector<std::vector<ReachItem>> reach_levels[SS_MAX_PLAYERS];
     // per traverser: cfv levels (bottom-up order); within a level the items
-    // with long frontiers come last, cfv_nlong of them, and of those the
-    // items with very long frontiers, cfv_nwide of them
+    // with long frontiers come last, cfv_nlong of them
     std::vector<std::vector<CfvItem>> cfv_levels[SS_MAX_PLAYERS];
     std::vector<int> cfv_nlong[SS_MAX_PLAYERS];
-    std::vector<int> cfv_nwide[SS_MAX_PLAYERS];
     std::vector<int> fr_off;           // [E + 1]
     std::vector<int> fr_items;         // val rows (= node ids)
     std::vector<int> root_fr[SS_MAX_PLAYERS];

@@ -132,12 +132,10 @@ __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx 
 // (street_solve.cu:1155-1175): v = sum_a sigma_a ev_a; r_a = (r_a + (ev_a - v))
 // * t/(t+1); s_a += t * sigma_a; ev_a = sum of val over frontier(edge a).
 // Each lane owns 2 hands, each warp 64 consecutive hands.  S == 1: the four
-// warps of a block take four hand chunks and walk whole frontiers.  S > 1
-// (items with long frontiers, which are few): the S warps of a block share
-// one hand chunk and each sums every S-th frontier row; warp 0 adds the S
-// partial sums in a fixed order and updates.  In the split form frontier row
-// indices are read 32 at a time (one per lane, handed out by shuffles), row
-// values 8 at a time, so a walk costs one dependent round trip per 8 rows.
+// warps of a block take four hand chunks and walk whole frontiers, eight row
+// loads in flight.  S > 1 (items with long frontiers, which are few): the S
+// warps of a block share one hand chunk and each sums every S-th frontier
+// row; warp 0 adds the S partial sums in a fixed order and updates.
 // --------------------------------------------------------------------------
 __device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ void st2(float *p, float2 v) { *reinterpret_cast<float2 *>(p) = v; }
@@ -163,16 +161,111 @@ __device__ __forceinline__ CfvView cfv_view(const DevCtx &c, int H) {
     return CfvView{c.R, c.S, c.val, c.fr_off, c.fr_items, c.iter, c.HS, H};
 }
 
-// threads per block of the value/regret kernel with S warps per hand chunk
-constexpr int cfv_threads(int S) { return S <= kCfvThreads / 32 ? kCfvThreads : 32 * S; }
 
-// Value, regret and strategy-sum update of one traverser node for the two
-// hands h0, h0 + 1 of this lane, from its edges' values ev (the frontier
-// sums): regret matching from R, v = sum_a sigma_a ev_a,
-// r_a = (r_a + ev_a - v) * t / (t + 1), s_a += t sigma_a, val[node] = v * scale.
-__device__ __forceinline__ void cfv_update(const CfvView &V, const CfvItem &I, int h0,
-                                           const float2 (&ev)[SS_MAX_ACTIONS]) {
+template <int S>
+__global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
+                                                     const CfvItem *__restrict__ items, int nchunk, int Hl,
+                                                     int trav) {
+    const int it = blockIdx.x / nchunk;
+    const int ch = blockIdx.x - it * nchunk;
+    const CfvItem I = items[it];
+    if (retired(ctxs, I.sg)) return;
+    const CfvView V = ctxs ? cfv_view(ctxs[I.sg], ctxs[I.sg].H[trav]) : cfv_view(c0, Hl);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h0 = (S == 1 ? ch * (kCfvThreads / 32) + warp : ch) * 64 + lane * 2;
+    const bool act = h0 < V.H;
+    if (S == 1 && !act) return;
     const size_t HS = static_cast<size_t>(V.HS);
+    const float *val = V.val + h0;
+    const int *__restrict__ fr = V.fr_items;
+    // the regret and strategy-sum rows are needed after the frontier sums:
+    // start bringing them into L1 now (no registers held)
+    if (act && (S == 1 || warp == 0)) {
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+            if (a < I.na) {
+                const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(V.R + off));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(V.S + off));
+            }
+        }
+    }
+    float2 ev[SS_MAX_ACTIONS];
+#pragma unroll
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a) ev[a] = make_float2(0.f, 0.f);
+    if constexpr (S == 1) {
+        // the frontiers of all edges are one contiguous run of rows: walk it
+        // eight rows at a time across edge boundaries (short frontiers, one
+        // row per edge at the lowest level, would otherwise leave one load in
+        // flight); each row adds to its edge in row order
+        const int fe = I.first_edge;
+        int bnd[SS_MAX_ACTIONS];
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
+        const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
+        for (int k = k0; k < kend; k += 8) {
+            float2 x[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                x[i] = k + i < kend ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS) : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (k + i < kend) {
+                    int e = 0;
+#pragma unroll
+                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
+#pragma unroll
+                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+                        if (e == a) add2(ev[a], x[i]);
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+            if (a < I.na && act) {
+                float2 e = make_float2(0.f, 0.f);
+                int k = V.fr_off[I.first_edge + a] + warp;
+                const int k1 = V.fr_off[I.first_edge + a + 1];
+                for (; k + 7 * S < k1; k += 8 * S) {
+                    float2 x[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) x[i] = ld2(val + static_cast<size_t>(__ldg(fr + k + i * S)) * HS);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) add2(e, x[i]);
+                }
+                if (k < k1) {
+                    // the last (< 8) rows of this warp, loaded together; the
+                    // missing ones add +0, so the sum is the row-order sum
+                    float2 x[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        x[i] = k + i * S < k1 ? ld2(val + static_cast<size_t>(__ldg(fr + k + i * S)) * HS)
+                                              : make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) add2(e, x[i]);
+                }
+                ev[a] = e;
+            }
+        }
+    }
+    if constexpr (S > 1) {
+        __shared__ float2 part[S][SS_MAX_ACTIONS][32];
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+            if (a < I.na) part[warp][a][lane] = ev[a];
+        __syncthreads();
+        if (warp != 0 || !act) return;
+#pragma unroll
+        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
+            if (a < I.na) {
+                float2 e = part[0][a][lane];
+#pragma unroll
+                for (int w = 1; w < S; ++w) add2(e, part[w][a][lane]);
+                ev[a] = e;
+            }
+        }
+    }
     // the regrets are read three times (sum, value, update) instead of being
     // held in registers; the rereads hit L1
     const float *Rh = V.R + static_cast<size_t>(I.first_edge) * HS + h0;
@@ -222,117 +315,6 @@ __device__ __forceinline__ void cfv_update(const CfvView &V, const CfvItem &I, i
     // scale 1 on a single street (exact: the row equals v); below chance
     // nodes the row carries their 1 / cards weights for the parent's frontier
     st2(V.val + static_cast<size_t>(I.node) * HS + h0, make_float2(v0 * I.scale, v1 * I.scale));
-}
-
-template <int S>
-__global__ void __launch_bounds__(cfv_threads(S), S > kCfvThreads / 32 ? 2 : 8)
-    k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs, const CfvItem *__restrict__ items, int nchunk, int Hl,
-          int trav) {
-    const int it = blockIdx.x / nchunk;
-    const int ch = blockIdx.x - it * nchunk;
-    const CfvItem I = items[it];
-    if (retired(ctxs, I.sg)) return;
-    const CfvView V = ctxs ? cfv_view(ctxs[I.sg], ctxs[I.sg].H[trav]) : cfv_view(c0, Hl);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int h0 = (S == 1 ? ch * (kCfvThreads / 32) + warp : ch) * 64 + lane * 2;
-    const bool act = h0 < V.H;
-    // whole warps past the hands leave; lanes past them stay for the shuffles
-    if (S == 1 && __all_sync(0xffffffffu, !act)) return;
-    const size_t HS = static_cast<size_t>(V.HS);
-    const float *val = V.val + (act ? h0 : 0);
-    const int *__restrict__ fr = V.fr_items;
-    // the regret and strategy-sum rows are needed after the frontier sums:
-    // start bringing them into L1 now (no registers held)
-    if (act && (S == 1 || warp == 0)) {
-#pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-            if (a < I.na) {
-                const size_t off = static_cast<size_t>(I.first_edge + a) * HS + h0;
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(V.R + off));
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(V.S + off));
-            }
-        }
-    }
-    float2 ev[SS_MAX_ACTIONS];
-#pragma unroll
-    for (int a = 0; a < SS_MAX_ACTIONS; ++a) ev[a] = make_float2(0.f, 0.f);
-    if constexpr (S == 1) {
-        // the frontiers of all edges are one contiguous run of rows: walk it
-        // eight rows at a time across edge boundaries (short frontiers, one
-        // row per edge at the lowest level, would otherwise leave one load in
-        // flight); each row adds to its edge in row order
-        const int fe = I.first_edge;
-        int bnd[SS_MAX_ACTIONS];
-#pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
-        const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
-        for (int k = k0; k < kend; k += 8) {
-            float2 x[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                x[i] = (k + i < kend && act) ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS)
-                                             : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (k + i < kend) {
-                    int e = 0;
-#pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
-#pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
-                        if (e == a) add2(ev[a], x[i]);
-                }
-            }
-        }
-    } else {
-#pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-            if (a < I.na) {
-                // this warp's rows of edge a: k0, k0 + S, ... below k1, in
-                // windows of 32 (row indices one per lane)
-                float2 e = make_float2(0.f, 0.f);
-                const int k0 = V.fr_off[I.first_edge + a] + warp;
-                const int k1 = V.fr_off[I.first_edge + a + 1];
-                for (int kb = k0; kb < k1; kb += 32 * S) {
-                    const int kl = kb + lane * S;
-                    const int idx = kl < k1 ? __ldg(fr + kl) : 0;
-                    const int nrow = min(32, (k1 - kb + S - 1) / S);
-                    for (int j = 0; j < nrow; j += 8) {
-                        // rows past the end add +0, so the sum is the row-order sum
-                        float2 x[8];
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            const int r = __shfl_sync(0xffffffffu, idx, j + i);
-                            x[i] = (j + i < nrow && act) ? ld2(val + static_cast<size_t>(r) * HS)
-                                                         : make_float2(0.f, 0.f);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) add2(e, x[i]);
-                    }
-                }
-                ev[a] = e;
-            }
-        }
-    }
-    if constexpr (S > 1) {
-        __shared__ float2 part[S][SS_MAX_ACTIONS][32];
-#pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a)
-            if (a < I.na) part[warp][a][lane] = ev[a];
-        __syncthreads();
-        if (warp != 0) return;
-#pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a) {
-            if (a < I.na) {
-                float2 e = part[0][a][lane];
-#pragma unroll
-                for (int w = 1; w < S; ++w) add2(e, part[w][a][lane]);
-                ev[a] = e;
-            }
-        }
-    }
-    if (!act) return;
-    cfv_update(V, I, h0, ev);
 }
 
 // --------------------------------------------------------------------------
@@ -2513,21 +2495,19 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
 }
 
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
-                       const DevCtx *ctxs, int trav, int n_wide) {
+                       const DevCtx *ctxs, int trav) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     n_long = n_long < 0 ? 0 : n_long > n ? n : n_long;
-    n_wide = n_wide < 0 ? 0 : n_wide > n_long ? n_long : n_wide;
-    const int n_short = n - n_long, n_split = n_long - n_wide;
+    const int n_short = n - n_long;
     if (n_short > 0) {
         const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
-        k_cfv<1><<<n_short * nc, cfv_threads(1), 0, s>>>(c, ctxs, items, nc, H, trav);
+        k_cfv<1><<<n_short * nc, kCfvThreads, 0, s>>>(c, ctxs, items, nc, H, trav);
     }
-    const int nc = (H + 63) / 64;
-    if (n_split > 0)
-        k_cfv<kCfvSplit><<<n_split * nc, cfv_threads(kCfvSplit), 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
-    if (n_wide > 0)
-        k_cfv<kCfvSplitWide><<<n_wide * nc, cfv_threads(kCfvSplitWide), 0, s>>>(c, ctxs, items + n_short + n_split,
-                                                                              nc, H, trav);
+    if (n_long > 0) {
+        const int nc = (H + 63) / 64;
+        static_assert(32 * kCfvSplit == kCfvThreads, "the split form fills one block of kCfvThreads");
+        k_cfv<kCfvSplit><<<n_long * nc, kCfvThreads, 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
+    }
     return cudaGetLastError();
 }
 

@@ -78,10 +78,8 @@ constexpr int kHandThreads = 64;
 constexpr int kHandsPerBlock = kHandThreads * 4;
 // threads per block of the value/regret kernel (2 hands each)
 constexpr int kCfvThreads = 128;
-// warps that share one hand chunk of a value/regret item with a long frontier,
-// and with a very long one
+// warps that share one hand chunk of a value/regret item with a long frontier
 constexpr int kCfvSplit = 4;
-constexpr int kCfvSplitWide = 16;
 // threads per block of the per-terminal kernels
 constexpr int kTermThreads = 256;
 
@@ -91,10 +89,9 @@ constexpr int kTermThreads = 256;
 // count of the launch).
 cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, cudaStream_t s,
                          const DevCtx *ctxs = nullptr, int player = -1);
-// The last n_long items (long frontiers) run with kCfvSplit warps per hand
-// chunk, the last n_wide of those (very long frontiers) with kCfvSplitWide.
+// The last n_long items (long frontiers) run with kCfvSplit warps per hand chunk.
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
-                       const DevCtx *ctxs = nullptr, int trav = -1, int n_wide = 0);
+                       const DevCtx *ctxs = nullptr, int trav = -1);
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                          cudaStream_t s, const DevCtx *ctxs = nullptr);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,

@@ -265,8 +265,7 @@ int solve_noalloc(const Problem &pb, int iterations, SSOutput *out) {
                                    static_cast<int>(P.term[t][k].size()), t, s0));
             for (size_t l = 0; l < cfv_lv[t].size(); ++l)
                 NA_CK(launch_cfv(c, reinterpret_cast<const CfvItem *>(base + o_cfv[t]) + cfv_lv[t][l].first,
-                                 cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t], s0, nullptr, -1,
-                                 P.cfv_nwide[t][l]));
+                                 cfv_lv[t][l].second, P.cfv_nlong[t][l], P.H[t], s0));
             NA_CK(reach(t));
         }
     }

@@ -243,13 +243,10 @@ int build_plan(const Problem &pb, Plan *out) {
             P.cfv_levels[t][h].push_back(it);
         }
         P.cfv_nlong[t].assign(P.cfv_levels[t].size(), 0);
-        P.cfv_nwide[t].assign(P.cfv_levels[t].size(), 0);
         for (size_t l = 0; l < P.cfv_levels[t].size(); ++l) {
-            const auto n = order_cfv_level(P.cfv_levels[t][l], [&](const CfvItem &it) {
+            P.cfv_nlong[t][l] = order_cfv_level(P.cfv_levels[t][l], [&](const CfvItem &it) {
                 return P.fr_off[it.first_edge + it.na] - P.fr_off[it.first_edge];
             });
-            P.cfv_nlong[t][l] = n.first;
-            P.cfv_nwide[t][l] = n.second;
         }
     }
 

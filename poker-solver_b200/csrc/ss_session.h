@@ -181,7 +181,7 @@ class Session {
             e = mark(PC_CFV, cfv_bytes[t][l], cfv_lv[t][l].second);
             if (e == cudaSuccess)
                 e = launch_cfv(c, cfv_items[t] + cfv_lv[t][l].first, cfv_lv[t][l].second, P.cfv_nlong[t][l],
-                               P.H[t], stream, nullptr, -1, P.cfv_nwide[t][l]);
+                               P.H[t], stream);
             if (e != cudaSuccess) return e;
         }
         return reach(t);
