@@ -608,6 +608,168 @@ SSB_CR3_HD void hand_mass_cls_slice(int a, int b, const Tables &t, const int *p3
     }
 }
 
+// ---------------------------------------------------------------------------
+// four-way showdowns on sparse ranges: the weaker parts' tables grown along
+// the walk, and the tying parts' pairs evaluated from them directly
+// ---------------------------------------------------------------------------
+// An opponent hand added to one side of the tables: dense cards x, y and a
+// positive reach r.
+struct EHand {
+    double r;
+    int x, y;
+};
+
+// Adds hands to the first opponent's matrix A (side 0) or the second's B
+// (side 1), keeping every table equal to a direct build of the larger
+// sets (up to the order of the FP64 additions; the counts exactly).  Work
+// items f = 0 .. kS-1 own card f -- for side 0 column f of P (rows x, y),
+// row f of A and PT, for side 1 row f of P and column f of PT, row f of B --
+// plus w[f], iw[f], d[f], id[f]; item kS adds to the scalars.  Within a call
+// only the other side's tables are read, so the items are independent:
+// side 0, then (after a block barrier) side 1 adds the product's cross
+// terms through the updated A.
+SSB_CR3_HD void add_hands(int tid, int nt, const Tables &t, int side, const EHand *L, int n) {
+    double *X = side == 0 ? t.A : t.B;            // the matrix that grows
+    const double *Y = side == 0 ? t.B : t.A;      // the other one
+    double *uX = side == 0 ? t.uA : t.uB;
+    const double *uY = side == 0 ? t.uB : t.uA;
+    int *iuX = side == 0 ? t.iuA : t.iuB;
+    const int *iuY = side == 0 ? t.iuB : t.iuA;
+    unsigned long long *mX = side == 0 ? t.mA : t.mB;
+    const unsigned long long *mY = side == 0 ? t.mB : t.mA;
+    for (int f = tid; f <= kS; f += nt) {
+        if (f == kS) {
+            double s0 = 0.0, s2 = 0.0, s3 = 0.0;
+            long long i2 = 0, i3 = 0;
+            for (int k = 0; k < n; ++k) {
+                const int x = L[k].x, y = L[k].y;
+                const double r = L[k].r;
+                s0 += r;
+                s2 += r * (uY[x] + uY[y]);
+                s3 += r * Y[x * kS + y];
+                i2 += iuY[x] + iuY[y];
+                i3 += static_cast<long long>((mY[x] >> y) & 1ull);
+            }
+            t.sc[side] += s0;
+            t.sc[2] += s2;
+            t.sc[3] += s3;
+            t.isc[side] += n;
+            t.isc[2] += i2;
+            t.isc[3] += i3;
+            continue;
+        }
+        double wf = 0.0;
+        int iwf = 0;
+        for (int k = 0; k < n; ++k) {
+            const int x = L[k].x, y = L[k].y;
+            const double r = L[k].r;
+            if (side == 0) {
+                // P = A B: rows x and y gain r * rows y and x of B
+                t.P[x * kS + f] += r * Y[y * kS + f];
+                t.P[y * kS + f] += r * Y[x * kS + f];
+                t.PT[f * kS + x] = t.P[x * kS + f];
+                t.PT[f * kS + y] = t.P[y * kS + f];
+            } else {
+                // columns x and y gain r * columns y and x of A
+                t.P[f * kS + x] += t.A[f * kS + y] * r;
+                t.P[f * kS + y] += t.A[f * kS + x] * r;
+                t.PT[x * kS + f] = t.P[f * kS + x];
+                t.PT[y * kS + f] = t.P[f * kS + y];
+            }
+            // w = A uB + B uA: the grown u at x, y times the other matrix's column
+            wf += r * (Y[f * kS + x] + Y[f * kS + y]);
+            iwf += static_cast<int>((mY[f] >> x) & 1ull) + static_cast<int>((mY[f] >> y) & 1ull);
+            if (f == x || f == y) {
+                const int o = f == x ? y : x;
+                X[f * kS + o] = r;
+                mX[f] |= 1ull << o;
+                uX[f] += r;
+                iuX[f] += 1;
+                wf += r * uY[o];
+                iwf += iuY[o];
+            }
+        }
+        t.w[f] += wf;
+        t.iw[f] += iwf;
+        t.d[f] = t.P[f * kS + f];
+        t.id[f] = popc64(t.mA[f] & t.mB[f]);
+    }
+}
+
+// One opponent's mass (and count of positive-reach hands) avoiding the six
+// cards c[0..5], from its side of the tables: F - sum u + sum of the matrix
+// over the pairs of the six (a hand touches at most two of them).
+SSB_CR3_HD void one_opp_avoid6(const double *M, const double *u, const unsigned long long *m, const int *iu, double F,
+                               long long iF, const int c[6], double *mass, long long *count) {
+    double s = F;
+    long long n = iF;
+    for (int i = 0; i < 6; ++i) {
+        s -= u[c[i]];
+        n -= iu[c[i]];
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = i + 1; j < 6; ++j) {
+            s += M[c[i] * kS + c[j]];
+            n += static_cast<long long>((m[c[i]] >> c[j]) & 1ull);
+        }
+    *mass = s;
+    *count = n;
+}
+
+// Class masses and exact tuple counts of pair pr (EL 1, LE 2, EE 3) for the
+// traverser hand (a, b) when the tables hold the weaker parts L1 (A) and L2
+// (B) and the tying parts are the short lists E1, E2: EL sums over E1 the
+// second opponent's L2 mass avoiding the six cards, LE over E2 the first's
+// L1 mass, EE enumerates E1 x E2.  Third-opponent entries k0, k0 + kstep, ...
+// below hi, split by class as in hand_mass_cls_slice; a term without a tuple
+// adds nothing, so a class whose count is 0 has mass exactly 0.
+SSB_CR3_HD void e_pair_slice(int pr, int a, int b, const Tables &t, const EHand *E1, int n1, const EHand *E2, int n2,
+                             const int *p3, int lo, int hi, long long k0, long long kstep, double out[2],
+                             long long cnt[2]) {
+    out[0] = out[1] = 0.0;
+    cnt[0] = cnt[1] = 0;
+    const long long n3 = t.isc[4];
+    const EHand *E = pr == 1 ? E1 : E2;
+    const int nE = pr == 1 ? n1 : n2;
+    for (long long k = k0; k < n3; k += kstep) {
+        if (p3[k] >= hi) continue;
+        const int x = t.xy[k] & 0xff, y = t.xy[k] >> 8;
+        if (x == a || x == b || y == a || y == b) continue;
+        const int cls = p3[k] < lo ? 0 : 1;
+        const double r3 = t.r3[k];
+        if (pr == 3) {
+            for (int i = 0; i < n1; ++i) {
+                const int e = E1[i].x, f = E1[i].y;
+                if (e == a || e == b || e == x || e == y || f == a || f == b || f == x || f == y) continue;
+                for (int j = 0; j < n2; ++j) {
+                    const int g = E2[j].x, h = E2[j].y;
+                    if (g == a || g == b || g == x || g == y || g == e || g == f || h == a || h == b || h == x ||
+                        h == y || h == e || h == f)
+                        continue;
+                    out[cls] += r3 * (E1[i].r * E2[j].r);
+                    cnt[cls] += 1;
+                }
+            }
+            continue;
+        }
+        for (int i = 0; i < nE; ++i) {
+            const int e = E[i].x, f = E[i].y;
+            if (e == a || e == b || e == x || e == y || f == a || f == b || f == x || f == y) continue;
+            const int c6[6] = {a, b, x, y, e, f};
+            double m;
+            long long n;
+            if (pr == 1)
+                one_opp_avoid6(t.B, t.uB, t.mB, t.iuB, t.sc[1], t.isc[1], c6, &m, &n);
+            else
+                one_opp_avoid6(t.A, t.uA, t.mA, t.iuA, t.sc[0], t.isc[0], c6, &m, &n);
+            if (n > 0) {
+                out[cls] += r3 * (E[i].r * m);
+                cnt[cls] += n;
+            }
+        }
+    }
+}
+
 // The largest FP64 rounding of hand_mass on a tuple set that is empty: each
 // of its ~H3 terms is a few F_A F_B in size times r3 <= F3, so 1e-9 of
 // F_A F_B F3 bounds it with a wide margin; a hand whose mass is at or below

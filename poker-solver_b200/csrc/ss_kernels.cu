@@ -2019,9 +2019,15 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const D
 // mass within rounding of 0 takes its exact tuple count (0: exactly 0).
 constexpr int kSd3Positions = 1081;   // C(47, 2): rank positions on every river board
 constexpr int kSd3Warps = kTermThreads / 32;
+// a tie group whose tying parts hold at most this many positive-reach hands
+// of each of the first two opponents takes the sparse steps (grown weaker
+// parts, tying pairs evaluated directly); a longer one rebuilds tables
+constexpr int kSd3MaxE = 64;
+// a table build in units of one D2 evaluation (the sparse steps' cost model)
+constexpr double kSd3BuildCost = 3000.0;
 constexpr size_t sd3_smem(int HS) {
     return cr3_smem(HS) + static_cast<size_t>(HS) * sizeof(int) + 16 + 3 * kTermThreads +
-           2 * kSd3Warps * (sizeof(double) + sizeof(long long)) + 64;
+           2 * kSd3Warps * (sizeof(double) + sizeof(long long)) + 64 + 2 * kSd3MaxE * sizeof(cr3::EHand) + 16 + 64;
 }
 
 template <class T>
@@ -2076,6 +2082,10 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     unsigned char *ga = cv.take<unsigned char>(kTermThreads);
     unsigned char *gb = cv.take<unsigned char>(kTermThreads);
     unsigned char *ghas = cv.take<unsigned char>(kTermThreads);
+    // the current tie group's tying hands of the first two opponents, and their numbers
+    cr3::EHand *elist1 = cv.take<cr3::EHand>(kSd3MaxE);
+    cr3::EHand *elist2 = cv.take<cr3::EHand>(kSd3MaxE);
+    int *en = cv.take<int>(2);
     const int lane = tid & 31, warp = tid >> 5;
     const T *reach = reach_rows<T>(c);
     const int o1 = I.opp_player[0], o2 = I.opp_player[1], o3 = I.opp_player[2];
@@ -2120,22 +2130,83 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
     // slice), and each hand's owner thread combines its warps' partials in
     // warp order.  A mass within rounding of 0 takes the exact tuple count
     // (a second pass of the same shape over the 0/1 tables).
+    // the weaker parts' tables (positions [0, t_hi) of the first two
+    // opponents), grown group by group while the groups' tying parts are short
+    bool t_valid = false;
+    int t_hi = 0;
     for (int g = q0; g < qend;) {
         const int lo = c.sd_combo[g].lo, hi = c.sd_combo[g].hi;
         const bool mine = st.h >= 0 && st.glo == lo;
-        if (__syncthreads_or(mine)) {
+        const int nmine = __syncthreads_count(mine);   // the traverser's hands of this group in the block
+        const bool any = nmine > 0;
+        // the group's tying hands of the first two opponents with positive
+        // reach, in rank order (warp 0: first opponent, warp 1: second)
+        if (warp < 2) {
+            const int *ph = c.pos_hand + static_cast<size_t>(warp == 0 ? o1 : o2) * nc;
+            const T *rr = warp == 0 ? in.r1 : in.r2;
+            const int *code = c.hand_code + static_cast<size_t>(warp == 0 ? o1 : o2) * hs;
+            cr3::EHand *E = warp == 0 ? elist1 : elist2;
+            int n = 0;
+            for (int base = lo; base < hi; base += 32) {
+                const int q = base + lane;
+                const int hh = q < hi ? ph[q] : -1;
+                const T rv = hh >= 0 ? rr[hh] : T(0);
+                const bool ok = hh >= 0 && rv > T(0);
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                const int at = n + __popc(bal & ((1u << lane) - 1u));
+                if (ok && at < kSd3MaxE) {
+                    const int hc = code[hh];
+                    E[at] = cr3::EHand{static_cast<double>(rv), (hc >> 20) & 63, (hc >> 26) & 63};
+                }
+                n += __popc(bal);
+            }
+            if (lane == 0) en[warp] = n;
+        }
+        __syncthreads();
+        const int n1 = en[0], n2 = en[1];
+        const bool small = n1 <= kSd3MaxE && n2 <= kSd3MaxE;
+        if (any) {
+            // LL from the weaker parts' tables (grown along the walk, or built
+            // here); a pair with a tying part is evaluated directly from them
+            // when that costs less than building its own tables (direct: a
+            // six-card one-opponent mass per tying hand and third-opponent
+            // hand; built: a table build shared by the group's hands, then one
+            // D2 per third-opponent hand) -- sparse ranges go direct, full
+            // ranges build; the direct pairs run first, while the tables
+            // still hold the weaker parts
+            if (!(t_valid && t_hi == lo)) {
+                build(0, lo, 0, lo);
+                t_valid = true;
+                t_hi = lo;
+            }
+            const double work = static_cast<double>(nmine) * static_cast<double>(t.isc[4]);
+            auto go_direct = [&](int pr) {
+                if (!small) return false;
+                const double terms = pr == 1 ? n1 : pr == 2 ? n2 : 0.125 * n1 * n2;
+                return work * (0.8 * terms) <= kSd3BuildCost + work;
+            };
+            int order[4] = {0, 0, 0, 0}, no = 1;
+            for (int pr = 1; pr < 4; ++pr)
+                if (go_direct(pr)) order[no++] = pr;
+            for (int pr = 1; pr < 4; ++pr)
+                if (!go_direct(pr)) order[no++] = pr;
             const int j0 = max(lo, q0) - q0, ng = min(hi, qend) - q0 - j0;
             const int per = ng >= kSd3Warps ? 1 : kSd3Warps / ng;   // warps per hand
             const int hpr = kSd3Warps / per;                          // hands per round
             const int r = warp / per, sl = warp - r * per;
             const int jl = tid - j0;                                  // this thread's index in the group
-            auto walk = [&](int base, bool want_count) {
+            auto walk = [&](int pr, bool direct, int base, bool want_count) {
                 const int j = j0 + base + r;
                 double o[2] = {0.0, 0.0};
                 long long n[2] = {0, 0};
-                if (r < hpr && base + r < ng && ghas[j])
-                    cr3::hand_mass_cls_slice(ga[j], gb[j], t, p3, lo, hi, sl * 32 + lane, per * 32, o, n,
-                                             want_count);
+                if (r < hpr && base + r < ng && ghas[j]) {
+                    if (direct)
+                        cr3::e_pair_slice(pr, ga[j], gb[j], t, elist1, n1, elist2, n2, p3, lo, hi, sl * 32 + lane,
+                                          per * 32, o, n);
+                    else
+                        cr3::hand_mass_cls_slice(ga[j], gb[j], t, p3, lo, hi, sl * 32 + lane, per * 32, o, n,
+                                                 want_count);
+                }
                 for (int off = 16; off > 0; off >>= 1) {
                     o[0] += __shfl_xor_sync(0xffffffffu, o[0], off);
                     o[1] += __shfl_xor_sync(0xffffffffu, o[1], off);
@@ -2150,7 +2221,8 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
                 }
                 __syncthreads();
             };
-            for (int pr = 0; pr < 4; ++pr) {
+            for (int step = 0; step < 4; ++step) {
+                const int pr = order[step];
                 int lo1, hi1, lo2, hi2;
                 cr3::sd3_pair_bounds(pr, lo, hi, &lo1, &hi1, &lo2, &hi2);
                 // an opponent without a hand in its part of the pair: no
@@ -2160,26 +2232,41 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
                     if (mine) st.m[pr][0] = st.m[pr][1] = 0.0;
                     continue;
                 }
-                build(lo1, hi1, lo2, hi2);
+                // direct: a pair with a short tying part, from the weaker
+                // parts' tables and the lists (masses and exact counts in one
+                // walk); otherwise the pair's own tables
+                const bool direct = pr > 0 && go_direct(pr);
+                if (pr > 0 && !direct) {
+                    build(lo1, hi1, lo2, hi2);
+                    t_valid = false;   // the pair's tables replace the weaker parts'
+                }
                 const double zb = cr3::zero_bound(t);
                 bool near_zero = false;
                 for (int base = 0; base < ng; base += hpr) {
-                    walk(base, false);
+                    walk(pr, direct, base, false);
                     if (mine && jl >= base && jl < base + hpr) {
                         double m0 = 0.0, m1 = 0.0;
+                        long long c0 = 0, c1 = 0;
                         for (int k = 0; k < per; ++k) {
                             m0 += part[2 * ((jl - base) * per + k)];
                             m1 += part[2 * ((jl - base) * per + k) + 1];
+                            c0 += partc[2 * ((jl - base) * per + k)];
+                            c1 += partc[2 * ((jl - base) * per + k) + 1];
                         }
-                        st.m[pr][0] = m0;
-                        st.m[pr][1] = m1;
-                        near_zero = fabs(m0) <= zb || fabs(m1) <= zb;
+                        if (direct) {
+                            st.m[pr][0] = c0 == 0 ? 0.0 : m0;
+                            st.m[pr][1] = c1 == 0 ? 0.0 : m1;
+                        } else {
+                            st.m[pr][0] = m0;
+                            st.m[pr][1] = m1;
+                            near_zero = fabs(m0) <= zb || fabs(m1) <= zb;
+                        }
                     }
                     __syncthreads();
                 }
                 if (__syncthreads_or(near_zero)) {
                     for (int base = 0; base < ng; base += hpr) {
-                        walk(base, true);
+                        walk(pr, false, base, true);
                         if (mine && jl >= base && jl < base + hpr)
                             for (int cls = 0; cls < 2; ++cls) {
                                 long long n = 0;
@@ -2189,6 +2276,23 @@ __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const D
                         __syncthreads();
                     }
                 }
+            }
+        }
+        // advance the weaker parts' tables past this group: its tying hands
+        // join the first opponent's side, then the second's
+        if (t_valid && t_hi == lo) {
+            if (!small) {
+                t_valid = false;
+            } else {
+                if (n1 > 0) {
+                    cr3::add_hands(tid, kTermThreads, t, 0, elist1, n1);
+                    __syncthreads();
+                }
+                if (n2 > 0) {
+                    cr3::add_hands(tid, kTermThreads, t, 1, elist2, n2);
+                    __syncthreads();
+                }
+                t_hi = hi;
             }
         }
         g = hi;

@@ -14,6 +14,12 @@ rules, street_solve.cu:771-823 folds, :936-1002 showdowns):
   class) and the value, with ties from few rank levels up to every hand
   tying, a pot / 3 equal to the bet, and a bet of 0; counts exact and the
   classes without a tuple exactly 0;
+* sparse four-way showdowns (tests/native/sd3inc_emul): the weaker parts'
+  tables grown hand by hand along the rank levels equal a direct build at
+  every level (FP64 fields to 1e-13 relative, masks and counts exactly), and
+  the pairs with a tying part evaluated from those tables and the tying
+  hands' lists equal each pair's own tables' class masses, with exact tuple
+  counts and classes without a tuple exactly 0;
 * both kernels' blocks driven by the planner's own work items and tables
   for seeded 4-player rivers and a 4-player turn (tests/native/term3_emul,
   with ss_plan.cpp and ss_tree.cpp): hand codes, pair tables, rank
@@ -107,3 +113,23 @@ def test_kernel_blocks_on_planned_items(term3, args):
     assert d["items"] > 0 and d["hands"] > 0
     assert d["max_rel_err"] <= 1e-12
     assert d["zero_bad"] == 0
+
+
+@pytest.fixture(scope="module")
+def sd3inc(tmp_path_factory):
+    return _build(tmp_path_factory, "sd3inc_emul")
+
+
+@pytest.mark.parametrize("args", [
+    (1, 20, 60, 0.3, 6),       # small deck, several hands per level
+    (2, 47, 120, 0.5, 12),     # river deck, half the weights zero
+    (3, 12, 40, 0.0, 3),       # few levels: large tying parts
+    (4, 30, 200, 0.6, 30),     # many levels, sparse
+])
+def test_sparse_showdown_steps_against_direct_builds(sd3inc, args):
+    r = subprocess.run([sd3inc] + [str(a) for a in args], check=True, capture_output=True, text=True)
+    d = json.loads(r.stdout)
+    assert d["hands"] > 0
+    assert d["bad"] == 0
+    assert d["max_table_err"] <= 1e-13
+    assert d["max_rel_err"] <= 1e-12
