@@ -819,6 +819,7 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int HS = V.HS;
     const int Dp = (V.deck + 3) & ~3;
+    const int hc_first = tid < V.Ht ? __ldg(V.code_t + tid) : 0;   // this thread's first hand code
     // shared memory was provisioned for c0's row stride (the largest of a batch)
     if (HS > c0.HS || V.deck > 52) return;
     Carve cv{smem};
@@ -965,10 +966,14 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     const bool leaf_first = gleaf[0] >= 0;
     const float gp0 = gpay[0];
     T *out0 = V.val + static_cast<size_t>(gnode[0]) * HS;
+    // the next hand's code is loaded one iteration ahead (the first one at
+    // the start of the block), so the loop does not wait on it
+    int hc_next = hc_first;
     for (int h = tid; h < HS; h += kTermThreads) {
+        const int hc = hc_next;
+        hc_next = h + kTermThreads < Ht ? __ldg(tc + h + kTermThreads) : 0;
         double v = 0.0;
         if (h < Ht && !none) {
-            const int hc = __ldg(tc + h);
             const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
             const bool on = (a < kCr2Off) && (b < kCr2Off);
             const Cr2Card ga = card[a], gb = card[b];
