@@ -28,6 +28,7 @@ import argparse
 import ctypes
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -282,7 +283,11 @@ def ncu_summary(csv_path, workload, command):
         d = launch.setdefault(r[ii], {"name": r[ki]})
         d[r[mi]] = float(r[vi].replace(",", ""))
     for d in launch.values():
-        cls = next((c for p, c in NCU_CLASSES if d["name"].startswith(p)), None)
+        # ncu prints the demangled signature ("void ...::k_term_cr2<float>(...)")
+        # or, with --print-kernel-base function, the bare name
+        m = re.search(r"(?:^|[\s:])(k_\w+)", d["name"])
+        base = m.group(1) if m else d["name"]
+        cls = next((c for p, c in NCU_CLASSES if base.startswith(p)), None)
         if cls is None:
             continue
         e = per.setdefault(cls, {"launches_captured": 0, "bytes": 0.0})
