@@ -163,8 +163,16 @@ enum TermKind : int {
 // (the traverser's own continuation choices below one opponent pair) form a
 // group: consecutive items, the first with gextra = number of followers, the
 // followers with follow = 1.  A zeroed item is a group of one.  Groups hold
-// at most kTermGroupMax items.
+// at most kTermGroupMax items.  Consecutive two-opponent groups on the same
+// first-opponent row form a chain of at most kCr2ChainMax groups, computed
+// by one block that builds the first opponent's matrix once: the chain's
+// first leader has chain = number of groups after it, the other leaders
+// chained = 1.  Chains are formed only where a launch keeps at least
+// kCr2ChainBlocks blocks (about three waves of the kernel on a B200: with
+// fewer, the longer blocks of a chain leave the last wave's SMs idle).
 constexpr int kTermGroupMax = 16;
+constexpr int kCr2ChainMax = 4;
+constexpr int kCr2ChainBlocks = 2048;
 struct alignas(16) TermItem {
     int node;
     int kind_detail;          // TK_ENUM: 0 fold, 1 leaf, 2 showdown; TK_SD2: log2 of the runs per block
@@ -178,6 +186,8 @@ struct alignas(16) TermItem {
     int opp_player[SS_MAX_PLAYERS - 1];
     int gextra;               // group leader: number of following items in its group
     int follow;               // 1: member of the group led by an earlier item
+    int chain;                // two-opponent chain head: number of groups after its own
+    int chained;              // 1: group leader computed by an earlier chain head
 };
 
 // Showdown tables for one board: every non-board 2-card combo ranked by the

@@ -516,8 +516,9 @@ __global__ void __launch_bounds__(kTermThreads) k_term_cr1_dup(DevCtx c0, const 
 
 // Per-card terms of the two-opponent closed form over the dense deck (the
 // non-board cards, renumbered 0 .. deck-1): FP64 sums and integer counts of
-// positive-reach cells, packed so a hand reads a few 16/32-byte entries per
-// card.  Entry 52 stays zero and stands for a board card of the traverser.
+// positive-reach cells.  Entry 52 stays zero and stands for a board card of
+// the traverser.  The tensor-core form packs the sums per card (Cr2Card);
+// k_term_cr2 keeps one array per field.
 struct alignas(16) Cr2Card {
     double u1, u2;      // per-card reach sums of opponents 1 and 2
     double g;           // u1 u2 + w - 2 d, w = (M2 u1 + M1 u2)(c), d = sum_b M1[c][b] M2[c][b]
@@ -541,7 +542,7 @@ constexpr int kMaxHS = 1344;  // largest row stride: 1326 combos rounded up to 3
 // terminal's leaf row, per-card terms, staged group items
 template <class T>
 constexpr size_t cr2_smem(int HS) {
-    return 3 * 52 * MS * sizeof(T) + static_cast<size_t>(HS) * 4 + 53 * sizeof(Cr2Card) + 53 * sizeof(Cr2Cnt) +
+    return 3 * 52 * MS * sizeof(T) + static_cast<size_t>(HS) * 4 + 3 * 56 * sizeof(double) + 53 * sizeof(Cr2Cnt) +
            53 * 16 + 5 * 48 * 4 + sizeof(Cr2Scalars) + 3 * kTermGroupMax * 4 + 8 * 16;
 }
 
@@ -712,7 +713,7 @@ __device__ __forceinline__ void product_mma48(const float *M1, const float *M2, 
 // independent partial sums in T (Dp is a multiple of 4; FP32 keeps the
 // relative error near 1e-7), added in FP64 in a fixed order
 template <class T>
-__device__ __forceinline__ void column_stats(const T *M1, const T *M2, int s, int Dp, Cr2Card *card,
+__device__ __forceinline__ void column_stats(const T *M1, const T *M2, int s, int Dp, double *cu1, double *cu2,
                                              ulonglong2 *Bm) {
     const bool second = s >= Dp;
     const int col = second ? s - Dp : s;
@@ -730,10 +731,10 @@ __device__ __forceinline__ void column_stats(const T *M1, const T *M2, int s, in
     const double tot = (static_cast<double>(u[0]) + static_cast<double>(u[1])) +
                        (static_cast<double>(u[2]) + static_cast<double>(u[3]));
     if (second) {
-        card[col].u2 = tot;
+        cu2[col] = tot;
         Bm[col].y = B;
     } else {
-        card[col].u1 = tot;
+        cu1[col] = tot;
         Bm[col].x = B;
     }
 }
@@ -801,19 +802,23 @@ __device__ __noinline__ int pair_count(const ulonglong2 *Bm, const Cr2Cnt *cnt, 
 // writes 0 when there are none.
 //
 // One block per group of terminals sharing both opponents' reach rows: the
-// masses are computed once and multiplied by each terminal's factor.
-// Phases: cp.async staging of both reach rows and the first leaf row; gather
-// (or clear + scatter for ranges that repeat a combo); P (tensor cores)
-// alongside per-column sums and masks; per-card FP64 terms and block scalars;
-// per-hand mass and one output row per terminal.
+// masses are computed once and multiplied by each terminal's factor.  A
+// chain of groups on the same first-opponent row (TermItem::chain) runs in
+// one block, one group after the other: the first opponent's matrix, its
+// column sums and masks are built once for the chain.
+// Phases per group: cp.async staging of the reach rows (both for the
+// chain's first group, the second opponent's for the others) and the first
+// leaf row; gather (or clear + scatter for ranges that repeat a combo); P
+// (tensor cores) alongside per-column sums and masks; per-card FP64 terms
+// and block scalars; per-hand mass and one output row per terminal.
 template <class T>
 __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                               const TermItem *__restrict__ items, int trav) {
     extern __shared__ __align__(16) char smem[];
     const TermItem *I0 = items + blockIdx.x;
-    if (I0->follow) return;   // written by the block of its group's first item
+    // followers are written by their group's leader, chained groups by the chain's head
+    if (I0->follow || I0->chained) return;
     if (retired(ctxs, I0->sg)) return;
-    const int ng = I0->gextra + 1;
     const int o0 = I0->opp_player[0], o1 = I0->opp_player[1];
     const Cr2View<T> V = ctxs ? cr2_view<T>(ctxs[I0->sg], trav, o0, o1) : cr2_view<T>(c0, trav, o0, o1);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -826,8 +831,9 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     T *M1 = cv.take<T>(52 * MS);
     T *M2 = cv.take<T>(52 * MS);
     T *P = cv.take<T>(52 * MS);
-    float *leaf0 = cv.take<float>(HS);
-    Cr2Card *card = cv.take<Cr2Card>(53);
+    // per-card terms, one array per field (a hand reads three of them at two
+    // cards; separate arrays keep those reads free of bank conflicts)
+    double *cu1 = cv.take<double>(56), *cu2 = cv.take<double>(56), *cg = cv.take<double>(56);
     Cr2Cnt *cnt = cv.take<Cr2Cnt>(53);
     ulonglong2 *Bm = cv.take<ulonglong2>(53);   // positive-cell masks of M1 (x) and M2 (y) per card
     float *rsum = cv.take<float>(2 * 48);       // tensor-core path: partial row / column sums of P
@@ -836,26 +842,33 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     int *gnode = cv.take<int>(kTermGroupMax);
     int *gleaf = cv.take<int>(kTermGroupMax);
     float *gpay = cv.take<float>(kTermGroupMax);
+    float *leaf0 = cv.take<float>(HS);   // last: every other offset is a constant
     // staged reach rows, each followed by a zero (P is written after the gather)
     T *r1 = P, *r2 = P + HS + 16 / sizeof(T);
+    bool mma = false;
+    if constexpr (sizeof(T) == 4) mma = Dp <= 48;
+    const int Ht = V.Ht;
+    const int *__restrict__ tc = V.code_t;
 
-    // staging: both opponents' reach rows (16-byte chunks; rows start on
-    // 128-byte boundaries) and the first terminal's leaf row (4-byte words)
-    {
-        const T *s1 = V.reach + static_cast<size_t>(I0->opp_row[0]) * HS;
-        const T *s2 = V.reach + static_cast<size_t>(I0->opp_row[1]) * HS;
+    // staging of a group: the second opponent's reach row (16-byte chunks;
+    // rows start on 128-byte boundaries), the group's first leaf row (4-byte
+    // words) and its items' fields; with_first: the first opponent's row too
+    auto stage = [&](const TermItem *G, bool with_first) {
+        const int ng = G->gextra + 1;
         constexpr int per = 16 / sizeof(T);
-        for (int q = tid * per; q < HS; q += kTermThreads * per) {
-            cp_async16(r1 + q, s1 + q);
-            cp_async16(r2 + q, s2 + q);
+        const T *s1 = V.reach + static_cast<size_t>(G->opp_row[0]) * HS;
+        const T *s2 = V.reach + static_cast<size_t>(G->opp_row[1]) * HS;
+        for (int i = tid * per; i < HS; i += kTermThreads * per) {
+            if (with_first) cp_async16(r1 + i, s1 + i);
+            cp_async16(r2 + i, s2 + i);
         }
-        const int lo = I0->leaf_off;
+        const int lo = G->leaf_off;
         if (lo >= 0) {
             const float *src = V.leaf + lo;
-            for (int h = tid; h < V.Ht; h += kTermThreads) cp_async4(leaf0 + h, src + h);
+            for (int h = tid; h < Ht; h += kTermThreads) cp_async4(leaf0 + h, src + h);
         }
         if (tid < ng) {
-            const TermItem &I = I0[tid];
+            const TermItem &I = G[tid];
             gnode[tid] = I.node;
             gleaf[tid] = I.leaf_off;
             gpay[tid] = I.payoff;
@@ -864,133 +877,156 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
             r1[HS] = T(0);
             r2[HS] = T(0);
         }
-    }
+    };
+    auto gather_second = [&]() {
+        if (V.dup)
+            scatter_dense(V.code1, V.H1, r2, M2);
+        else
+            gather_dense(V.tab1, r2, M2, Dp);
+    };
+
+    // the chain's first group: both opponents' matrices
+    stage(I0, true);
     if (V.dup) {
         zero_matrix(M1);
         zero_matrix(M2);
     }
     cp_async_wait_all();
     __syncthreads();
-    if (V.dup) {
+    if (V.dup)
         scatter_dense(V.code0, V.H0, r1, M1);
-        scatter_dense(V.code1, V.H1, r2, M2);
-    } else {
+    else
         gather_dense(V.tab0, r1, M1, Dp);
-        gather_dense(V.tab1, r2, M2, Dp);
-    }
+    gather_second();
     __syncthreads();
 
-    // phase A: P = M1 M2 (tensor cores when the deck fits 48 cards, else
-    // 4x4 SIMT tiles); per-column reach sums and positive-cell masks
-    bool mma = false;
-    if constexpr (sizeof(T) == 4) mma = Dp <= 48;
-    if (mma) {
-        if constexpr (sizeof(T) == 4) {
-            if (warp < 6) product_mma48(M1, M2, P, rsum, csum, warp, lane);
-        }
-        // columns: warps 6-7 take 0..63, warp 0 (after its MMA tiles) 64..95
-        const int s = tid >= 6 * 32 ? tid - 6 * 32 : tid < 32 ? 64 + tid : 2 * 52;
-        if (s < 2 * Dp) column_stats(M1, M2, s, Dp, card, Bm);
-    } else {
-        const int nt = Dp >> 2;
-        if (tid < nt * nt) product_tile(M1, M2, P, (tid / nt) * 4, (tid % nt) * 4, Dp);
-        const int s = kTermThreads - 1 - tid;
-        if (s < 2 * Dp) column_stats(M1, M2, s, Dp, card, Bm);
-    }
-    __syncthreads();
+    const TermItem *G = I0;
+    const int nchain = I0->chain;
+    for (int q = 0;; ++q) {
+        const bool first = q == 0;
+        const int ng = G->gextra + 1;
 
-    // phase B: per-card terms (w from the row and column sums of P, d from its
-    // diagonal: P = M1 M2 with symmetric M1, M2 gives rowsum = M1 u2,
-    // colsum = M2 u1, P[c][c] = d(c)); entries beyond the deck are zeroed;
-    // the last warp forms the block scalars
-    if (tid < Dp) {
-        const int col = tid;
-        double w;
+        // phase A: P = M1 M2 (tensor cores when the deck fits 48 cards, else
+        // 4x4 SIMT tiles); per-column reach sums and positive-cell masks (the
+        // first opponent's for the chain's first group only: they stay in
+        // cu1 and Bm[].x)
         if (mma) {
-            w = (static_cast<double>(rsum[col]) + static_cast<double>(rsum[48 + col])) +
-                ((static_cast<double>(csum[col]) + static_cast<double>(csum[48 + col])) +
-                 static_cast<double>(csum[96 + col]));
+            if constexpr (sizeof(T) == 4) {
+                if (warp < 6) product_mma48(M1, M2, P, rsum, csum, warp, lane);
+            }
+            // columns: warps 6-7 take 0..63, warp 0 (after its MMA tiles) 64..95
+            const int s = tid >= 6 * 32 ? tid - 6 * 32 : tid < 32 ? 64 + tid : 2 * 52;
+            if (s < 2 * Dp && (first || s >= Dp)) column_stats(M1, M2, s, Dp, cu1, cu2, Bm);
         } else {
-            w = 0.0;
-            for (int b = 0; b < Dp; ++b)
-                w += static_cast<double>(P[col * MS + b]) + static_cast<double>(P[b * MS + col]);
+            const int nt = Dp >> 2;
+            if (tid < nt * nt) product_tile(M1, M2, P, (tid / nt) * 4, (tid % nt) * 4, Dp);
+            const int s = kTermThreads - 1 - tid;
+            if (s < 2 * Dp && (first || s >= Dp)) column_stats(M1, M2, s, Dp, cu1, cu2, Bm);
         }
-        const double d = P[col * MS + col];
-        const double u1 = card[col].u1, u2 = card[col].u2;
-        card[col].g = u1 * u2 + w - 2.0 * d;
-        card[col].d = d;
-        const ulonglong2 Bc = Bm[col];
-        cnt[col] = Cr2Cnt{__popcll(Bc.x), __popcll(Bc.y), 0, 0};
-    } else if (tid <= kCr2Off) {
-        card[tid] = Cr2Card{0.0, 0.0, 0.0, 0.0};
-        cnt[tid] = Cr2Cnt{0, 0, 0, 0};
-        Bm[tid] = make_ulonglong2(0ull, 0ull);
-    } else if (warp == kTermThreads / 32 - 1) {
-        double a1 = 0.0, a2 = 0.0, qq = 0.0, e = 0.0;
-        int n1 = 0, n2 = 0, nq = 0, nd = 0;
-        for (int k = lane; k < Dp; k += 32) {
-            const double u1 = card[k].u1, u2 = card[k].u2;
-            a1 += u1;
-            a2 += u2;
-            qq += u1 * u2;
-            e += static_cast<double>(P[k * MS + k]);
-            const ulonglong2 B = Bm[k];
-            const int p1 = __popcll(B.x), p2 = __popcll(B.y);
-            n1 += p1;
-            n2 += p2;
-            nq += p1 * p2;
-            nd += __popcll(B.x & B.y);
-        }
-        a1 = warp_sum(a1);
-        a2 = warp_sum(a2);
-        qq = warp_sum(qq);
-        e = warp_sum(e);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            n1 += __shfl_xor_sync(0xffffffffu, n1, o);
-            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
-            nq += __shfl_xor_sync(0xffffffffu, nq, o);
-            nd += __shfl_xor_sync(0xffffffffu, nd, o);
-        }
-        if (lane == 0) *sc = Cr2Scalars{0.5 * a1, 0.5 * a2, 0.5 * e - qq, n1 / 2, n2 / 2, nd / 2 - nq, 0};
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // phase C: card-removal mass of every traverser hand, written out as
-    // factor x mass for every terminal of the group
-    const Cr2Scalars S = *sc;
-    const double zmin = 1e-4 * S.F1 * S.F2;
-    const bool none = !(S.F1 > 0.0 && S.F2 > 0.0);   // an opponent without positive reach: all zero
-    const int Ht = V.Ht;
-    const int *__restrict__ tc = V.code_t;
-    const bool leaf_first = gleaf[0] >= 0;
-    const float gp0 = gpay[0];
-    T *out0 = V.val + static_cast<size_t>(gnode[0]) * HS;
-    // the next hand's code is loaded one iteration ahead (the first one at
-    // the start of the block), so the loop does not wait on it
-    int hc_next = hc_first;
-    for (int h = tid; h < HS; h += kTermThreads) {
-        const int hc = hc_next;
-        hc_next = h + kTermThreads < Ht ? __ldg(tc + h + kTermThreads) : 0;
-        double v = 0.0;
-        if (h < Ht && !none) {
-            const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
-            const bool on = (a < kCr2Off) && (b < kCr2Off);
-            const Cr2Card ga = card[a], gb = card[b];
-            const double m1 = on ? static_cast<double>(M1[a * MS + b]) : 0.0;
-            const double m2 = on ? static_cast<double>(M2[a * MS + b]) : 0.0;
-            const double pp = on ? static_cast<double>(P[a * MS + b] + P[b * MS + a]) : 0.0;
-            const double A1 = S.F1 - ga.u1 - gb.u1 + m1;
-            const double A2 = S.F2 - ga.u2 - gb.u2 + m2;
-            v = A1 * A2 + S.QD + ga.g + gb.g - m2 * (ga.u1 + gb.u1) - m1 * (ga.u2 + gb.u2) + 3.0 * m1 * m2 - pp;
-            if (fabs(v) <= zmin && pair_count(Bm, cnt, a, b, S.IF1, S.IF2, S.IQD) <= 0) v = 0.0;
+        // phase B: per-card terms (w from the row and column sums of P, d from its
+        // diagonal: P = M1 M2 with symmetric M1, M2 gives rowsum = M1 u2,
+        // colsum = M2 u1, P[c][c] = d(c)); entries beyond the deck are zeroed;
+        // the last warp forms the block scalars
+        if (tid < Dp) {
+            const int col = tid;
+            double w;
+            if (mma) {
+                w = (static_cast<double>(rsum[col]) + static_cast<double>(rsum[48 + col])) +
+                    ((static_cast<double>(csum[col]) + static_cast<double>(csum[48 + col])) +
+                     static_cast<double>(csum[96 + col]));
+            } else {
+                w = 0.0;
+                for (int b = 0; b < Dp; ++b)
+                    w += static_cast<double>(P[col * MS + b]) + static_cast<double>(P[b * MS + col]);
+            }
+            const double d = P[col * MS + col];
+            cg[col] = cu1[col] * cu2[col] + w - 2.0 * d;
+            const ulonglong2 Bc = Bm[col];
+            cnt[col] = Cr2Cnt{__popcll(Bc.x), __popcll(Bc.y), 0, 0};
+        } else if (tid <= kCr2Off) {
+            cu1[tid] = 0.0;
+            cu2[tid] = 0.0;
+            cg[tid] = 0.0;
+            cnt[tid] = Cr2Cnt{0, 0, 0, 0};
+            Bm[tid] = make_ulonglong2(0ull, 0ull);
+        } else if (warp == kTermThreads / 32 - 1) {
+            double a1 = 0.0, a2 = 0.0, qq = 0.0, e = 0.0;
+            int n1 = 0, n2 = 0, nq = 0, nd = 0;
+            for (int k = lane; k < Dp; k += 32) {
+                const double u1 = cu1[k], u2 = cu2[k];
+                a1 += u1;
+                a2 += u2;
+                qq += u1 * u2;
+                e += static_cast<double>(P[k * MS + k]);
+                const ulonglong2 B = Bm[k];
+                const int p1 = __popcll(B.x), p2 = __popcll(B.y);
+                n1 += p1;
+                n2 += p2;
+                nq += p1 * p2;
+                nd += __popcll(B.x & B.y);
+            }
+            a1 = warp_sum(a1);
+            a2 = warp_sum(a2);
+            qq = warp_sum(qq);
+            e = warp_sum(e);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+                n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+                nq += __shfl_xor_sync(0xffffffffu, nq, o);
+                nd += __shfl_xor_sync(0xffffffffu, nd, o);
+            }
+            if (lane == 0) *sc = Cr2Scalars{0.5 * a1, 0.5 * a2, 0.5 * e - qq, n1 / 2, n2 / 2, nd / 2 - nq, 0};
         }
-        const float f0 = h >= Ht ? 0.f : leaf_first ? leaf0[h] : gp0;
-        out0[h] = static_cast<T>(static_cast<double>(f0) * v);
-        for (int g = 1; g < ng; ++g) {
-            const float f = h >= Ht ? 0.f : gleaf[g] >= 0 ? __ldg(V.leaf + gleaf[g] + h) : gpay[g];
-            V.val[static_cast<size_t>(gnode[g]) * HS + h] = static_cast<T>(static_cast<double>(f) * v);
+        __syncthreads();
+
+        // phase C: card-removal mass of every traverser hand, written out as
+        // factor x mass for every terminal of the group
+        const Cr2Scalars S = *sc;
+        const double zmin = 1e-4 * S.F1 * S.F2;
+        const bool none = !(S.F1 > 0.0 && S.F2 > 0.0);   // an opponent without positive reach: all zero
+        const bool leaf_first = gleaf[0] >= 0;
+        const float gp0 = gpay[0];
+        T *out0 = V.val + static_cast<size_t>(gnode[0]) * HS;
+        // the next hand's code is loaded one iteration ahead (the first one at
+        // the start of the block), so the loop does not wait on it
+        int hc_next = hc_first;
+        for (int h = tid; h < HS; h += kTermThreads) {
+            const int hc = hc_next;
+            hc_next = h + kTermThreads < Ht ? __ldg(tc + h + kTermThreads) : 0;
+            double v = 0.0;
+            if (h < Ht && !none) {
+                const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
+                const bool on = (a < kCr2Off) && (b < kCr2Off);
+                const double ua1 = cu1[a], ua2 = cu2[a], ub1 = cu1[b], ub2 = cu2[b];
+                const double m1 = on ? static_cast<double>(M1[a * MS + b]) : 0.0;
+                const double m2 = on ? static_cast<double>(M2[a * MS + b]) : 0.0;
+                const double pp = on ? static_cast<double>(P[a * MS + b] + P[b * MS + a]) : 0.0;
+                const double A1 = S.F1 - ua1 - ub1 + m1;
+                const double A2 = S.F2 - ua2 - ub2 + m2;
+                v = A1 * A2 + S.QD + cg[a] + cg[b] - m2 * (ua1 + ub1) - m1 * (ua2 + ub2) + 3.0 * m1 * m2 - pp;
+                if (fabs(v) <= zmin && pair_count(Bm, cnt, a, b, S.IF1, S.IF2, S.IQD) <= 0) v = 0.0;
+            }
+            const float f0 = h >= Ht ? 0.f : leaf_first ? leaf0[h] : gp0;
+            out0[h] = static_cast<T>(static_cast<double>(f0) * v);
+            for (int g = 1; g < ng; ++g) {
+                const float f = h >= Ht ? 0.f : gleaf[g] >= 0 ? __ldg(V.leaf + gleaf[g] + h) : gpay[g];
+                V.val[static_cast<size_t>(gnode[g]) * HS + h] = static_cast<T>(static_cast<double>(f) * v);
+            }
         }
+        if (q == nchain) break;
+        // the chain's next group: its second-opponent matrix replaces the
+        // last one once every thread is done with the shared state
+        G += ng;
+        __syncthreads();
+        stage(G, false);
+        if (V.dup) zero_matrix(M2);
+        cp_async_wait_all();
+        __syncthreads();
+        gather_second();
+        __syncthreads();
     }
 }
 

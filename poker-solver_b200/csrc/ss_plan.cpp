@@ -373,6 +373,26 @@ int build_plan(const Problem &pb, Plan *out) {
             }
         }
 
+    // two-opponent chains: groups on the same first-opponent row, as many per
+    // chain as keep the launch at kCr2ChainBlocks blocks or more
+    for (int t = 0; t < np; ++t) {
+        std::vector<TermItem> &v = P.term[t][TK_CR2];
+        std::vector<size_t> leads;
+        for (size_t i = 0; i < v.size(); i += static_cast<size_t>(v[i].gextra) + 1) leads.push_back(i);
+        const int len = std::min(kCr2ChainMax, std::max(1, static_cast<int>(leads.size()) / kCr2ChainBlocks));
+        if (len < 2) continue;
+        for (size_t g = 0; g < leads.size();) {
+            const TermItem &h = v[leads[g]];
+            size_t e = g + 1;
+            while (e < leads.size() && static_cast<int>(e - g) < len && v[leads[e]].opp_row[0] == h.opp_row[0] &&
+                   v[leads[e]].opp_player[0] == h.opp_player[0] && v[leads[e]].opp_player[1] == h.opp_player[1])
+                ++e;
+            v[leads[g]].chain = static_cast<int>(e - g - 1);
+            for (size_t m = g + 1; m < e; ++m) v[leads[m]].chained = 1;
+            g = e;
+        }
+    }
+
     // showdown tables: every non-board combo ranked on the 5-card board
     P.ncomb = 0;
     P.sd_combo.clear();

@@ -1,6 +1,7 @@
 // Prints, as JSON, the terminal nodes of a tree and the planner's work-list
 // sizes per traverser and terminal kind, for tests/test_plan_runs.py.
-//   plan_kinds <players> <board cards (4 or 5)> <hands> <dup player or -1> <leaf values 0/1> <raises>
+//   plan_kinds <players> <board cards (4 or 5)> <hands> <dup player or -1> <leaf values 0/1> <raises> [<bet sizes>]
+// (bet sizes: 1 -> {1.0} (default), 2 -> {0.5, 1.0}, 3 -> {0.33, 0.75, 1.5})
 // Turn trees get continuation leaves; each range is the first <hands>
 // non-board combos in card order, with the first combo repeated for the
 // dup player.
@@ -19,16 +20,19 @@ const char *last_error() { return g_err.c_str(); }
 }  // namespace ssb
 
 int main(int argc, char **argv) {
-    if (argc != 7) return 2;
+    if (argc != 7 && argc != 8) return 2;
     const int np = std::atoi(argv[1]), nb = std::atoi(argv[2]), nh = std::atoi(argv[3]);
     const int dup = std::atoi(argv[4]), with_leaves = std::atoi(argv[5]), raises = std::atoi(argv[6]);
     const int board[5] = {0, 13, 26, 40, 51};
-    float bets[1] = {1.0f};
+    const int nbets = argc == 8 ? std::atoi(argv[7]) : 1;
+    if (nbets < 1 || nbets > 3) return 2;
+    const float bet_sets[3][3] = {{1.0f}, {0.5f, 1.0f}, {0.33f, 0.75f, 1.5f}};
+    const float *bets = bet_sets[nbets - 1];
     int order[SS_MAX_PLAYERS];
     for (int p = 0; p < np; ++p) order[p] = p;
     const bool river = nb == 5;
     ssb::BuiltTree bt;
-    if (ssb::build_street_tree(board, nb, 100, 400, bets, 1, np, order, river ? 1 : 0, river ? 0 : 1, raises, &bt) !=
+    if (ssb::build_street_tree(board, nb, 100, 400, bets, nbets, np, order, river ? 1 : 0, river ? 0 : 1, raises, &bt) !=
         SS_OK)
         return 3;
     std::vector<int> base;
@@ -112,6 +116,17 @@ int main(int argc, char **argv) {
                 }
             std::printf("]");
         }
+        std::printf("]");
+    }
+    // two-opponent chains: per traverser, every item's [chain, chained]
+    std::printf("], \"chains\": [");
+    for (int t = 0; t < np; ++t) {
+        std::printf("%s[", t ? ", " : "");
+        if (rc == SS_OK)
+            for (size_t i = 0; i < P.term[t][ssb::TK_CR2].size(); ++i) {
+                const ssb::TermItem &it = P.term[t][ssb::TK_CR2][i];
+                std::printf("%s[%d, %d]", i ? ", " : "", it.chain, it.chained);
+            }
         std::printf("]");
     }
     std::printf("]}\n");

@@ -187,3 +187,49 @@ def check_groups(d):
                     assert nxt[2:] != lead[2:], "a full group ends where its rows end"
                 i += n
 
+
+
+CHAIN_MAX, CHAIN_BLOCKS = 4, 2048   # kCr2ChainMax, kCr2ChainBlocks (ss_engine.h)
+
+
+@pytest.mark.parametrize("raises,bets", [(2, 2), (2, 3), (3, 2), (1, 1)])
+def test_two_opponent_chains(kinds_driver, raises, bets):
+    """Two-opponent groups on the same first-opponent row (same opponents)
+    form chains that one block computes: a head with chain = c is followed
+    by c group leaders marked chained, on its first opponent's row and
+    players; at most CHAIN_MAX groups per chain; followers carry no chain
+    marks; and a traverser's launch keeps at least CHAIN_BLOCKS working
+    blocks (small trees are not chained)."""
+    r = subprocess.run([kinds_driver, "3", "4", "200", "-1", "1", str(raises), str(bets)], check=True,
+                       capture_output=True, text=True)
+    d = json.loads(r.stdout)
+    assert d["rc"] == 0
+    chained_any = False
+    long_launch = False
+    for t in range(3):
+        items = d["groups"][t][1]          # TK_CR2: [gextra, follow, rows 0..2, players 0..2]
+        marks = d["chains"][t]             # [chain, chained]
+        assert len(items) == len(marks)
+        leads = [i for i, it in enumerate(items) if it[1] == 0]
+        for i, it in enumerate(items):
+            if it[1] == 1:
+                assert marks[i] == [0, 0], "followers carry no chain marks"
+        g = 0
+        blocks = 0
+        while g < len(leads):
+            head = leads[g]
+            assert marks[head][1] == 0, "a chain starts with an unchained leader"
+            c = marks[head][0]
+            assert 0 <= c <= CHAIN_MAX - 1
+            for m in leads[g + 1:g + 1 + c]:
+                assert marks[m] == [0, 1]
+                assert items[m][2] == items[head][2] and items[m][5:7] == items[head][5:7]
+            chained_any = chained_any or c > 0
+            blocks += 1
+            g += 1 + c
+        assert blocks >= min(len(leads), CHAIN_BLOCKS)
+        if len(leads) < 2 * CHAIN_BLOCKS:
+            assert blocks == len(leads), "a launch of fewer than two chain lengths' worth of groups is not chained"
+        long_launch = long_launch or len(leads) >= 2 * CHAIN_BLOCKS
+    assert chained_any == long_launch
+    assert long_launch == ((raises, bets) in ((2, 3), (3, 2)))
