@@ -105,6 +105,7 @@ constexpr int kTcWaitLimit = 1 << 22;
 
 __global__ void __launch_bounds__(kTermThreads, 4) k_term_cr2_tc(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                                   const TermItem *__restrict__ items, int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     const TermItem *I0 = items + blockIdx.x;
     if (I0->follow) return;   // written by the block of its group's first item

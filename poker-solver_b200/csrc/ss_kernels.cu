@@ -32,6 +32,36 @@ constexpr unsigned kFaultTcWait = 2u;    // k_term_cr2_tc: the MMA completion wa
 
 constexpr int MS = 52;  // shared-memory row stride of a 52x52 combo matrix (16-byte rows)
 
+// Programmatic dependent launch: the kernels of an iteration are launched
+// with it (pdl_launch), so a kernel's blocks are scheduled while the kernel
+// before it in the stream drains.  Every kernel starts here:
+// griddepcontrol.wait returns once the preceding kernel has completed and its
+// writes are visible (at once when there is no programmatic predecessor).
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... P, typename... A>
+cudaError_t pdl_launch(void (*kernel)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                       A &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+// pdl_launch(kernel, grid, block, shared bytes, stream, kernel arguments...),
+// returning its error from the enclosing function
+#define SSB_LAUNCH(...)                                      \
+    do {                                                     \
+        const cudaError_t le_ = pdl_launch(__VA_ARGS__);     \
+        if (le_ != cudaSuccess) return le_;                  \
+    } while (0)
+
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ float get(const float4 &v, int i) {
@@ -94,6 +124,7 @@ __device__ __forceinline__ bool retired(const DevCtx *ctxs, int sg) { return ctx
 __global__ void __launch_bounds__(kHandThreads) k_reach(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                         const ReachItem *__restrict__ items, int nchunk, int H,
                                                         int p) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
@@ -166,6 +197,7 @@ template <int S>
 __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                      const CfvItem *__restrict__ items, int nchunk, int Hl,
                                                      int trav) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const CfvItem I = items[it];
@@ -341,6 +373,7 @@ template <class T>
 __global__ void __launch_bounds__(kHandThreads) k_term_fill(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                             const TermItem *__restrict__ items, int nchunk,
                                                             int trav, int zero) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int h0 = (ch * kHandThreads + threadIdx.x) * 4;
@@ -456,6 +489,7 @@ constexpr size_t cr1_smem() {
 template <class T>
 __global__ void __launch_bounds__(kTermThreads) k_term_cr1_dup(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                            const TermItem *__restrict__ items, int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     Carve cv{smem};
     T *M = cv.take<T>(52 * MS);
@@ -814,6 +848,7 @@ __device__ __noinline__ int pair_count(const ulonglong2 *Bm, const Cr2Cnt *cnt, 
 template <class T>
 __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                               const TermItem *__restrict__ items, int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     const TermItem *I0 = items + blockIdx.x;
     // followers are written by their group's leader, chained groups by the chain's head
@@ -1048,6 +1083,7 @@ constexpr size_t cr1_gather_smem(int HS) {
 template <class T>
 __global__ void __launch_bounds__(kTermThreads) k_term_cr1(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                            const TermItem *__restrict__ items, int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     const TermItem *I0 = items + blockIdx.x;
     if (I0->follow) return;   // written by the block of its group's first item
@@ -1168,6 +1204,7 @@ constexpr size_t sd1_smem() {
 template <class T>
 __global__ void __launch_bounds__(kTermThreads) k_term_sd1(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                            const TermItem *__restrict__ items, int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     Carve cv{smem};
     T *Rr = cv.take<T>(1326);
@@ -1651,6 +1688,7 @@ template <class T>
 __global__ void __launch_bounds__(kTermThreads, 4) k_term_sd2(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                               const TermItem *__restrict__ items, int trav, int lgm,
                                                               const int2 *__restrict__ bmap) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     int it_idx, grp;
     if (bmap) {
@@ -1855,6 +1893,7 @@ template <class T>
 __global__ void __launch_bounds__(32 * kEnumWarps) k_term_enum(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                                const TermItem *__restrict__ items, int nchunk,
                                                                int trav) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1980,6 +2019,7 @@ template <class T>
 __global__ void __launch_bounds__(kTermThreads, 2) k_term_cr3(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                              const TermItem *__restrict__ items, int nchunk,
                                                              int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
@@ -2075,6 +2115,7 @@ template <class T>
 __global__ void __launch_bounds__(kTermThreads, 2) k_term_sd3(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                              const TermItem *__restrict__ items, int nchunk,
                                                              int trav) {
+    wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
@@ -2355,6 +2396,7 @@ __device__ __forceinline__ double avg_sigma(const float *avg, int di, int a, int
 __global__ void __launch_bounds__(128) k_br_reach(DevCtx c, const ReachItem *__restrict__ items, int nchunk,
                                                   int H, const float *__restrict__ avg,
                                                   const int *__restrict__ edge_di, int max_h) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
     if (h >= H) return;
@@ -2372,6 +2414,7 @@ __global__ void __launch_bounds__(128) k_br_reach(DevCtx c, const ReachItem *__r
 __global__ void __launch_bounds__(128) k_br_value(DevCtx c, const CfvItem *__restrict__ items, int nchunk,
                                                   int H, const float *__restrict__ avg,
                                                   const int *__restrict__ edge_di, int max_h, int mode) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int h = (blockIdx.x - it * nchunk) * blockDim.x + threadIdx.x;
     if (h >= H) return;
@@ -2401,6 +2444,7 @@ __global__ void __launch_bounds__(128) k_br_value(DevCtx c, const CfvItem *__res
 // reduction order.
 __global__ void __launch_bounds__(1024) k_br_root(DevCtx c, const int *__restrict__ rows, int n, int H,
                                                   int weight_row, int trav, int skip_blocked, double *out) {
+    wait_prior_grid();
     __shared__ double part[32];
     const size_t HS = static_cast<size_t>(c.HS);
     double acc = 0.0;
@@ -2425,6 +2469,7 @@ __global__ void __launch_bounds__(1024) k_br_root(DevCtx c, const int *__restric
 // that have left the batch return at once.
 __global__ void __launch_bounds__(128) k_avg_many(const DevCtx *__restrict__ ctxs,
                                                   const AvgItem *__restrict__ items, int nchunk) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const AvgItem I = items[it];
     if (!ctxs[I.sg].live) return;
@@ -2453,6 +2498,7 @@ __global__ void __launch_bounds__(128) k_avg_many(const DevCtx *__restrict__ ctx
 
 __global__ void __launch_bounds__(128) k_br_reach_many(const DevCtx *__restrict__ ctxs,
                                                        const ReachItem *__restrict__ items, int nchunk, int p) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const ReachItem I = items[it];
     if (!ctxs[I.sg].live) return;
@@ -2469,6 +2515,7 @@ __global__ void __launch_bounds__(128) k_br_reach_many(const DevCtx *__restrict_
 __global__ void __launch_bounds__(128) k_br_value_many(const DevCtx *__restrict__ ctxs,
                                                        const CfvItem *__restrict__ items, int nchunk, int trav,
                                                        int mode) {
+    wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const CfvItem I = items[it];
     if (!ctxs[I.sg].live) return;
@@ -2497,6 +2544,7 @@ __global__ void __launch_bounds__(128) k_br_value_many(const DevCtx *__restrict_
 // one block per item, same fixed reduction order as k_br_root
 __global__ void __launch_bounds__(1024) k_br_root_many(const DevCtx *__restrict__ ctxs,
                                                        const RootItem *__restrict__ items, double *out) {
+    wait_prior_grid();
     __shared__ double part[32];
     const RootItem I = items[blockIdx.x];
     if (!ctxs[I.sg].live) return;
@@ -2522,6 +2570,7 @@ __global__ void __launch_bounds__(1024) k_br_root_many(const DevCtx *__restrict_
 
 // batched form: advance the iteration counter of every listed subgame
 __global__ void k_bump_many(const DevCtx *__restrict__ ctxs, const int *__restrict__ sgs, int n) {
+    wait_prior_grid();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n && ctxs[sgs[i]].live) *const_cast<int *>(ctxs[sgs[i]].iter) += 1;
 }
@@ -2530,6 +2579,7 @@ __global__ void k_bump_many(const DevCtx *__restrict__ ctxs, const int *__restri
 // of every listed subgame, one block per subgame, into its ctx.snap
 __global__ void __launch_bounds__(128) k_snapshot_many(const DevCtx *__restrict__ ctxs,
                                                        const int *__restrict__ sgs) {
+    wait_prior_grid();
     const DevCtx &c = ctxs[sgs[blockIdx.x]];
     if (!c.live) return;
     const int H = c.H[c.root_player];
@@ -2542,11 +2592,13 @@ __global__ void __launch_bounds__(128) k_snapshot_many(const DevCtx *__restrict_
     }
 }
 
-__global__ void k_bump(int *iter) { *iter += 1; }
+__global__ void k_bump(int *iter) {
+    wait_prior_grid(); *iter += 1; }
 
 // out[h] = sum over rows of val[row][h]
 __global__ void __launch_bounds__(kHandThreads) k_sum_rows(DevCtx c, const int *__restrict__ rows, int n,
                                                            float *out, int H) {
+    wait_prior_grid();
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= H) return;
     float s = 0.f;
@@ -2557,6 +2609,7 @@ __global__ void __launch_bounds__(kHandThreads) k_sum_rows(DevCtx c, const int *
 // regret-matched (and frozen) strategy of one node, [na][H] (street_solve.cu:1564-1573)
 __global__ void __launch_bounds__(kHandThreads) k_root_strategy(DevCtx c, int fe, int na, int frozen,
                                                                 int H, float *out) {
+    wait_prior_grid();
     const int h0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     if (h0 >= H) return;
     float r[SS_MAX_ACTIONS][4], sig[SS_MAX_ACTIONS][4];
@@ -2572,6 +2625,7 @@ __global__ void __launch_bounds__(128) k_avg_strategy(DevCtx c, const int *__res
                                                       const int *__restrict__ dec_na,
                                                       const int *__restrict__ dec_player, int nchunk,
                                                       int max_h, float *out) {
+    wait_prior_grid();
     const int di = blockIdx.x / nchunk;
     const int h = (blockIdx.x - di * nchunk) * blockDim.x + threadIdx.x;
     if (h >= max_h) return;
@@ -2635,7 +2689,7 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
                          const DevCtx *ctxs, int player) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = chunks(H);
-    k_reach<<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, H, player);
+    SSB_LAUNCH(k_reach, n * nc, kHandThreads, 0, s, c, ctxs, items, nc, H, player);
     return cudaGetLastError();
 }
 
@@ -2646,12 +2700,12 @@ cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long,
     const int n_short = n - n_long;
     if (n_short > 0) {
         const int nc = (H + 2 * kCfvThreads - 1) / (2 * kCfvThreads);
-        k_cfv<1><<<n_short * nc, kCfvThreads, 0, s>>>(c, ctxs, items, nc, H, trav);
+        SSB_LAUNCH(k_cfv<1>, n_short * nc, kCfvThreads, 0, s, c, ctxs, items, nc, H, trav);
     }
     if (n_long > 0) {
         const int nc = (H + 63) / 64;
         static_assert(32 * kCfvSplit == kCfvThreads, "the split form fills one block of kCfvThreads");
-        k_cfv<kCfvSplit><<<n_long * nc, kCfvThreads, 0, s>>>(c, ctxs, items + n_short, nc, H, trav);
+        SSB_LAUNCH(k_cfv<kCfvSplit>, n_long * nc, kCfvThreads, 0, s, c, ctxs, items + n_short, nc, H, trav);
     }
     return cudaGetLastError();
 }
@@ -2665,7 +2719,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
         case TK_ZERO:
         case TK_LEAF0: {
             const int nc = chunks(c.HS);
-            k_term_fill<T><<<n * nc, kHandThreads, 0, s>>>(c, ctxs, items, nc, trav, kind == TK_ZERO);
+            SSB_LAUNCH(k_term_fill<T>, n * nc, kHandThreads, 0, s, c, ctxs, items, nc, trav, kind == TK_ZERO);
             break;
         }
         case TK_CR1: {
@@ -2674,11 +2728,11 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
                 e = cudaFuncSetAttribute(k_term_cr1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(cr1_gather_smem<T>(kMaxHS)));
             if (e != cudaSuccess) return e;
-            k_term_cr1<T><<<n, kTermThreads, sm, s>>>(c, ctxs, items, trav);
+            SSB_LAUNCH(k_term_cr1<T>, n, kTermThreads, sm, s, c, ctxs, items, trav);
             break;
         }
         case TK_CR1D:
-            k_term_cr1_dup<T><<<n, kTermThreads, cr1_smem<T>(), s>>>(c, ctxs, items, trav);
+            SSB_LAUNCH(k_term_cr1_dup<T>, n, kTermThreads, cr1_smem<T>(), s, c, ctxs, items, trav);
             break;
         case TK_CR2: {
             // c.HS: the row stride (the largest of a batch); the staging of two
@@ -2689,7 +2743,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
                     e = cudaFuncSetAttribute(k_term_cr2_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(cr2_tc_smem(kMaxHS)));
                     if (e != cudaSuccess) return e;
-                    k_term_cr2_tc<<<n, kTermThreads, cr2_tc_smem(c.HS), s>>>(c, ctxs, items, trav);
+                    SSB_LAUNCH(k_term_cr2_tc, n, kTermThreads, cr2_tc_smem(c.HS), s, c, ctxs, items, trav);
                     break;
                 }
             }
@@ -2698,7 +2752,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
                 e = cudaFuncSetAttribute(k_term_cr2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(cr2_smem<T>(kMaxHS)));
             if (e != cudaSuccess) return e;
-            k_term_cr2<T><<<n, kTermThreads, sm, s>>>(c, ctxs, items, trav);
+            SSB_LAUNCH(k_term_cr2<T>, n, kTermThreads, sm, s, c, ctxs, items, trav);
             break;
         }
         case TK_SD1:
@@ -2706,7 +2760,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
                 e = cudaFuncSetAttribute(k_term_sd1<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(sd1_smem<T>()));
             if (e != cudaSuccess) return e;
-            k_term_sd1<T><<<n, kTermThreads, sd1_smem<T>(), s>>>(c, ctxs, items, trav);
+            SSB_LAUNCH(k_term_sd1<T>, n, kTermThreads, sd1_smem<T>(), s, c, ctxs, items, trav);
             break;
         case TK_SD2: {
             // runs per block: about two waves of four blocks per SM at most
@@ -2714,14 +2768,14 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             const size_t sm = sd2_smem<T>(c.sd_span[lgm], c.ncomb);
             e = cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
             if (e != cudaSuccess) return e;
-            k_term_sd2<T><<<n * (kSd2Chunks >> lgm), kTermThreads, sm, s>>>(c, ctxs, items, trav, lgm, nullptr);
+            SSB_LAUNCH(k_term_sd2<T>, n * (kSd2Chunks >> lgm), kTermThreads, sm, s, c, ctxs, items, trav, lgm, nullptr);
             break;
         }
         case TK_ENUM: {
             // blocks per terminal: one per 4 hands, at most 16 (they stride
             // over a larger range; a batch's c.HS is its largest row stride)
             const int nc = std::min((c.HS + kEnumWarps - 1) / kEnumWarps, 16);
-            k_term_enum<T><<<n * nc, 32 * kEnumWarps, 0, s>>>(c, ctxs, items, nc, trav);
+            SSB_LAUNCH(k_term_enum<T>, n * nc, 32 * kEnumWarps, 0, s, c, ctxs, items, nc, trav);
             break;
         }
         case TK_SD3: {
@@ -2731,7 +2785,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             e = cudaFuncSetAttribute(k_term_sd3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(sd3_smem(kMaxHS)));
             if (e != cudaSuccess) return e;
-            k_term_sd3<T><<<n * nc, kTermThreads, sd3_smem(c.HS), s>>>(c, ctxs, items, nc, trav);
+            SSB_LAUNCH(k_term_sd3<T>, n * nc, kTermThreads, sd3_smem(c.HS), s, c, ctxs, items, nc, trav);
             break;
         }
         case TK_CR3: {
@@ -2740,7 +2794,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
             e = cudaFuncSetAttribute(k_term_cr3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(cr3_smem(kMaxHS)));
             if (e != cudaSuccess) return e;
-            k_term_cr3<T><<<n * nc, kTermThreads, cr3_smem(c.HS), s>>>(c, ctxs, items, nc, trav);
+            SSB_LAUNCH(k_term_cr3<T>, n * nc, kTermThreads, cr3_smem(c.HS), s, c, ctxs, items, nc, trav);
             break;
         }
         default:
@@ -2762,7 +2816,7 @@ cudaError_t launch_sd2_mapped_t(const DevCtx &c, const TermItem *items, const in
     cudaError_t e =
         cudaFuncSetAttribute(k_term_sd2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm));
     if (e != cudaSuccess) return e;
-    k_term_sd2<T><<<nblocks, kTermThreads, sm, s>>>(c, ctxs, items, trav, 0, bmap);
+    SSB_LAUNCH(k_term_sd2<T>, nblocks, kTermThreads, sm, s, c, ctxs, items, trav, 0, bmap);
     return cudaGetLastError();
 }
 
@@ -2780,7 +2834,7 @@ cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, 
 cudaError_t launch_avg_many(const DevCtx *ctxs, const AvgItem *items, int n, int max_h, cudaStream_t s) {
     if (n <= 0 || max_h <= 0) return cudaSuccess;
     const int nc = (max_h + 127) / 128;
-    k_avg_many<<<n * nc, 128, 0, s>>>(ctxs, items, nc);
+    SSB_LAUNCH(k_avg_many, n * nc, 128, 0, s, ctxs, items, nc);
     return cudaGetLastError();
 }
 
@@ -2788,7 +2842,7 @@ cudaError_t launch_br_reach_many(const DevCtx *ctxs, const ReachItem *items, int
                                  cudaStream_t s) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = (H + 127) / 128;
-    k_br_reach_many<<<n * nc, 128, 0, s>>>(ctxs, items, nc, player);
+    SSB_LAUNCH(k_br_reach_many, n * nc, 128, 0, s, ctxs, items, nc, player);
     return cudaGetLastError();
 }
 
@@ -2796,33 +2850,33 @@ cudaError_t launch_br_value_many(const DevCtx *ctxs, const CfvItem *items, int n
                                  cudaStream_t s) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = (H + 127) / 128;
-    k_br_value_many<<<n * nc, 128, 0, s>>>(ctxs, items, nc, trav, mode);
+    SSB_LAUNCH(k_br_value_many, n * nc, 128, 0, s, ctxs, items, nc, trav, mode);
     return cudaGetLastError();
 }
 
 cudaError_t launch_br_root_many(const DevCtx *ctxs, const RootItem *items, int n, double *out, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    k_br_root_many<<<n, 1024, 0, s>>>(ctxs, items, out);
+    SSB_LAUNCH(k_br_root_many, n, 1024, 0, s, ctxs, items, out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bump(int *iter, cudaStream_t s) {
-    k_bump<<<1, 1, 0, s>>>(iter);
+    SSB_LAUNCH(k_bump, 1, 1, 0, s, iter);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sum_rows(const DevCtx &c, const int *rows, int n, float *out, int H,
                             cudaStream_t s) {
     if (H <= 0) return cudaSuccess;
-    k_sum_rows<<<(H + kHandThreads - 1) / kHandThreads, kHandThreads, 0, s>>>(c, rows, n, out, H);
+    SSB_LAUNCH(k_sum_rows, (H + kHandThreads - 1) / kHandThreads, kHandThreads, 0, s, c, rows, n, out, H);
     return cudaGetLastError();
 }
 
 cudaError_t launch_root_strategy(const DevCtx &c, int first_edge, int na, int frozen, int H,
                                  float *out, cudaStream_t s) {
     if (H <= 0) return cudaSuccess;
-    k_root_strategy<<<(H + kHandsPerBlock - 1) / kHandsPerBlock, kHandThreads, 0, s>>>(
-        c, first_edge, na, frozen, H, out);
+    SSB_LAUNCH(k_root_strategy, (H + kHandsPerBlock - 1) / kHandsPerBlock, kHandThreads, 0, s,
+               c, first_edge, na, frozen, H, out);
     return cudaGetLastError();
 }
 
@@ -2831,7 +2885,7 @@ cudaError_t launch_avg_strategy(const DevCtx &c, const int *dec_fe, const int *d
                                 cudaStream_t s) {
     if (num_dec <= 0) return cudaSuccess;
     const int nc = (max_h + 127) / 128;
-    k_avg_strategy<<<num_dec * nc, 128, 0, s>>>(c, dec_fe, dec_na, dec_player, nc, max_h, out);
+    SSB_LAUNCH(k_avg_strategy, num_dec * nc, 128, 0, s, c, dec_fe, dec_na, dec_player, nc, max_h, out);
     return cudaGetLastError();
 }
 
@@ -2839,7 +2893,7 @@ cudaError_t launch_br_reach(const DevCtx &c, const ReachItem *items, int n, int 
                             const int *edge_di, int max_h, cudaStream_t s) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = (H + 127) / 128;
-    k_br_reach<<<n * nc, 128, 0, s>>>(c, items, nc, H, avg, edge_di, max_h);
+    SSB_LAUNCH(k_br_reach, n * nc, 128, 0, s, c, items, nc, H, avg, edge_di, max_h);
     return cudaGetLastError();
 }
 
@@ -2847,25 +2901,25 @@ cudaError_t launch_br_value(const DevCtx &c, const CfvItem *items, int n, int H,
                             const int *edge_di, int max_h, int mode, cudaStream_t s) {
     if (n <= 0 || H <= 0) return cudaSuccess;
     const int nc = (H + 127) / 128;
-    k_br_value<<<n * nc, 128, 0, s>>>(c, items, nc, H, avg, edge_di, max_h, mode);
+    SSB_LAUNCH(k_br_value, n * nc, 128, 0, s, c, items, nc, H, avg, edge_di, max_h, mode);
     return cudaGetLastError();
 }
 
 cudaError_t launch_br_root(const DevCtx &c, const int *rows, int n, int H, int weight_row, int trav,
                            int skip_blocked, double *out, cudaStream_t s) {
-    k_br_root<<<1, 1024, 0, s>>>(c, rows, n, H, weight_row, trav, skip_blocked, out);
+    SSB_LAUNCH(k_br_root, 1, 1024, 0, s, c, rows, n, H, weight_row, trav, skip_blocked, out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bump_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    k_bump_many<<<(n + 127) / 128, 128, 0, s>>>(ctxs, sgs, n);
+    SSB_LAUNCH(k_bump_many, (n + 127) / 128, 128, 0, s, ctxs, sgs, n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_snapshot_many(const DevCtx *ctxs, const int *sgs, int n, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
-    k_snapshot_many<<<n, 128, 0, s>>>(ctxs, sgs);
+    SSB_LAUNCH(k_snapshot_many, n, 128, 0, s, ctxs, sgs);
     return cudaGetLastError();
 }
 
