@@ -248,7 +248,8 @@ def flow_bytes_per_iteration(td, H):
     return total
 
 
-KERNEL_SOURCES = ("ss_kernels.cu", "ss_cr3.cuh", "ss_rank.cuh", "ss_kernels.h")
+KERNEL_SOURCES = ("ss_kernels.cu", "ss_cr3.cuh", "ss_cr2_tc.cuh", "ss_rank.cuh", "ss_kernels.h", "ss_engine.h",
+                  "ss_plan.cpp")
 # kernel name prefix -> profile class of ss_session_profile
 NCU_CLASSES = [("k_term_cr2", "term_cr2"), ("k_term_cr1", "term_cr1"), ("k_term_sd", "term_sd"),
                ("k_term_enum", "term_enum"), ("k_term_cr3", "term_enum"), ("k_term_fill", "term_fill"),

@@ -210,6 +210,7 @@ int build_plan(const FSTreeData &td, FsPlan *out) {
             it.frozen = -1;
             it.node = x;
             it.scale = static_cast<float>(w[x]);
+            inline_frontier(it, P.fr_off, P.fr_items);
             P.cfv_levels[t][h].push_back(it);
         }
         P.cfv_nlong[t].assign(P.cfv_levels[t].size(), 0);

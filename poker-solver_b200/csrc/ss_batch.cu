@@ -178,6 +178,9 @@ class Batch {
         int map_blocks = 0;
         int map_lg = 0;
         int cr2_form = -1;  // two-opponent terminals: 1 tensor-core form, 0 mma.sync form
+        // grouped terminal kinds: the items that start work, one block each
+        size_t heads_off = 0;
+        int n_heads = 0;
     };
     DevCtx *dctx = nullptr;
     char *dlists = nullptr;
@@ -199,17 +202,20 @@ class Batch {
                     return launch_sd2_mapped(cmax, reinterpret_cast<const TermItem *>(dlists + L.off),
                                              reinterpret_cast<const int2 *>(dlists + L.map_off), L.map_blocks,
                                              L.map_lg, L.t, stream, dctx, false);
-                if (L.cr2_form >= 0) {
-                    // the launch context picks the form: a dense deck of 48 and no
-                    // repeated combo for the tensor-core one, no deck for the other
-                    DevCtx cl = cmax;
-                    cl.deck = L.cr2_form == 1 ? 48 : 0;
-                    for (int p = 0; p < SS_MAX_PLAYERS; ++p) cl.dup[p] = 0;
-                    return launch_terms(cl, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
-                                        stream, dctx);
+                {
+                    const int *heads = L.n_heads > 0 ? reinterpret_cast<const int *>(dlists + L.heads_off) : nullptr;
+                    if (L.cr2_form >= 0) {
+                        // the launch context picks the form: a dense deck of 48 and no
+                        // repeated combo for the tensor-core one, no deck for the other
+                        DevCtx cl = cmax;
+                        cl.deck = L.cr2_form == 1 ? 48 : 0;
+                        for (int p = 0; p < SS_MAX_PLAYERS; ++p) cl.dup[p] = 0;
+                        return launch_terms(cl, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n,
+                                            L.t, stream, dctx, heads, L.n_heads);
+                    }
+                    return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
+                                        stream, dctx, heads, L.n_heads);
                 }
-                return launch_terms(cmax, L.kind, reinterpret_cast<const TermItem *>(dlists + L.off), L.n, L.t,
-                                    stream, dctx);
             case L_CFV:
                 return launch_cfv(cmax, reinterpret_cast<const CfvItem *>(dlists + L.off), L.n, L.kind, L.H, stream,
                                   dctx, L.t);
@@ -308,6 +314,13 @@ class Batch {
         auto term_launch = [&](int type, int k, int t, const std::vector<TermItem> &items) {
             Launch L{type, k, t, put(items.data(), items.size() * sizeof(TermItem)), static_cast<int>(items.size()),
                      0};
+            if (type == L_TERM && k == TK_CR2) {
+                std::vector<int> heads;
+                for (size_t i = 0; i < items.size(); ++i)
+                    if (!items[i].follow && !items[i].chained) heads.push_back(static_cast<int>(i));
+                L.heads_off = put(heads.data(), heads.size() * sizeof(int));
+                L.n_heads = static_cast<int>(heads.size());
+            }
             if (k == TK_SD2) {
                 std::vector<int2> bmap;
                 for (size_t i = 0; i < items.size(); ++i) {

@@ -195,6 +195,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
 
     // ---- static tables and the minimum bytes of every launch ------------
     Blob b;
+    size_t o_heads[SS_MAX_PLAYERS][TK_COUNT] = {};
     size_t o_reach[SS_MAX_PLAYERS], o_cfv[SS_MAX_PLAYERS], o_term[SS_MAX_PLAYERS][TK_COUNT],
         o_rootfr[SS_MAX_PLAYERS];
     for (int p = 0; p < np; ++p) {
@@ -229,6 +230,7 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
             }
             term_bytes[p][k] = by;
             o_term[p][k] = b.add(P.term[p][k]);
+            if (!P.term_heads[p][k].empty()) o_heads[p][k] = b.add(P.term_heads[p][k]);
         }
         o_rootfr[p] = b.add(P.root_fr[p]);
     }
@@ -260,8 +262,11 @@ int Session::init(const Problem &pb, const SolveConfig &cfg) {
     for (int p = 0; p < np; ++p) {
         reach_items[p] = reinterpret_cast<const ReachItem *>(dbase + o_reach[p]);
         cfv_items[p] = reinterpret_cast<const CfvItem *>(dbase + o_cfv[p]);
-        for (int k = 0; k < TK_COUNT; ++k)
+        for (int k = 0; k < TK_COUNT; ++k) {
             term_items[p][k] = reinterpret_cast<const TermItem *>(dbase + o_term[p][k]);
+            term_heads[p][k] = P.term_heads[p][k].empty() ? nullptr
+                                                          : reinterpret_cast<const int *>(dbase + o_heads[p][k]);
+        }
         root_fr[p] = reinterpret_cast<const int *>(dbase + o_rootfr[p]);
     }
     dec_fe = reinterpret_cast<const int *>(dbase + o_dfe);

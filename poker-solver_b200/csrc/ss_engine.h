@@ -89,6 +89,10 @@ struct alignas(16) ReachItem {
 
 // Bottom-up value and regret update at one traverser decision node; the value
 // of edge e is the sum of val[] over frontier(e) = fr_items[fr_off[e] .. fr_off[e+1]).
+// A frontier of at most kCfvInline rows in all is also held in the item
+// (nfr > 0), so the value kernel reads the rows without the two dependent
+// index loads (fr_off, then fr_items).
+constexpr int kCfvInline = 8;
 struct alignas(16) CfvItem {
     int first_edge;
     int na;
@@ -96,8 +100,12 @@ struct alignas(16) CfvItem {
     int node;
     int sg = 0;               // subgame of a batch (0 for a single subgame)
     float scale = 1.f;        // the node's value row is stored times this (chance weights; 1 on one street)
-    int pad_[2] = {0, 0};
+    int nfr = 0;              // inline frontier: its number of rows (0: not inline)
+    int fr_bnd = 0;           // inline frontier: end of edge a's rows at bits 4a .. 4a+3 (15 past the last edge)
+    int fr[kCfvInline] = {};  // inline frontier: the rows of all edges, in order
 };
+// fills the inline frontier of it when the frontier is short enough
+void inline_frontier(CfvItem &it, const std::vector<int> &fr_off, const std::vector<int> &fr_items);
 
 // A value/regret item whose edges' frontiers hold at least this many rows in
 // total is long: several warps share each of its hand chunks.
@@ -222,6 +230,12 @@ struct Plan {
     // with long frontiers come last, cfv_nlong of them
     std::vector<std::vector<CfvItem>> cfv_levels[SS_MAX_PLAYERS];
     std::vector<int> cfv_nlong[SS_MAX_PLAYERS];
+    // two-opponent terminals (TK_CR2): the items that start work (group leaders
+    // that no chain head computes); the launch gets one block each.  (One block
+    // per item, as for every other kind, keeps the one-opponent launches
+    // faster: their blocks are short, and reading the head first would add a
+    // memory round trip to each.)
+    std::vector<int> term_heads[SS_MAX_PLAYERS][TK_COUNT];
     std::vector<int> fr_off;           // [E + 1]
     std::vector<int> fr_items;         // val rows (= node ids)
     std::vector<int> root_fr[SS_MAX_PLAYERS];

@@ -15,6 +15,7 @@
 #include "ss_kernels.h"
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdlib>
 #include "ss_cr3.cuh"
 
@@ -193,6 +194,20 @@ __device__ __forceinline__ CfvView cfv_view(const DevCtx &c, int H) {
 }
 
 
+// the first 32 bytes of a CfvItem (the inline frontier rows follow), read
+// with two 16-byte loads
+struct CfvHead {
+    int first_edge, na, frozen, node, sg;
+    float scale;
+    int nfr, fr_bnd;
+};
+static_assert(sizeof(CfvItem) == 64 && offsetof(CfvItem, nfr) == 24 && offsetof(CfvItem, fr) == 32,
+              "CfvItem layout read by cfv_head");
+__device__ __forceinline__ CfvHead cfv_head(const CfvItem *p) {
+    const int4 a = __ldg(reinterpret_cast<const int4 *>(p)), b = __ldg(reinterpret_cast<const int4 *>(p) + 1);
+    return CfvHead{a.x, a.y, a.z, a.w, b.x, __int_as_float(b.y), b.z, b.w};
+}
+
 template <int S>
 __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                      const CfvItem *__restrict__ items, int nchunk, int Hl,
@@ -200,7 +215,7 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
     wait_prior_grid();
     const int it = blockIdx.x / nchunk;
     const int ch = blockIdx.x - it * nchunk;
-    const CfvItem I = items[it];
+    const CfvHead I = cfv_head(items + it);
     if (retired(ctxs, I.sg)) return;
     const CfvView V = ctxs ? cfv_view(ctxs[I.sg], ctxs[I.sg].H[trav]) : cfv_view(c0, Hl);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -226,29 +241,56 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
 #pragma unroll
     for (int a = 0; a < SS_MAX_ACTIONS; ++a) ev[a] = make_float2(0.f, 0.f);
     if constexpr (S == 1) {
-        // the frontiers of all edges are one contiguous run of rows: walk it
-        // eight rows at a time across edge boundaries (short frontiers, one
-        // row per edge at the lowest level, would otherwise leave one load in
-        // flight); each row adds to its edge in row order
-        const int fe = I.first_edge;
-        int bnd[SS_MAX_ACTIONS];
+        if (I.nfr > 0) {
+            // a short frontier held in the item: its rows load at once, with
+            // no index loads before them; each row adds to its edge in row order
+            const unsigned bnd = static_cast<unsigned>(I.fr_bnd);
+            static_assert(kCfvInline == 8, "two 16-byte loads of inline rows");
+            const int4 f0 = __ldg(reinterpret_cast<const int4 *>(items + it) + 2);
+            const int4 f1 = __ldg(reinterpret_cast<const int4 *>(items + it) + 3);
+            const int rows[kCfvInline] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
+            float2 x[kCfvInline];
 #pragma unroll
-        for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
-        const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
-        for (int k = k0; k < kend; k += 8) {
-            float2 x[8];
+            for (int i = 0; i < kCfvInline; ++i)
+                x[i] = i < I.nfr ? ld2(val + static_cast<size_t>(rows[i]) * HS) : make_float2(0.f, 0.f);
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-                x[i] = k + i < kend ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS) : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (k + i < kend) {
+            for (int i = 0; i < kCfvInline; ++i) {
+                if (i < I.nfr) {
                     int e = 0;
 #pragma unroll
-                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
+                    for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a)
+                        e += i >= static_cast<int>((bnd >> (4 * a)) & 15u) ? 1 : 0;
 #pragma unroll
                     for (int a = 0; a < SS_MAX_ACTIONS; ++a)
                         if (e == a) add2(ev[a], x[i]);
+                }
+            }
+        } else {
+            // the frontiers of all edges are one contiguous run of rows: walk
+            // it eight rows at a time across edge boundaries (short frontiers,
+            // one row per edge at the lowest level, would otherwise leave one
+            // load in flight); each row adds to its edge in row order
+            const int fe = I.first_edge;
+            int bnd[SS_MAX_ACTIONS];
+#pragma unroll
+            for (int a = 0; a < SS_MAX_ACTIONS; ++a) bnd[a] = a < I.na ? V.fr_off[fe + a + 1] : 0x7fffffff;
+            const int k0 = V.fr_off[fe], kend = V.fr_off[fe + I.na];
+            for (int k = k0; k < kend; k += 8) {
+                float2 x[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    x[i] = k + i < kend ? ld2(val + static_cast<size_t>(__ldg(fr + k + i)) * HS)
+                                        : make_float2(0.f, 0.f);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (k + i < kend) {
+                        int e = 0;
+#pragma unroll
+                        for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a) e += k + i >= bnd[a] ? 1 : 0;
+#pragma unroll
+                        for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+                            if (e == a) add2(ev[a], x[i]);
+                    }
                 }
             }
         }
@@ -847,10 +889,11 @@ __device__ __noinline__ int pair_count(const ulonglong2 *Bm, const Cr2Cnt *cnt, 
 // and block scalars; per-hand mass and one output row per terminal.
 template <class T>
 __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
-                                                              const TermItem *__restrict__ items, int trav) {
+                                                              const TermItem *__restrict__ items,
+                                                              const int *__restrict__ heads, int trav) {
     wait_prior_grid();
     extern __shared__ __align__(16) char smem[];
-    const TermItem *I0 = items + blockIdx.x;
+    const TermItem *I0 = items + (heads ? __ldg(heads + blockIdx.x) : static_cast<int>(blockIdx.x));
     // followers are written by their group's leader, chained groups by the chain's head
     if (I0->follow || I0->chained) return;
     if (retired(ctxs, I0->sg)) return;
@@ -2712,8 +2755,8 @@ cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long,
 
 template <class T>
 cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                           cudaStream_t s, const DevCtx *ctxs) {
-    if (n <= 0) return cudaSuccess;
+                           cudaStream_t s, const DevCtx *ctxs, const int *heads = nullptr, int n_heads = 0) {
+    if (n <= 0 || (heads && n_heads <= 0)) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     switch (kind) {
         case TK_ZERO:
@@ -2752,7 +2795,7 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
                 e = cudaFuncSetAttribute(k_term_cr2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(cr2_smem<T>(kMaxHS)));
             if (e != cudaSuccess) return e;
-            SSB_LAUNCH(k_term_cr2<T>, n, kTermThreads, sm, s, c, ctxs, items, trav);
+            SSB_LAUNCH(k_term_cr2<T>, heads ? n_heads : n, kTermThreads, sm, s, c, ctxs, items, heads, trav);
             break;
         }
         case TK_SD1:
@@ -2804,8 +2847,8 @@ cudaError_t launch_terms_t(const DevCtx &c, int kind, const TermItem *items, int
 }
 
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                         cudaStream_t s, const DevCtx *ctxs) {
-    return launch_terms_t<float>(c, kind, items, n, trav, s, ctxs);
+                         cudaStream_t s, const DevCtx *ctxs, const int *heads, int n_heads) {
+    return launch_terms_t<float>(c, kind, items, n, trav, s, ctxs, heads, n_heads);
 }
 
 template <class T>

@@ -92,8 +92,12 @@ cudaError_t launch_reach(const DevCtx &c, const ReachItem *items, int n, int H, 
 // The last n_long items (long frontiers) run with kCfvSplit warps per hand chunk.
 cudaError_t launch_cfv(const DevCtx &c, const CfvItem *items, int n, int n_long, int H, cudaStream_t s,
                        const DevCtx *ctxs = nullptr, int trav = -1);
+// heads (optional, TK_CR2): the n_heads items that start work (TermItem
+// groups and chains); the launch then has one block per head instead of one
+// per item (the tensor-core two-opponent form takes every item)
 cudaError_t launch_terms(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
-                         cudaStream_t s, const DevCtx *ctxs = nullptr);
+                         cudaStream_t s, const DevCtx *ctxs = nullptr, const int *heads = nullptr,
+                         int n_heads = 0);
 cudaError_t launch_terms_fp64(const DevCtx &c, int kind, const TermItem *items, int n, int trav,
                               cudaStream_t s, const DevCtx *ctxs = nullptr);
 // Three-way showdowns of many subgames (batches): block b sweeps run group

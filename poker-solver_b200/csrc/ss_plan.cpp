@@ -100,6 +100,19 @@ bool validate(const Problem &pb, Plan &P) {
 
 }  // namespace
 
+void inline_frontier(CfvItem &it, const std::vector<int> &fr_off, const std::vector<int> &fr_items) {
+    const int k0 = fr_off[it.first_edge], n = fr_off[it.first_edge + it.na] - k0;
+    it.nfr = 0;
+    it.fr_bnd = 0;
+    if (n <= 0 || n > kCfvInline || it.na > SS_MAX_ACTIONS) return;
+    unsigned bnd = 0;
+    for (int a = 0; a < SS_MAX_ACTIONS; ++a)
+        bnd |= static_cast<unsigned>(a < it.na ? fr_off[it.first_edge + a + 1] - k0 : 15) << (4 * a);
+    for (int i = 0; i < n; ++i) it.fr[i] = fr_items[k0 + i];
+    it.nfr = n;
+    it.fr_bnd = static_cast<int>(bnd);
+}
+
 int build_plan(const Problem &pb, Plan *out) {
     Plan &P = *out;
     if (!validate(pb, P)) return SS_ERR_INVALID;
@@ -240,6 +253,7 @@ int build_plan(const Problem &pb, Plan *out) {
             it.na = nd[x].num_children;
             it.frozen = frozen_of(x);
             it.node = x;
+            inline_frontier(it, P.fr_off, P.fr_items);
             P.cfv_levels[t][h].push_back(it);
         }
         P.cfv_nlong[t].assign(P.cfv_levels[t].size(), 0);
@@ -392,6 +406,14 @@ int build_plan(const Problem &pb, Plan *out) {
             g = e;
         }
     }
+    for (int t = 0; t < np; ++t)
+        for (int k = 0; k < TK_COUNT; ++k) {
+            P.term_heads[t][k].clear();
+            if (k != TK_CR2) continue;
+            const std::vector<TermItem> &v = P.term[t][k];
+            for (size_t i = 0; i < v.size(); ++i)
+                if (!v[i].follow && !v[i].chained) P.term_heads[t][k].push_back(static_cast<int>(i));
+        }
 
     // showdown tables: every non-board combo ranked on the 5-card board
     P.ncomb = 0;

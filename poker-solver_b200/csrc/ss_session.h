@@ -56,6 +56,7 @@ class Session {
     const CfvItem *cfv_items[SS_MAX_PLAYERS] = {};
     std::vector<std::pair<int, int>> cfv_lv[SS_MAX_PLAYERS];
     const TermItem *term_items[SS_MAX_PLAYERS][TK_COUNT] = {};
+    const int *term_heads[SS_MAX_PLAYERS][TK_COUNT] = {};   // null for kinds without P.term_heads
     const int *root_fr[SS_MAX_PLAYERS] = {};
     const int *dec_fe = nullptr, *dec_na = nullptr, *dec_pl = nullptr;
     std::vector<int> dec_na_host, dec_player_host;   // per decision node (index order): actions, acting player
@@ -135,6 +136,12 @@ class Session {
         return cudaSuccess;
     }
 
+    // traverser t's terminals of kind k (grouped kinds: one block per head)
+    cudaError_t terms(int t, int k, cudaStream_t s) {
+        return launch_terms(c, k, term_items[t][k], static_cast<int>(P.term[t][k].size()), t, s, nullptr,
+                            term_heads[t][k], static_cast<int>(P.term_heads[t][k].size()));
+    }
+
     cudaError_t pass(int t, bool snapshot_root) {
         cudaError_t e = cudaSuccess;
         if (snapshot_root) {
@@ -156,8 +163,7 @@ class Session {
             for (int i = 0; i < nk; ++i) {
                 const int k = kinds[i];
                 e = mark(term_class(k), term_bytes[t][k], static_cast<int>(P.term[t][k].size()));
-                if (e == cudaSuccess)
-                    e = launch_terms(c, k, term_items[t][k], static_cast<int>(P.term[t][k].size()), t, stream);
+                if (e == cudaSuccess) e = terms(t, k, stream);
                 if (e != cudaSuccess) return e;
             }
         } else {
@@ -166,13 +172,10 @@ class Session {
                 const int k = kinds[i];
                 if (k == main_k) continue;
                 e = cudaStreamWaitEvent(side[k], ev_fork, 0);
-                if (e == cudaSuccess)
-                    e = launch_terms(c, k, term_items[t][k], static_cast<int>(P.term[t][k].size()), t, side[k]);
+                if (e == cudaSuccess) e = terms(t, k, side[k]);
                 if (e == cudaSuccess) e = cudaEventRecord(ev_join[k], side[k]);
             }
-            if (e == cudaSuccess)
-                e = launch_terms(c, main_k, term_items[t][main_k], static_cast<int>(P.term[t][main_k].size()), t,
-                                 stream);
+            if (e == cudaSuccess) e = terms(t, main_k, stream);
             for (int i = 0; i < nk && e == cudaSuccess; ++i)
                 if (kinds[i] != main_k) e = cudaStreamWaitEvent(stream, ev_join[kinds[i]], 0);
             if (e != cudaSuccess) return e;

@@ -118,6 +118,20 @@ int main(int argc, char **argv) {
         }
         std::printf("]");
     }
+    // launch heads: per traverser, [CR1 heads (none), CR2 heads]
+    std::printf("], \"heads\": [");
+    for (int t = 0; t < np; ++t) {
+        std::printf("%s[", t ? ", " : "");
+        int kk = 0;
+        for (int kind : {ssb::TK_CR1, ssb::TK_CR2}) {
+            std::printf("%s[", kk++ ? ", " : "");
+            if (rc == SS_OK)
+                for (size_t i = 0; i < P.term_heads[t][kind].size(); ++i)
+                    std::printf("%s%d", i ? ", " : "", P.term_heads[t][kind][i]);
+            std::printf("]");
+        }
+        std::printf("]");
+    }
     // two-opponent chains: per traverser, every item's [chain, chained]
     std::printf("], \"chains\": [");
     for (int t = 0; t < np; ++t) {

@@ -165,6 +165,19 @@ def test_terminal_routing(kinds_driver, np_, nb, nh, dup, leaves, raises):
     assert d["dup"] == [1 if p == dup else 0 for p in range(np_)]
     assert d["kinds"] == expected_kinds(d, np_, nb == 5, leaves)
     check_groups(d)
+    check_heads(d)
+
+
+def check_heads(d):
+    """Two-opponent launches have one block per head: every group leader
+    (follow 0) that no chain head computes (chained 0), in item order; the
+    one-opponent kind keeps one block per item (no heads)."""
+    for t, per_kind in enumerate(d["groups"]):
+        items = per_kind[1]                          # CR2
+        chained = [c[1] for c in d["chains"][t]]
+        want = [i for i, it in enumerate(items) if it[1] == 0 and chained[i] == 0]
+        assert d["heads"][t][1] == want
+        assert d["heads"][t][0] == []
 
 
 def check_groups(d):
@@ -204,6 +217,7 @@ def test_two_opponent_chains(kinds_driver, raises, bets):
                        capture_output=True, text=True)
     d = json.loads(r.stdout)
     assert d["rc"] == 0
+    check_heads(d)
     chained_any = False
     long_launch = False
     for t in range(3):
