@@ -101,7 +101,7 @@ struct alignas(16) CfvItem {
     int sg = 0;               // subgame of a batch (0 for a single subgame)
     float scale = 1.f;        // the node's value row is stored times this (chance weights; 1 on one street)
     int nfr = 0;              // inline frontier: its number of rows (0: not inline)
-    int fr_bnd = 0;           // inline frontier: end of edge a's rows at bits 4a .. 4a+3 (15 past the last edge)
+    int fr_bnd = 0;           // inline frontier: (end of edge a's rows) - 1 at bits 4a .. 4a+3 (15 past the last edge)
     int fr[kCfvInline] = {};  // inline frontier: the rows of all edges, in order
 };
 // fills the inline frontier of it when the frontier is short enough

@@ -246,8 +246,8 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
             // no index loads before them; each row adds to its edge in row order
             const unsigned bnd = static_cast<unsigned>(I.fr_bnd);
             static_assert(kCfvInline == 8, "two 16-byte loads of inline rows");
-            const int4 f0 = __ldg(reinterpret_cast<const int4 *>(items + it) + 2);
-            const int4 f1 = __ldg(reinterpret_cast<const int4 *>(items + it) + 3);
+            const int4 *fp = reinterpret_cast<const int4 *>(items + it) + 2;
+            const int4 f0 = __ldg(fp), f1 = __ldg(fp + 1);
             const int rows[kCfvInline] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
             float2 x[kCfvInline];
 #pragma unroll
@@ -256,10 +256,10 @@ __global__ void __launch_bounds__(kCfvThreads, 8) k_cfv(DevCtx c0, const DevCtx 
 #pragma unroll
             for (int i = 0; i < kCfvInline; ++i) {
                 if (i < I.nfr) {
-                    int e = 0;
+                    int e = 0;   // the edge of row i: the edges whose last row (nibble) is before it
 #pragma unroll
                     for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a)
-                        e += i >= static_cast<int>((bnd >> (4 * a)) & 15u) ? 1 : 0;
+                        e += i > static_cast<int>((bnd >> (4 * a)) & 15u) ? 1 : 0;
 #pragma unroll
                     for (int a = 0; a < SS_MAX_ACTIONS; ++a)
                         if (e == a) add2(ev[a], x[i]);

@@ -107,7 +107,7 @@ void inline_frontier(CfvItem &it, const std::vector<int> &fr_off, const std::vec
     if (n <= 0 || n > kCfvInline || it.na > SS_MAX_ACTIONS) return;
     unsigned bnd = 0;
     for (int a = 0; a < SS_MAX_ACTIONS; ++a)
-        bnd |= static_cast<unsigned>(a < it.na ? fr_off[it.first_edge + a + 1] - k0 : 15) << (4 * a);
+        bnd |= static_cast<unsigned>(a < it.na ? fr_off[it.first_edge + a + 1] - k0 - 1 : 15) << (4 * a);
     for (int i = 0; i < n; ++i) it.fr[i] = fr_items[k0 + i];
     it.nfr = n;
     it.fr_bnd = static_cast<int>(bnd);

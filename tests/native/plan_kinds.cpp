@@ -118,6 +118,27 @@ int main(int argc, char **argv) {
         }
         std::printf("]");
     }
+    // value/regret items with an inline frontier: rows and per-edge ends
+    // decode to the frontier tables (bad = mismatches), and every frontier
+    // short enough is inline
+    int inl = 0, bad = 0;
+    if (rc == SS_OK)
+        for (int t = 0; t < np; ++t)
+            for (const auto &lv : P.cfv_levels[t])
+                for (const ssb::CfvItem &it : lv) {
+                    const int k0 = P.fr_off[it.first_edge], n = P.fr_off[it.first_edge + it.na] - k0;
+                    if ((n <= ssb::kCfvInline) != (it.nfr == n)) ++bad;
+                    if (it.nfr == 0) continue;
+                    ++inl;
+                    for (int i = 0; i < n; ++i) {
+                        if (it.fr[i] != P.fr_items[k0 + i]) ++bad;
+                        int e = 0;
+                        for (int a = 0; a < SS_MAX_ACTIONS - 1; ++a)
+                            e += i > static_cast<int>((static_cast<unsigned>(it.fr_bnd) >> (4 * a)) & 15u) ? 1 : 0;
+                        if (!(P.fr_off[it.first_edge + e] <= k0 + i && k0 + i < P.fr_off[it.first_edge + e + 1])) ++bad;
+                    }
+                }
+    std::printf("], \"cfv_inline\": [%d, %d", inl, bad);
     // launch heads: per traverser, [CR1 heads (none), CR2 heads]
     std::printf("], \"heads\": [");
     for (int t = 0; t < np; ++t) {

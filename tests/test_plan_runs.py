@@ -166,6 +166,8 @@ def test_terminal_routing(kinds_driver, np_, nb, nh, dup, leaves, raises):
     assert d["kinds"] == expected_kinds(d, np_, nb == 5, leaves)
     check_groups(d)
     check_heads(d)
+    inline, bad = d["cfv_inline"]
+    assert bad == 0 and inline > 0, "inline value/regret frontiers decode to the frontier tables"
 
 
 def check_heads(d):
