@@ -618,7 +618,7 @@ constexpr int kMaxHS = 1344;  // largest row stride: 1326 combos rounded up to 3
 // terminal's leaf row, per-card terms, staged group items
 template <class T>
 constexpr size_t cr2_smem(int HS) {
-    return 3 * 52 * MS * sizeof(T) + static_cast<size_t>(HS) * 4 + 3 * 56 * sizeof(double) + 53 * sizeof(Cr2Cnt) +
+    return 3 * 52 * MS * sizeof(T) + (static_cast<size_t>(HS) + 4) * sizeof(T) + 3 * 56 * sizeof(double) + 53 * sizeof(Cr2Cnt) +
            53 * 16 + 5 * 48 * 4 + sizeof(Cr2Scalars) + 3 * kTermGroupMax * 4 + 8 * 16;
 }
 
@@ -883,10 +883,11 @@ __device__ __noinline__ int pair_count(const ulonglong2 *Bm, const Cr2Cnt *cnt, 
 // one block, one group after the other: the first opponent's matrix, its
 // column sums and masks are built once for the chain.
 // Phases per group: cp.async staging of the reach rows (both for the
-// chain's first group, the second opponent's for the others) and the first
-// leaf row; gather (or clear + scatter for ranges that repeat a combo); P
-// (tensor cores) alongside per-column sums and masks; per-card FP64 terms
-// and block scalars; per-hand mass and one output row per terminal.
+// chain's first group; the next group's second-opponent row is staged while
+// this group's mass is computed); gather (or clear + scatter for ranges that
+// repeat a combo); P (tensor cores) alongside per-column sums and masks;
+// per-card FP64 terms and block scalars; per-hand mass and one output row
+// per terminal (the leaf factors read one hand ahead from global memory).
 template <class T>
 __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_cr2(DevCtx c0, const DevCtx *__restrict__ ctxs,
                                                               const TermItem *__restrict__ items,
@@ -920,19 +921,20 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     int *gnode = cv.take<int>(kTermGroupMax);
     int *gleaf = cv.take<int>(kTermGroupMax);
     float *gpay = cv.take<float>(kTermGroupMax);
-    float *leaf0 = cv.take<float>(HS);   // last: every other offset is a constant
-    // staged reach rows, each followed by a zero (P is written after the gather)
-    T *r1 = P, *r2 = P + HS + 16 / sizeof(T);
+    // the second opponent's staged reach row, followed by a zero (last: every
+    // other offset is a constant); the next group's row lands here while
+    // this group's mass is computed.  The first opponent's row is staged in
+    // P's space (P is written after the gather).
+    T *r2 = cv.take<T>(HS + 16 / sizeof(T));
+    T *r1 = P;
     bool mma = false;
     if constexpr (sizeof(T) == 4) mma = Dp <= 48;
     const int Ht = V.Ht;
     const int *__restrict__ tc = V.code_t;
 
-    // staging of a group: the second opponent's reach row (16-byte chunks;
-    // rows start on 128-byte boundaries), the group's first leaf row (4-byte
-    // words) and its items' fields; with_first: the first opponent's row too
-    auto stage = [&](const TermItem *G, bool with_first) {
-        const int ng = G->gextra + 1;
+    // staging: a group's second-opponent reach row (16-byte chunks; rows
+    // start on 128-byte boundaries), the first opponent's row with with_first
+    auto stage_rows = [&](const TermItem *G, bool with_first) {
         constexpr int per = 16 / sizeof(T);
         const T *s1 = V.reach + static_cast<size_t>(G->opp_row[0]) * HS;
         const T *s2 = V.reach + static_cast<size_t>(G->opp_row[1]) * HS;
@@ -940,20 +942,14 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
             if (with_first) cp_async16(r1 + i, s1 + i);
             cp_async16(r2 + i, s2 + i);
         }
-        const int lo = G->leaf_off;
-        if (lo >= 0) {
-            const float *src = V.leaf + lo;
-            for (int h = tid; h < Ht; h += kTermThreads) cp_async4(leaf0 + h, src + h);
-        }
-        if (tid < ng) {
+    };
+    // a group's items' fields
+    auto stage_items = [&](const TermItem *G) {
+        if (tid <= G->gextra) {
             const TermItem &I = G[tid];
             gnode[tid] = I.node;
             gleaf[tid] = I.leaf_off;
             gpay[tid] = I.payoff;
-        }
-        if (tid == 0) {
-            r1[HS] = T(0);
-            r2[HS] = T(0);
         }
     };
     auto gather_second = [&]() {
@@ -964,7 +960,12 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
     };
 
     // the chain's first group: both opponents' matrices
-    stage(I0, true);
+    stage_rows(I0, true);
+    stage_items(I0);
+    if (tid == 0) {
+        r1[HS] = T(0);
+        r2[HS] = T(0);
+    }
     if (V.dup) {
         zero_matrix(M1);
         zero_matrix(M2);
@@ -1002,6 +1003,9 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
             if (s < 2 * Dp && (first || s >= Dp)) column_stats(M1, M2, s, Dp, cu1, cu2, Bm);
         }
         __syncthreads();
+        // the chain's next group: its second-opponent row is brought in while
+        // this group's mass is computed (the gather of this group's is done)
+        if (q < nchain) stage_rows(G + ng, false);
 
         // phase B: per-card terms (w from the row and column sums of P, d from its
         // diagonal: P = M1 M2 with symmetric M1, M2 gives rowsum = M1 u2,
@@ -1065,15 +1069,18 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
         const Cr2Scalars S = *sc;
         const double zmin = 1e-4 * S.F1 * S.F2;
         const bool none = !(S.F1 > 0.0 && S.F2 > 0.0);   // an opponent without positive reach: all zero
-        const bool leaf_first = gleaf[0] >= 0;
+        const int gl0 = gleaf[0];
         const float gp0 = gpay[0];
         T *out0 = V.val + static_cast<size_t>(gnode[0]) * HS;
         // the next hand's code is loaded one iteration ahead (the first one at
         // the start of the block), so the loop does not wait on it
         int hc_next = hc_first;
+        float f_next = tid < Ht ? (gl0 >= 0 ? __ldg(V.leaf + gl0 + tid) : gp0) : 0.f;
         for (int h = tid; h < HS; h += kTermThreads) {
             const int hc = hc_next;
+            const float f0 = f_next;
             hc_next = h + kTermThreads < Ht ? __ldg(tc + h + kTermThreads) : 0;
+            f_next = h + kTermThreads < Ht ? (gl0 >= 0 ? __ldg(V.leaf + gl0 + h + kTermThreads) : gp0) : 0.f;
             double v = 0.0;
             if (h < Ht && !none) {
                 const int a = min((hc >> 20) & 63, kCr2Off), b = min((hc >> 26) & 63, kCr2Off);
@@ -1087,7 +1094,6 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
                 v = A1 * A2 + S.QD + cg[a] + cg[b] - m2 * (ua1 + ub1) - m1 * (ua2 + ub2) + 3.0 * m1 * m2 - pp;
                 if (fabs(v) <= zmin && pair_count(Bm, cnt, a, b, S.IF1, S.IF2, S.IQD) <= 0) v = 0.0;
             }
-            const float f0 = h >= Ht ? 0.f : leaf_first ? leaf0[h] : gp0;
             out0[h] = static_cast<T>(static_cast<double>(f0) * v);
             for (int g = 1; g < ng; ++g) {
                 const float f = h >= Ht ? 0.f : gleaf[g] >= 0 ? __ldg(V.leaf + gleaf[g] + h) : gpay[g];
@@ -1099,7 +1105,7 @@ __global__ void __launch_bounds__(kTermThreads, sizeof(T) == 4 ? 5 : 2) k_term_c
         // last one once every thread is done with the shared state
         G += ng;
         __syncthreads();
-        stage(G, false);
+        stage_items(G);
         if (V.dup) zero_matrix(M2);
         cp_async_wait_all();
         __syncthreads();
