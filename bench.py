@@ -267,10 +267,10 @@ def kernel_sources_sha16():
     return h.hexdigest()[:16]
 
 
-def ncu_summary(csv_path, workload, command):
+def ncu_summary(csv_path, workload, command, path=None):
     """Per profile class: launches captured and mean DRAM bytes (read + write)
     per launch, from an ncu --csv launch list with dram__bytes_read.sum and
-    dram__bytes_write.sum; merged into profiles/dram_traffic.json."""
+    dram__bytes_write.sum; merged into path (profiles/dram_traffic.json)."""
     import csv
     per = {}
     with open(csv_path) as f:
@@ -294,7 +294,7 @@ def ncu_summary(csv_path, workload, command):
         e = per.setdefault(cls, {"launches_captured": 0, "bytes": 0.0})
         e["launches_captured"] += 1
         e["bytes"] += d.get("dram__bytes_read.sum", 0.0) + d.get("dram__bytes_write.sum", 0.0)
-    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    path = path or os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         tr = json.load(open(path))
     except Exception:

@@ -46,3 +46,42 @@ def test_reference_cpu_solver_binding():
     secs = RefSolverC().solve(cfg["board"], cfg["hands"], cfg["weights"], cfg["pot"], cfg["stack"],
                               cfg["bet_sizes"], 5)
     assert 0.0 < secs < 60.0
+
+
+def test_ncu_summary_classes(bench, tmp_path):
+    """bench.py --ncu-summary: launches are matched to profile classes by their
+    base function name, whether ncu prints the demangled signature or the bare
+    name; each class keeps its mean DRAM bytes (read + write) per launch, and
+    the file is stamped with the kernel sources' hash."""
+    import csv
+    import json
+    head = ["ID", "Process ID", "Process Name", "Host Name", "Kernel Name", "Context", "Stream", "Block Size",
+            "Grid Size", "Device", "CC", "Section Name", "Metric Name", "Metric Unit", "Metric Value"]
+    launches = [
+        ("0", "void unnamed>::k_term_cr2<float>(DevCtx, const DevCtx *, const TermItem *, const int *, int)",
+         1000, 300),
+        ("1", "void unnamed>::k_term_cr2<float>(DevCtx, const DevCtx *, const TermItem *, const int *, int)",
+         3000, 700),
+        ("2", "void ssb::(anonymous namespace)::k_cfv<1>(DevCtx, const DevCtx *, const CfvItem *, int, int, int)",
+         500, 0),
+        ("3", "k_reach", "1,024", 0),
+        ("4", "cutlass_kernel_not_ours", 9, 9),
+    ]
+    rows = [head]
+    for i, name, rd, wr in launches:
+        for metric, v in (("dram__bytes_read.sum", rd), ("dram__bytes_write.sum", wr),
+                          ("gpu__time_duration.sum", 10)):
+            rows.append([i, "1", "python3", "127.0.0.1", name, "1", "7", "(256, 1, 1)", "(8, 1, 1)", "0", "10.0",
+                         "Command line profiler metrics", metric, "byte", str(v)])
+    src = tmp_path / "launches.csv"
+    with open(src, "w", newline="") as f:
+        f.write("==PROF== Connected to process 1\n")
+        csv.writer(f).writerows(rows)
+    out = tmp_path / "dram_traffic.json"
+    bench.ncu_summary(str(src), "turn3", "ncu ...", path=str(out))
+    tr = json.load(open(out))
+    assert tr["kernel_sources_sha16"] == bench.kernel_sources_sha16()
+    cls = tr["workloads"]["turn3"]["classes"]
+    assert cls == {"term_cr2": {"launches_captured": 2, "dram_bytes_per_launch": 2500},
+                   "cfv": {"launches_captured": 1, "dram_bytes_per_launch": 500},
+                   "reach": {"launches_captured": 1, "dram_bytes_per_launch": 1024}}
