@@ -958,8 +958,8 @@ class Server {
             if (rc == SS_OK) rc = batch.check(pct, nash);
             if (rc != SS_OK && !add.empty() && context_usable()) {
                 // a failure that left the context usable (an allocation or a
-                // graph build for the members added this round): those members
-                // leave with the error, the rest of the batch carries on
+                // graph build for the members admitted before this block):
+                // those members leave with the error, the rest carries on
                 const std::string msg = last_error();
                 for (auto &rs : add) {
                     Request *r = rs.first;
